@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark: Euler N=4 DOF-stage updates per second on a B200.
+
+Workload (the headline configuration): compressible Euler, gamma 1.4,
+periodic unit cube of 32^3 hexahedra x 6 = 196,608 tetrahedra, N=4 (Np=35),
+5 conserved variables, rho = 1 + 0.2 sin(2 pi (x+y+z)), v = (1, 0.5, 0.25),
+p = 1, CFL 0.4, FP64.  Synthetic: the mesh and state are generated here.
+
+A bench "step" is one LSERK time step (5 stages) over the whole mesh.
+DOF-stages per step = K * Np * 5 variables * 5 stages.
+
+Arms:
+  default            libdglm.so: state resident in HBM, steps as captured
+                     CUDA graphs (value); e2e through the C ABI with the state
+                     copied host->device and back every step (e2e).
+  --impl reference   the reference's own CPU solver (oracle/_ref, compiled
+                     from its sources) on this machine's cores; falls back to
+                     the oracle's C restatement when oracle/_ref is absent.
+
+Multi-GPU (torchrun): every rank advances its own replica of the workload
+("replicas only": the single-partition path has no exchange step); value is
+the sum over ranks of DOF-stages divided by the max over ranks of the time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Euler N=4 DOF-stage/s (FP64)"
+UNIT = "DOF-stage/s"
+NOMINAL_FP64_TFLOPS = 40.0     # B200 datasheet FP64 (vector and tensor)
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=32, help="hexahedra per axis (K = 6 n^3)")
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return FALLBACK_PEAKS, "fallback"
+
+
+def bytes_per_element_stage(nvar, Np, Nfp, advection=False):
+    """Algorithmic HBM bytes per element-stage of the fused design: read u,
+    write u', read k, write k; 9 metrics + 4 Fscale + 12 normals + 4 tau;
+    vmapP (int32); advection adds the per-node velocity."""
+    b = 4 * nvar * Np * 8 + 29 * 8 + 4 * 4 * Nfp
+    if advection:
+        b += 3 * Np * 8
+    return b
+
+
+def flops_per_element_stage(nvar, Np, Nfp):
+    """FMA = 2 flops; the three volume and the LIFT contractions only."""
+    return nvar * (6 * Np * Np + 2 * Np * 4 * Nfp)
+
+
+def read_traffic(kernel_tag):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu
+    summary (profiles/stage_traffic.txt: '<tag> <bytes_per_launch>')."""
+    path = os.path.join(ROOT, "profiles", "stage_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel_tag and not line.startswith("#"):
+                try:
+                    return float(parts[1])
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(a):
+    from exadglm_b200 import problem as P
+    return P.euler_sine(n=a.n, N=a.order, cfl=0.4)
+
+
+def dof_stages_per_step(p):
+    return p.K * p.Np * p.nvar * 5
+
+
+def cpu_reference_rate(p, steps, threads=None):
+    """Time `steps` LSERK steps of the reference CPU solver (or the oracle
+    port) on this host.  Returns (rate, kind, cores, seconds)."""
+    import oracle
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    if oracle.ref_available(p.physics, p.N):
+        r = oracle.RefSolver(p)
+        r.run(1)                                  # warm the caches / page in
+        r.set_state(p.u0)
+        t0 = time.perf_counter()
+        done = r.run(steps)
+        dt = time.perf_counter() - t0
+        r.close()
+        kind = "reference"
+    else:
+        o = oracle.Oracle(p)
+        o.run(1)
+        t0 = time.perf_counter()
+        _, _, clk, _ = o.run(steps)
+        dt = time.perf_counter() - t0
+        done = clk.tstep
+        kind = "port"
+    return dof_stages_per_step(p) * done / dt, kind, threads, dt
+
+
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    p = build_problem(a)
+    import oracle
+    threads = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    have_ref = oracle.ref_available(p.physics, p.N)
+    solver = oracle.RefSolver(p) if have_ref else oracle.Oracle(p)
+    kind = "reference" if have_ref else "port"
+
+    def one_step():
+        if have_ref:
+            solver.run(1)
+        else:
+            solver_state["u"], solver_state["k"], _, _ = solver.run(
+                1, u=solver_state["u"], k=solver_state["k"])
+
+    solver_state = {"u": p.u0.copy(), "k": None}
+    for _ in range(a.warmup):
+        one_step()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        one_step()
+    el = time.perf_counter() - t0
+    rate = dof_stages_per_step(p) * a.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * el / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"euler_sine N={p.N} K={p.K} (n={a.n}) CFL 0.4, 1 LSERK step",
+                   "K": p.K, "N": p.N, "Np": p.Np, "nvar": 5},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{a.steps} full LSERK steps of the K={p.K} mesh"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if have_ref:
+        solver.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference_arm(a)
+
+    import numpy as np
+    import torch
+    from exadglm_b200.capi import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p = build_problem(a)
+    s = Solver(p, precision=a.precision, device=local)
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    per_step = dof_stages_per_step(p)
+
+    # ---- device-resident value -------------------------------------------
+    s.step(a.warmup)
+    s.sync()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.step(a.steps)
+    ev1.record(stream)
+    launches = s.kernel_launches()
+    ev1.synchronize()
+    s.sync()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    barrier()
+    ms_max = max_over_ranks(ms)
+    value = world * per_step * a.steps / (ms_max * 1e-3)
+
+    # ---- stage kernel alone, for the roofline -----------------------------
+    t, dt, _ = s.time()
+    reps = 25
+    for i in range(5):
+        s.stage(i % 5, dt)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream.synchronize()
+    e0.record(stream)
+    for i in range(reps):
+        s.stage(i % 5, dt)
+    e1.record(stream)
+    e1.synchronize()
+    stage_ms = e0.elapsed_time(e1) / reps
+    peaks, peak_kind = load_peaks()
+    B = bytes_per_element_stage(p.nvar, p.Np, p.Nfp) * p.K
+    F = flops_per_element_stage(p.nvar, p.Np, p.Nfp) * p.K
+    achieved_gbs = B / (stage_ms * 1e-3) / 1e9
+    achieved_tf = F / (stage_ms * 1e-3) / 1e12
+    tag = f"euler_N{p.N}_K{p.K}_{a.precision}"
+    roof = {
+        "kernel": "stage_fp64_kernel<EUL,%d>" % p.N,
+        "bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+        "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": read_traffic(tag),
+        "peak_source": f"{peak_kind} hbm_gbs (burst, kernel timed alone)",
+        "algorithmic_bytes_per_launch": B, "launch_ms": stage_ms,
+        "binding_roof": "fp64",
+        "fp64": {"achieved_tflops": achieved_tf, "peak_tflops": NOMINAL_FP64_TFLOPS,
+                 "peak_source": "nominal B200 FP64 (not measured on this pool)",
+                 "frac": achieved_tf / NOMINAL_FP64_TFLOPS, "flops_per_launch": F},
+    }
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    nv, n = p.nvar, p.K * p.Np
+    host_in = torch.empty((nv, n), dtype=torch.float64, pin_memory=True)
+    host_in.copy_(torch.from_numpy(np.ascontiguousarray(p.u0)))
+    host_out = torch.empty((nv, n), dtype=torch.float64, pin_memory=True)
+    pin_in = [host_in[v].data_ptr() for v in range(nv)]
+    pin_out = [host_out[v].data_ptr() for v in range(nv)]
+    e2e_steps = max(3, min(a.steps, 10))
+    for _ in range(2):
+        s.set_state_ptrs(pin_in, 0)
+        s.step(1)
+        s.get_state_ptrs(pin_out, 0)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.set_state_ptrs(pin_in, 0)     # H2D of the step's input state
+        s.step(1)
+        s.get_state_ptrs(pin_out, 0)    # D2H of the step's result (synchronises)
+    el = time.perf_counter() - t0
+    el = max_over_ranks(el)
+    e2e = {"value": world * per_step * e2e_steps / el, "unit": UNIT,
+           "h2d_bytes_per_step": nv * n * 8, "d2h_bytes_per_step": nv * n * 8,
+           "what": "per step: dglm_set_state from pinned host, dglm_step(1), "
+                   "dglm_get_state to pinned host"}
+    s.close()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"euler_sine N={p.N} K={p.K} (n={a.n}^3 x 6) CFL 0.4, "
+                               f"{a.precision}, one replica per GPU",
+                   "K": p.K, "N": p.N, "Np": p.Np, "nvar": 5, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (state 3 x 275 MB)"},
+        "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+    }
+    if rank == 0 and not a.no_cpu_baseline:
+        sample_steps = 1
+        rate, kind, cores, secs = cpu_reference_rate(p, sample_steps)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": f"{sample_steps} LSERK step of the K={p.K} mesh "
+                                          f"({secs:.1f} s)"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

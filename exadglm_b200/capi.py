@@ -1,0 +1,227 @@
+"""ctypes binding of libdglm.so (include/dglm.h).
+
+The library is built in-tree by ``python -m exadglm_b200.build``; loading
+fails loudly when it is missing -- there is no CPU fallback on this path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdglm.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_NONFINITE, ERR_UNSUPPORTED, ERR_STATE, ERR_NOMEM, ERR_IO = range(8)
+ADVECTION, EULER = 0, 1
+PREC_FP64, PREC_TF32X3, PREC_BF16X3 = 0, 1, 2
+PRECISIONS = {"fp64": PREC_FP64, "tf32x3": PREC_TF32X3, "bf16x3": PREC_BF16X3}
+
+# every symbol include/dglm.h declares
+EXPORTS = (
+    "dglm_last_error", "dglm_abi_version", "dglm_order_supported", "dglm_create",
+    "dglm_destroy", "dglm_set_stream", "dglm_upload_mesh", "dglm_set_state", "dglm_get_state",
+    "dglm_step", "dglm_step_fixed_dt", "dglm_stage", "dglm_sync", "dglm_get_time", "dglm_get_dt_history",
+    "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
+    "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
+    "dglm_update_rhs", "dglm_lserk_stage",
+)
+
+
+class DglmError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"[dglm status {status}] {msg}")
+        self.status = status
+
+
+class Desc(C.Structure):
+    _fields_ = [("N", C.c_int), ("physics", C.c_int), ("K", C.c_int), ("precision", C.c_int),
+                ("cfl", C.c_double), ("gamma", C.c_double), ("tau_scale", C.c_double),
+                ("tmax", C.c_double), ("device", C.c_int)]
+
+
+_P = C.c_void_p
+_MESH_FIELDS = ["WDr", "WDs", "WDt", "LIFT", "matrix_order", "rx", "ry", "rz", "sx", "sy", "sz",
+                "tx", "ty", "tz", "Fscale", "nx", "ny", "nz", "EtoB", "vmapF", "vmapP", "Fmask",
+                "vx", "vy", "vz"]
+
+
+class MeshArrays(C.Structure):
+    _fields_ = [(n, C.c_char if n == "matrix_order" else _P) for n in _MESH_FIELDS]
+
+
+_lib = None
+
+
+def lib():
+    """Load libdglm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m exadglm_b200.build` "
+                               "(the CUDA library is the only implementation of this path)")
+        L = C.CDLL(LIB_PATH)
+        L.dglm_last_error.restype = C.c_char_p
+        L.dglm_create.argtypes = [C.POINTER(Desc), C.POINTER(_P)]
+        L.dglm_upload_mesh.argtypes = [_P, C.POINTER(MeshArrays)]
+        L.dglm_set_state.argtypes = [_P, _P, C.c_int]
+        L.dglm_get_state.argtypes = [_P, _P, C.c_int]
+        L.dglm_step.argtypes = [_P, C.c_int]
+        L.dglm_step_fixed_dt.argtypes = [_P, C.c_int, C.c_double]
+        L.dglm_stage.argtypes = [_P, C.c_int, C.c_double]
+        L.dglm_set_stream.argtypes = [_P, _P]
+        L.dglm_sync.argtypes = [_P]
+        L.dglm_destroy.argtypes = [_P]
+        L.dglm_get_time.argtypes = [_P, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                    C.POINTER(C.c_int)]
+        L.dglm_get_dt_history.argtypes = [_P, C.c_int, C.c_int, _P]
+        L.dglm_rhs.argtypes = [_P, _P, _P]
+        L.dglm_kernel_launches.argtypes = [_P]
+        L.dglm_kernel_launches.restype = C.c_long
+        L.dglm_device_bytes.argtypes = [_P]
+        L.dglm_device_bytes.restype = C.c_size_t
+        D, I = C.c_double, C.c_int
+        L.dglm_calc_maxv.argtypes = [I, I, I, D, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.dglm_calc_dt.argtypes = [I, I, D, _P, _P, _P]
+        L.dglm_update_tau.argtypes = [I, D, _P, _P, _P, _P]
+        L.dglm_update_ub.argtypes = [I, I, I, _P, _P, _P, _P, _P]
+        L.dglm_calc_fluxLM.argtypes = [I, I, I, D, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                       _P, _P]
+        L.dglm_calc_fluxes.argtypes = [I, I, I, D, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.dglm_update_rhs.argtypes = [I, I, I, _P, _P, _P, _P, C.c_char, _P, _P, _P, _P, _P, _P]
+        L.dglm_lserk_stage.argtypes = [I, I, I, D, D, D, _P, _P, _P, _P]
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != OK:
+        raise DglmError(status, lib().dglm_last_error().decode())
+
+
+def ptr_table(ptrs):
+    """HOST array of device (or host) pointers, as the per-variable tables of
+    the C ABI expect."""
+    arr = (C.c_void_p * len(ptrs))(*[C.c_void_p(int(p)) for p in ptrs])
+    return arr
+
+
+def _np_ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Solver:
+    """A solver handle for one problem (see :mod:`exadglm_b200.problem`).
+
+    ``state`` arrays are numpy (nvar, K*Np) on the host, or lists of device
+    pointers for the on-device variants."""
+
+    def __init__(self, problem, precision="fp64", device=0, matrix_order="c", arrays=None):
+        self.p = problem
+        L = lib()
+        d = Desc()
+        d.N, d.K = problem.N, problem.K
+        d.physics = EULER if problem.physics == "euler" else ADVECTION
+        d.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        d.cfl, d.gamma, d.tau_scale, d.tmax = problem.cfl, problem.gamma, problem.tau_scale, \
+            problem.tmax
+        d.device = device
+        h = _P()
+        check(L.dglm_create(C.byref(d), C.byref(h)))
+        self.h, self.L = h, L
+        arr = arrays if arrays is not None else problem.datain_arrays()
+        keep = {}
+
+        def f64(name, a, order="C"):
+            keep[name] = np.ascontiguousarray(np.asarray(a, np.float64).ravel(order))
+            return keep[name].ctypes.data
+
+        def i32(name, a):
+            keep[name] = np.ascontiguousarray(np.asarray(a, np.int32).ravel())
+            return keep[name].ctypes.data
+
+        m = MeshArrays()
+        m.matrix_order = matrix_order.encode()
+        order = "F" if matrix_order == "f" else "C"
+        for n in ("WDr", "WDs", "WDt", "LIFT"):
+            setattr(m, n, f64(n, arr[n], order))
+        for n in ("rx", "ry", "rz", "sx", "sy", "sz", "tx", "ty", "tz", "Fscale", "nx", "ny",
+                  "nz"):
+            setattr(m, n, f64(n, arr[n]))
+        for n in ("EtoB", "vmapF", "vmapP", "Fmask"):
+            setattr(m, n, i32(n, arr[n]))
+        if problem.vel is not None:
+            m.vx, m.vy, m.vz = (f64(n, problem.vel[i]) for i, n in enumerate(("vx", "vy", "vz")))
+        check(L.dglm_upload_mesh(h, C.byref(m)))
+        self.set_state(problem.u0)
+
+    # -- state ------------------------------------------------------------
+    def set_state(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.p.nvar, -1)
+        self._u_host = u
+        check(self.L.dglm_set_state(self.h, ptr_table([u[v].ctypes.data for v in range(len(u))]),
+                                    0))
+
+    def set_state_ptrs(self, ptrs, on_device):
+        check(self.L.dglm_set_state(self.h, ptr_table(ptrs), int(on_device)))
+
+    def get_state_ptrs(self, ptrs, on_device):
+        check(self.L.dglm_get_state(self.h, ptr_table(ptrs), int(on_device)))
+
+    def set_state_device(self, ptrs):
+        check(self.L.dglm_set_state(self.h, ptr_table(ptrs), 1))
+
+    def get_state(self):
+        out = np.empty((self.p.nvar, self.p.K * self.p.Np))
+        check(self.L.dglm_get_state(self.h, ptr_table([out[v].ctypes.data
+                                                        for v in range(len(out))]), 0))
+        return out
+
+    def get_state_device(self, ptrs):
+        check(self.L.dglm_get_state(self.h, ptr_table(ptrs), 1))
+
+    # -- time stepping ----------------------------------------------------
+    def step(self, nsteps=1, dt=None):
+        if dt is None:
+            check(self.L.dglm_step(self.h, int(nsteps)))
+        else:
+            check(self.L.dglm_step_fixed_dt(self.h, int(nsteps), float(dt)))
+
+    def stage(self, stage, dt):
+        check(self.L.dglm_stage(self.h, int(stage), float(dt)))
+
+    def sync(self):
+        check(self.L.dglm_sync(self.h))
+
+    def time(self):
+        t, dt, ts = C.c_double(), C.c_double(), C.c_int()
+        check(self.L.dglm_get_time(self.h, C.byref(t), C.byref(dt), C.byref(ts)))
+        return t.value, dt.value, ts.value
+
+    def dt_history(self, first, count):
+        out = np.zeros(count)
+        check(self.L.dglm_get_dt_history(self.h, int(first), int(count), _np_ptr(out)))
+        return out
+
+    def rhs_device(self, u_ptrs, rhs_ptrs):
+        check(self.L.dglm_rhs(self.h, ptr_table(u_ptrs), ptr_table(rhs_ptrs)))
+
+    def set_stream(self, stream_ptr):
+        check(self.L.dglm_set_stream(self.h, C.c_void_p(int(stream_ptr))))
+
+    def kernel_launches(self):
+        return int(self.L.dglm_kernel_launches(self.h))
+
+    def device_bytes(self):
+        return int(self.L.dglm_device_bytes(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dglm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,115 @@
+// Internal declarations shared by the libdglm translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "dglm.h"
+
+namespace dglm {
+
+constexpr int kMaxOrder = 8;
+constexpr int kHistory = 65536;          // dt history ring (steps)
+
+__host__ __device__ constexpr int np_of(int N) { return (N + 1) * (N + 2) * (N + 3) / 6; }
+__host__ __device__ constexpr int nfp_of(int N) { return (N + 1) * (N + 2) / 2; }
+
+// Per-handle scalars that live on the device so a step needs no host round
+// trip: the CFL dt is computed from a device-wide max of the face wave
+// speeds (reference: cublasIdamax + a blocking copy, euler_nopad_dglm.cu:79-96).
+struct DevScalars {
+  double t;                       // simulated time
+  double dt;                      // dt of the step in flight / last step
+  double dt_fixed;                // > 0: prescribed dt instead of the CFL dt
+  unsigned long long acc[2];      // max over faces of maxv*Fscale, as bits
+  int tstep;                      // steps taken
+  int parity;                     // which acc[] the next step reads
+  int active;                     // 1 while t < tmax for the step in flight
+  int flags;                      // bit 0: non-finite dt / wave speed; bit 1: non-finite state
+};
+
+// Arguments of the fused stage kernels.  Field arrays are one allocation
+// with `vs` doubles between variables.
+struct StageArgs {
+  const double *AT;      // stacked operators, k-major: (3Np+NFF) x IP
+  const double *geo;     // rx,ry,rz,sx,sy,sz,tx,ty,tz, each K doubles
+  const double *fscale;  // K*4
+  const double *nrm;     // nx, ny, nz, each K*4
+  const double *tau;     // K*4
+  const int *vmapP;      // K*4*Nfp
+  const int *Fmask;      // 4*Nfp
+  const double *vel;     // advection: vx, vy, vz with stride vs
+  const double *u_in;
+  double *u_out;
+  double *kreg;
+  double *maxv;          // K*4 (written on the last stage)
+  DevScalars *sc;
+  long vs;
+  int K;
+  double gamma;
+  double rka, rkb;
+  int last_stage;        // 1: also compute maxv of the new state (Euler)
+  int rhs_only;          // 1: write the right-hand side to u_out, no LSERK update
+  double dt_override;    // >= 0: use this dt instead of sc->dt
+};
+
+// Reference Euler flux (F, G, W) of the state q, in the arithmetic order of
+// euler_dglm.cpp:152-168 / euler_nopad_dglm.cu:181-198 (vb2 is |m|^2).
+__device__ __forceinline__ void euler_flux(double g, const double q[5], double F[5],
+                                           double G[5], double W[5]) {
+  const double u1 = q[0], u2 = q[1], u3 = q[2], u4 = q[3], u5 = q[4];
+  const double v2 = u2 * u2 + u3 * u3 + u4 * u4;
+  const double p = (g - 1) * (u5 - 0.5 * v2 / u1);
+  F[0] = u2;
+  F[1] = (u2 * u2) / u1 + p;
+  F[2] = (u2 * u3) / u1;
+  F[3] = (u2 * u4) / u1;
+  F[4] = (u5 + p) * (u2 / u1);
+  G[0] = u3;
+  G[1] = u2 * u3 / u1;
+  G[2] = (u3 * u3) / u1 + p;
+  G[3] = u3 * u4 / u1;
+  G[4] = (u5 + p) * (u3 / u1);
+  W[0] = u4;
+  W[1] = u2 * u4 / u1;
+  W[2] = u3 * u4 / u1;
+  W[3] = (u4 * u4) / u1 + p;
+  W[4] = (u5 + p) * (u4 / u1);
+}
+
+// Maxima of non-negative doubles are taken on their bit patterns: for
+// sign-bit-clear doubles the unsigned order is the numeric order, and a NaN
+// (exponent all ones, non-zero mantissa) orders above +Inf, so it propagates
+// into dt where the step kernel flags it.
+__device__ __forceinline__ unsigned long long dbits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+__device__ __forceinline__ unsigned long long warp_max_bits(unsigned long long b) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_xor_sync(0xffffffffu, b, o);
+    b = x > b ? x : b;
+  }
+  return b;
+}
+
+// error plumbing (dglm_solver.cu)
+dglm_status set_error(dglm_status s, const std::string &msg);
+dglm_status cuda_check(cudaError_t e, const char *what);
+
+// fused FP64 stage launcher (dglm_stage_fp64.cu)
+bool stage_fp64_supported(int physics, int N);
+int stage_rows_padded(int physics, int N);  // IP: padded row count of AT
+cudaError_t launch_stage_fp64(int physics, int N, const StageArgs &a, cudaStream_t s);
+cudaError_t launch_face_maxv(int physics, int N, const StageArgs &a, int parity_slot,
+                             cudaStream_t s);
+cudaError_t launch_step_begin(int N, double cfl, double tmax, int frozen, DevScalars *sc,
+                              double *dt_hist, cudaStream_t s);
+cudaError_t launch_tau(int K, double tau_scale, const int *vmapF, const double *maxv,
+                       double *tau, cudaStream_t s);
+cudaError_t launch_step_end(DevScalars *sc, cudaStream_t s);
+cudaError_t launch_finite_check(const double *u, long vs, long n, int nvar, DevScalars *sc,
+                                cudaStream_t s);
+
+}  // namespace dglm

@@ -1,0 +1,542 @@
+// Solver handle: owns the device arrays of one mesh partition and runs the
+// LSERK time loop (the reference's DataDev, euler_nopad_data_dev.cu:9-266,
+// and runRK, euler_nopad_time.cu:32-108) as a captured CUDA graph of
+//   step_begin (dt on the device) -> tau -> 5 fused stages -> step_end
+// with no host synchronisation inside a step.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dglm_common.cuh"
+
+namespace dglm {
+
+static thread_local std::string g_last_error;
+
+dglm_status set_error(dglm_status s, const std::string &msg) {
+  g_last_error = msg;
+  return s;
+}
+
+dglm_status cuda_check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return DGLM_OK;
+  return set_error(DGLM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace dglm
+
+using namespace dglm;
+
+struct dglm_handle {
+  dglm_desc d{};
+  int nvar = 0, Np = 0, Nfp = 0, NFF = 0, IP = 0;
+  long vs = 0;                    // doubles between variables of a field
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // mesh, operators
+  double *AT = nullptr, *geo = nullptr, *fscale = nullptr, *nrm = nullptr;
+  double *tau = nullptr, *maxv = nullptr, *vel = nullptr;
+  int *vmapP = nullptr, *vmapF = nullptr, *Fmask = nullptr;
+  // state
+  double *u[2] = {nullptr, nullptr};
+  double *kreg = nullptr;
+  int cur = 0;
+  DevScalars *sc = nullptr;
+  double *dt_hist = nullptr;
+  // one-off right-hand side evaluation
+  double *rhs_in = nullptr, *rhs_out = nullptr, *maxv_s = nullptr, *tau_s = nullptr;
+  DevScalars *sc_s = nullptr;
+  bool mesh_ready = false, state_ready = false;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long launches = 0;
+  size_t bytes = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+// Carpenter & Kennedy 5-stage 4th-order 2N-storage coefficients
+// (euler_data.cpp:41-60).
+const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0,
+                       -2404267990393.0 / 2016746695238.0, -3550918686646.0 / 2091501179385.0,
+                       -1275806237668.0 / 842570457699.0};
+const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                       2277821191437.0 / 14882151754819.0};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (dev >= 0 && dev != prev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+template <typename T>
+dglm_status dalloc(dglm_handle *h, T **p, size_t count) {
+  void *q = nullptr;
+  const size_t n = count * sizeof(T);
+  cudaError_t e = cudaMalloc(&q, n ? n : 16);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(DGLM_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+  }
+  h->allocs.push_back(q);
+  h->bytes += n;
+  *p = static_cast<T *>(q);
+  return DGLM_OK;
+}
+
+void drop_graphs(dglm_handle *h) {
+  for (auto &g : h->graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+}
+
+bool all_finite(const double *a, size_t n) {
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+bool in_range(const int *a, size_t n, long lo, long hi) {
+  for (size_t i = 0; i < n; i++)
+    if (a[i] < lo || a[i] >= hi) return false;
+  return true;
+}
+
+StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
+  StageArgs a{};
+  a.AT = h->AT;
+  a.geo = h->geo;
+  a.fscale = h->fscale;
+  a.nrm = h->nrm;
+  a.tau = h->tau;
+  a.vmapP = h->vmapP;
+  a.Fmask = h->Fmask;
+  a.vel = h->vel;
+  a.u_in = u_in;
+  a.u_out = u_out;
+  a.kreg = h->kreg;
+  a.maxv = h->maxv;
+  a.sc = h->sc;
+  a.vs = h->vs;
+  a.K = h->d.K;
+  a.gamma = h->d.gamma;
+  a.rka = s >= 0 ? RKA[s] : 0.0;
+  a.rkb = s >= 0 ? RKB[s] : 0.0;
+  a.last_stage = (s == 4);
+  a.rhs_only = 0;
+  a.dt_override = -1.0;
+  return a;
+}
+
+// Issues one LSERK step starting from u[cur] (ends in u[cur^1]).
+dglm_status issue_step(dglm_handle *h, int cur, cudaStream_t s) {
+  const int frozen = h->d.physics == DGLM_ADVECTION;
+  cudaError_t e = launch_step_begin(h->d.N, h->d.cfl, h->d.tmax, frozen, h->sc, h->dt_hist, s);
+  if (e == cudaSuccess && !frozen)
+    e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv, h->tau, s);
+  for (int st = 0; st < 5 && e == cudaSuccess; st++) {
+    const int in = (cur + st) & 1;
+    StageArgs a = stage_args(h, h->u[in], h->u[in ^ 1], st);
+    e = launch_stage_fp64(h->d.physics, h->d.N, a, s);
+  }
+  if (e == cudaSuccess) e = launch_step_end(h->sc, s);
+  return cuda_check(e, "step launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dglm_last_error(void) { return g_last_error.c_str(); }
+int dglm_abi_version(void) { return DGLM_ABI_VERSION; }
+int dglm_order_supported(int N) { return N >= 1 && N <= kMaxOrder; }
+
+dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
+  if (!desc || !out) return set_error(DGLM_ERR_INVALID, "dglm_create: NULL argument");
+  *out = nullptr;
+  const dglm_desc &d = *desc;
+  if (d.physics != DGLM_EULER && d.physics != DGLM_ADVECTION)
+    return set_error(DGLM_ERR_INVALID, "dglm_create: unknown physics");
+  if (!stage_fp64_supported(d.physics, d.N))
+    return set_error(DGLM_ERR_UNSUPPORTED,
+                     "dglm_create: order N=" + std::to_string(d.N) + " is not built (1..8)");
+  if (d.K <= 0) return set_error(DGLM_ERR_INVALID, "dglm_create: K must be positive");
+  if (d.precision != DGLM_PREC_FP64)
+    return set_error(DGLM_ERR_UNSUPPORTED, "dglm_create: precision mode not built");
+  if (!(d.cfl > 0) || !(d.tau_scale >= 0) || !(d.tmax > 0) ||
+      (d.physics == DGLM_EULER && !(d.gamma > 1)))
+    return set_error(DGLM_ERR_INVALID, "dglm_create: cfl/gamma/tau_scale/tmax out of range");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(DGLM_ERR_CUDA, "dglm_create: no CUDA device");
+  if (d.device >= ndev) return set_error(DGLM_ERR_INVALID, "dglm_create: device out of range");
+
+  dglm_handle *h = new dglm_handle();
+  h->d = d;
+  if (d.device < 0) cudaGetDevice(&h->dev); else h->dev = d.device;
+  DeviceGuard g(h->dev);
+  h->nvar = d.physics == DGLM_EULER ? 5 : 1;
+  h->Np = np_of(d.N);
+  h->Nfp = nfp_of(d.N);
+  h->NFF = 4 * h->Nfp;
+  h->IP = stage_rows_padded(d.physics, d.N);
+  const long n = (long)d.K * h->Np;
+  h->vs = (n + 31) / 32 * 32;  // 256-byte aligned variable blocks
+  dglm_status st = DGLM_OK;
+  const long K = d.K;
+  auto chk = [&](dglm_status s) {
+    if (st == DGLM_OK) st = s;
+  };
+  chk(dalloc(h, &h->AT, (size_t)(3 * h->Np + h->NFF) * h->IP));
+  chk(dalloc(h, &h->geo, (size_t)9 * K));
+  chk(dalloc(h, &h->fscale, (size_t)4 * K));
+  chk(dalloc(h, &h->nrm, (size_t)12 * K));
+  chk(dalloc(h, &h->tau, (size_t)4 * K));
+  chk(dalloc(h, &h->maxv, (size_t)4 * K));
+  chk(dalloc(h, &h->vmapP, (size_t)K * h->NFF));
+  chk(dalloc(h, &h->vmapF, (size_t)4 * K));
+  chk(dalloc(h, &h->Fmask, (size_t)h->NFF));
+  if (d.physics == DGLM_ADVECTION) chk(dalloc(h, &h->vel, (size_t)3 * h->vs));
+  chk(dalloc(h, &h->u[0], (size_t)h->nvar * h->vs));
+  chk(dalloc(h, &h->u[1], (size_t)h->nvar * h->vs));
+  chk(dalloc(h, &h->kreg, (size_t)h->nvar * h->vs));
+  chk(dalloc(h, &h->sc, 1));
+  chk(dalloc(h, &h->dt_hist, (size_t)kHistory));
+  if (st == DGLM_OK) {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+      st = set_error(DGLM_ERR_CUDA, "dglm_create: stream creation failed");
+    else
+      h->own_stream = true;
+  }
+  if (st != DGLM_OK) {
+    std::string msg = g_last_error;
+    dglm_destroy(h);
+    return set_error(st, msg);
+  }
+  // zero-padded tails stay zero for the whole life of the handle
+  for (void *p : {(void *)h->u[0], (void *)h->u[1], (void *)h->kreg})
+    cudaMemset(p, 0, sizeof(double) * h->nvar * h->vs);
+  cudaMemset(h->AT, 0, sizeof(double) * (3 * h->Np + h->NFF) * h->IP);
+  *out = h;
+  return cuda_check(cudaDeviceSynchronize(), "dglm_create");
+}
+
+dglm_status dglm_destroy(dglm_handle *h) {
+  if (!h) return DGLM_OK;
+  DeviceGuard g(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return DGLM_OK;
+}
+
+dglm_status dglm_set_stream(dglm_handle *h, void *stream) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_set_stream: NULL handle");
+  DeviceGuard g(h->dev);
+  cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  h->own_stream = false;
+  h->stream = (cudaStream_t)stream;
+  return DGLM_OK;
+}
+
+dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *m) {
+  if (!h || !m) return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: NULL argument");
+  const long K = h->d.K, Np = h->Np, NFF = h->NFF, IP = h->IP;
+  const double *req_d[] = {m->WDr, m->WDs, m->WDt, m->LIFT, m->rx, m->ry, m->rz, m->sx,
+                           m->sy,  m->sz,  m->tx,  m->ty,   m->tz, m->Fscale, m->nx, m->ny,
+                           m->nz};
+  for (const double *p : req_d)
+    if (!p) return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: a real array is NULL");
+  if (!m->vmapP || !m->vmapF || !m->Fmask)
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: an index array is NULL");
+  if (m->matrix_order != 'c' && m->matrix_order != 'f')
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: matrix_order must be 'c' or 'f'");
+  if (h->d.physics == DGLM_ADVECTION && (!m->vx || !m->vy || !m->vz))
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: advection needs vx, vy, vz");
+  // host-side validation of every index array and every real array
+  if (!in_range(m->vmapP, (size_t)K * NFF, 0, K * Np))
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: vmapP entry outside [0, K*Np)");
+  if (!in_range(m->vmapF, (size_t)4 * K, 0, 4 * K))
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: vmapF entry outside [0, 4K)");
+  if (!in_range(m->Fmask, (size_t)NFF, 0, Np))
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: Fmask entry outside [0, Np)");
+  const size_t nop = (size_t)Np * Np, nl = (size_t)Np * NFF;
+  if (!all_finite(m->WDr, nop) || !all_finite(m->WDs, nop) || !all_finite(m->WDt, nop) ||
+      !all_finite(m->LIFT, nl))
+    return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: non-finite operator entry");
+  for (int i = 4; i < 13; i++)
+    if (!all_finite(req_d[i], (size_t)K))
+      return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: non-finite metric");
+  for (int i = 13; i < 17; i++)
+    if (!all_finite(req_d[i], (size_t)4 * K))
+      return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: non-finite face array");
+  if (h->d.physics == DGLM_ADVECTION) {
+    for (const double *p : {m->vx, m->vy, m->vz})
+      if (!all_finite(p, (size_t)K * Np))
+        return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: non-finite velocity");
+  }
+
+  // stacked operators, k-major with padded rows: AT[k][i]
+  const bool cm = m->matrix_order == 'f';
+  std::vector<double> AT((size_t)(3 * Np + NFF) * IP, 0.0);
+  auto at = [&](const double *M, long i, long j, long cols) {
+    return cm ? M[j * Np + i] : M[i * cols + j];
+  };
+  for (long i = 0; i < Np; i++) {
+    for (long j = 0; j < Np; j++) {
+      AT[(size_t)(0 * Np + j) * IP + i] = at(m->WDr, i, j, Np);
+      AT[(size_t)(1 * Np + j) * IP + i] = at(m->WDs, i, j, Np);
+      AT[(size_t)(2 * Np + j) * IP + i] = at(m->WDt, i, j, Np);
+    }
+    for (long j = 0; j < NFF; j++) AT[(size_t)(3 * Np + j) * IP + i] = -at(m->LIFT, i, j, NFF);
+  }
+  std::vector<double> geo((size_t)9 * K), nrm((size_t)12 * K);
+  const double *g9[9] = {m->rx, m->ry, m->rz, m->sx, m->sy, m->sz, m->tx, m->ty, m->tz};
+  for (int q = 0; q < 9; q++) std::memcpy(&geo[(size_t)q * K], g9[q], sizeof(double) * K);
+  std::memcpy(&nrm[0], m->nx, sizeof(double) * 4 * K);
+  std::memcpy(&nrm[(size_t)4 * K], m->ny, sizeof(double) * 4 * K);
+  std::memcpy(&nrm[(size_t)8 * K], m->nz, sizeof(double) * 4 * K);
+
+  DeviceGuard g(h->dev);
+  cudaStreamSynchronize(h->stream);
+  const auto H2D = cudaMemcpyHostToDevice;
+  cudaError_t e = cudaMemcpy(h->AT, AT.data(), sizeof(double) * AT.size(), H2D);
+  if (e == cudaSuccess) e = cudaMemcpy(h->geo, geo.data(), sizeof(double) * geo.size(), H2D);
+  if (e == cudaSuccess) e = cudaMemcpy(h->nrm, nrm.data(), sizeof(double) * nrm.size(), H2D);
+  if (e == cudaSuccess) e = cudaMemcpy(h->fscale, m->Fscale, sizeof(double) * 4 * K, H2D);
+  if (e == cudaSuccess) e = cudaMemcpy(h->vmapP, m->vmapP, sizeof(int) * K * NFF, H2D);
+  if (e == cudaSuccess) e = cudaMemcpy(h->vmapF, m->vmapF, sizeof(int) * 4 * K, H2D);
+  if (e == cudaSuccess) e = cudaMemcpy(h->Fmask, m->Fmask, sizeof(int) * NFF, H2D);
+  if (h->d.physics == DGLM_ADVECTION) {
+    const double *v3[3] = {m->vx, m->vy, m->vz};
+    for (int q = 0; q < 3 && e == cudaSuccess; q++)
+      e = cudaMemcpy(h->vel + (size_t)q * h->vs, v3[q], sizeof(double) * K * Np, H2D);
+  }
+  if (e != cudaSuccess) return cuda_check(e, "dglm_upload_mesh");
+  h->mesh_ready = true;
+  h->state_ready = false;
+  return DGLM_OK;
+}
+
+dglm_status dglm_set_state(dglm_handle *h, const double *const *u, int on_device) {
+  if (!h || !u) return set_error(DGLM_ERR_INVALID, "dglm_set_state: NULL argument");
+  if (!h->mesh_ready) return set_error(DGLM_ERR_STATE, "dglm_set_state: upload the mesh first");
+  const long n = (long)h->d.K * h->Np;
+  for (int v = 0; v < h->nvar; v++)
+    if (!u[v]) return set_error(DGLM_ERR_INVALID, "dglm_set_state: NULL variable pointer");
+  DeviceGuard g(h->dev);
+  cudaStream_t s = h->stream;
+  h->cur = 0;
+  cudaError_t e = cudaSuccess;
+  for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
+    e = cudaMemcpyAsync(h->u[0] + (size_t)v * h->vs, u[v], sizeof(double) * n,
+                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->kreg, 0, sizeof(double) * h->nvar * h->vs, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->sc, 0, sizeof(DevScalars), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dt_hist, 0, sizeof(double) * kHistory, s);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_set_state");
+  e = launch_finite_check(h->u[0], h->vs, n, h->nvar, h->sc, s);
+  StageArgs a = stage_args(h, h->u[0], h->u[1], -1);
+  if (e == cudaSuccess) e = launch_face_maxv(h->d.physics, h->d.N, a, 0, s);
+  if (e == cudaSuccess && h->d.physics == DGLM_ADVECTION)
+    e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv, h->tau, s);
+  int flags = 0;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpy(&flags, &h->sc->flags, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_set_state");
+  if (flags & 2) {
+    h->state_ready = false;
+    return set_error(DGLM_ERR_NONFINITE, "dglm_set_state: non-finite value in the state");
+  }
+  h->state_ready = true;
+  return DGLM_OK;
+}
+
+dglm_status dglm_get_state(dglm_handle *h, double *const *u, int on_device) {
+  if (!h || !u) return set_error(DGLM_ERR_INVALID, "dglm_get_state: NULL argument");
+  if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_get_state: no state set");
+  DeviceGuard g(h->dev);
+  const long n = (long)h->d.K * h->Np;
+  cudaError_t e = cudaSuccess;
+  for (int v = 0; v < h->nvar && e == cudaSuccess; v++) {
+    if (!u[v]) return set_error(DGLM_ERR_INVALID, "dglm_get_state: NULL variable pointer");
+    e = cudaMemcpyAsync(u[v], h->u[h->cur] + (size_t)v * h->vs, sizeof(double) * n,
+                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        h->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return cuda_check(e, "dglm_get_state");
+}
+
+static dglm_status run_steps(dglm_handle *h, int nsteps) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_step: NULL handle");
+  if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_step: set a state first");
+  if (nsteps < 0) return set_error(DGLM_ERR_INVALID, "dglm_step: negative step count");
+  DeviceGuard g(h->dev);
+  for (int i = 0; i < nsteps; i++) {
+    const int c = h->cur;
+    if (!h->graph[c]) {
+      // capture one step from u[c]; fall back to direct launches on failure
+      cudaGraph_t graph = nullptr;
+      cudaStream_t cs = h->stream;
+      bool ok = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      dglm_status st = ok ? issue_step(h, c, cs) : DGLM_OK;
+      ok = (cudaStreamEndCapture(cs, &graph) == cudaSuccess) && ok && st == DGLM_OK;
+      if (ok && cudaGraphInstantiate(&h->graph[c], graph, 0) != cudaSuccess) {
+        h->graph[c] = nullptr;
+        ok = false;
+      }
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      if (!ok) {
+        dglm_status s2 = issue_step(h, c, h->stream);
+        if (s2 != DGLM_OK) return s2;
+        h->launches += h->d.physics == DGLM_ADVECTION ? 7 : 8;
+        h->cur ^= 1;
+        continue;
+      }
+    }
+    cudaError_t e = cudaGraphLaunch(h->graph[c], h->stream);
+    if (e != cudaSuccess) return cuda_check(e, "dglm_step: graph launch");
+    h->launches += h->d.physics == DGLM_ADVECTION ? 7 : 8;
+    h->cur ^= 1;
+  }
+  return DGLM_OK;
+}
+
+dglm_status dglm_step(dglm_handle *h, int nsteps) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_step: NULL handle");
+  DeviceGuard g(h->dev);
+  const double zero = 0.0;
+  cudaError_t e = cudaMemcpyAsync(&h->sc->dt_fixed, &zero, sizeof(double),
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_step");
+  // the pageable source must stay alive until the copy is staged
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_step");
+  h->launches = 0;
+  return run_steps(h, nsteps);
+}
+
+dglm_status dglm_step_fixed_dt(dglm_handle *h, int nsteps, double dt) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_step_fixed_dt: NULL handle");
+  if (!(dt > 0) || !std::isfinite(dt))
+    return set_error(DGLM_ERR_INVALID, "dglm_step_fixed_dt: dt must be positive and finite");
+  DeviceGuard g(h->dev);
+  cudaError_t e = cudaMemcpyAsync(&h->sc->dt_fixed, &dt, sizeof(double),
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_step_fixed_dt");
+  h->launches = 0;
+  return run_steps(h, nsteps);
+}
+
+dglm_status dglm_stage(dglm_handle *h, int stage, double dt) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_stage: NULL handle");
+  if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_stage: set a state first");
+  if (stage < 0 || stage > 4 || !(dt >= 0) || !std::isfinite(dt))
+    return set_error(DGLM_ERR_INVALID, "dglm_stage: stage must be 0..4 and dt >= 0");
+  DeviceGuard g(h->dev);
+  StageArgs a = stage_args(h, h->u[h->cur], h->u[h->cur ^ 1], stage);
+  a.dt_override = dt;
+  cudaError_t e = launch_stage_fp64(h->d.physics, h->d.N, a, h->stream);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_stage");
+  h->cur ^= 1;
+  return DGLM_OK;
+}
+
+dglm_status dglm_sync(dglm_handle *h) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_sync: NULL handle");
+  DeviceGuard g(h->dev);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_sync");
+  int flags = 0;
+  e = cudaMemcpy(&flags, &h->sc->flags, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_sync");
+  if (flags & 3)
+    return set_error(DGLM_ERR_NONFINITE, "non-finite wave speed, dt or state met");
+  return DGLM_OK;
+}
+
+dglm_status dglm_get_time(dglm_handle *h, double *t, double *dt, int *tstep) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_get_time: NULL handle");
+  DeviceGuard g(h->dev);
+  DevScalars s{};
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(&s, h->sc, sizeof(s), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_get_time");
+  if (t) *t = s.t;
+  if (dt) *dt = s.dt;
+  if (tstep) *tstep = s.tstep;
+  return DGLM_OK;
+}
+
+dglm_status dglm_get_dt_history(dglm_handle *h, int first, int count, double *dt_out) {
+  if (!h || !dt_out || first < 0 || count < 0 || count > kHistory)
+    return set_error(DGLM_ERR_INVALID, "dglm_get_dt_history: bad argument");
+  DeviceGuard g(h->dev);
+  std::vector<double> ring(kHistory);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ring.data(), h->dt_hist, sizeof(double) * kHistory, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_get_dt_history");
+  for (int i = 0; i < count; i++) dt_out[i] = ring[(first + i) % kHistory];
+  return DGLM_OK;
+}
+
+dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs) {
+  if (!h || !u || !rhs) return set_error(DGLM_ERR_INVALID, "dglm_rhs: NULL argument");
+  if (!h->mesh_ready) return set_error(DGLM_ERR_STATE, "dglm_rhs: upload the mesh first");
+  DeviceGuard g(h->dev);
+  dglm_status st = DGLM_OK;
+  if (!h->rhs_in) {
+    const long K = h->d.K;
+    st = dalloc(h, &h->rhs_in, (size_t)h->nvar * h->vs);
+    if (st == DGLM_OK) st = dalloc(h, &h->rhs_out, (size_t)h->nvar * h->vs);
+    if (st == DGLM_OK) st = dalloc(h, &h->maxv_s, (size_t)4 * K);
+    if (st == DGLM_OK) st = dalloc(h, &h->tau_s, (size_t)4 * K);
+    if (st == DGLM_OK) st = dalloc(h, &h->sc_s, 1);
+    if (st != DGLM_OK) return st;
+    cudaMemset(h->rhs_in, 0, sizeof(double) * h->nvar * h->vs);
+  }
+  cudaStream_t s = h->stream;
+  const long n = (long)h->d.K * h->Np;
+  cudaError_t e = cudaSuccess;
+  for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
+    e = cudaMemcpyAsync(h->rhs_in + (size_t)v * h->vs, u[v], sizeof(double) * n,
+                        cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->sc_s, 0, sizeof(DevScalars), s);
+  StageArgs a = stage_args(h, h->rhs_in, h->rhs_out, -1);
+  a.maxv = h->maxv_s;
+  a.tau = h->tau_s;
+  a.sc = h->sc_s;
+  a.rhs_only = 1;
+  if (e == cudaSuccess) e = launch_face_maxv(h->d.physics, h->d.N, a, 0, s);
+  if (e == cudaSuccess) e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv_s, h->tau_s, s);
+  if (e == cudaSuccess) e = launch_stage_fp64(h->d.physics, h->d.N, a, s);
+  for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
+    e = cudaMemcpyAsync(rhs[v], h->rhs_out + (size_t)v * h->vs, sizeof(double) * n,
+                        cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return cuda_check(e, "dglm_rhs");
+}
+
+long dglm_kernel_launches(dglm_handle *h) { return h ? h->launches : 0; }
+size_t dglm_device_bytes(dglm_handle *h) { return h ? h->bytes : 0; }
+
+}  // extern "C"

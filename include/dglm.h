@@ -1,0 +1,188 @@
+/*
+ * dglm.h -- C ABI of the B200 (sm_100a) explicit DGLM solver library
+ * (libdglm.so): the right-hand side and 5-stage low-storage Runge-Kutta
+ * step of ExaDGLM for linear advection (nvar = 1) and compressible Euler
+ * (nvar = 5) on one tetrahedral mesh partition.
+ *
+ * The reference has no library interface: its single-GPU solver is a main()
+ * that reads datain/*.bin, loops runRK() and writes dataout/ snapshots
+ * (dim3/src/cuda/euler_nopad_main.cu:4-20), with kernels that take raw
+ * device pointers (dim3/src/cuda/euler_nopad_dglm.cu, euler_nopad_time.cu).
+ * This header is the boundary that replaces it:
+ *
+ *   - a solver handle (dglm_create ... dglm_destroy) that owns the device
+ *     arrays the reference's DataDev owns (euler_nopad_data_dev.cu:9-266)
+ *     and runs its runRK (euler_nopad_time.cu:32-108) as fused kernels;
+ *   - one entry point per reference kernel (calc_maxv, calc_dt, update_tau,
+ *     update_ub, calc_fluxLM, calc_fluxes, update_rhs, lserk_stage) with the
+ *     reference's argument meaning, on caller-owned device arrays.
+ *
+ * Conventions
+ *   - All pointers are plain C pointers; "device" pointers are CUDA device
+ *     addresses of the current device, "host" pointers are CPU memory.
+ *   - Field arrays keep the reference layout: one array per conserved
+ *     variable ("per-variable pointer tables", the reference's p_u), each of
+ *     K*Np doubles with node i of element e at e*Np + i.  Trace arrays (ub,
+ *     fluxLM) hold K*4*Nfp doubles at (e*4 + f)*Nfp + j.
+ *   - Operators WDr/WDs/WDt (Np x Np) and LIFT (Np x 4Nfp) are given with a
+ *     matrix_order flag: 'c' row-major (the CPU datain) or 'f' column-major
+ *     (the GPU datain, dglm_3d_launcher.py:144-147).
+ *   - stream may be NULL (the legacy default stream).
+ *   - Every function returns a dglm_status; dglm_last_error() gives the
+ *     message of the calling thread's last failure.  Nothing prints.
+ */
+#ifndef DGLM_H
+#define DGLM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGLM_ABI_VERSION 1
+
+typedef enum {
+    DGLM_OK = 0,
+    DGLM_ERR_INVALID = 1,      /* bad argument, size or index array */
+    DGLM_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    DGLM_ERR_NONFINITE = 3,    /* NaN/Inf met in the state or in dt */
+    DGLM_ERR_UNSUPPORTED = 4,  /* order / physics / precision not built */
+    DGLM_ERR_STATE = 5,        /* call out of order (e.g. step before mesh) */
+    DGLM_ERR_NOMEM = 6,        /* device allocation failed */
+    DGLM_ERR_IO = 7            /* file read/write failed */
+} dglm_status;
+
+typedef enum { DGLM_ADVECTION = 0, DGLM_EULER = 1 } dglm_physics;
+
+/* Arithmetic of the four operator contractions.  The state, the LSERK
+ * registers, the geometric factors and the face fluxes stay FP64 in every
+ * mode. */
+typedef enum {
+    DGLM_PREC_FP64 = 0,        /* plain method: FP64 throughout */
+    DGLM_PREC_TF32X3 = 1,      /* 3-pass TF32 on tcgen05, FP32 accumulate */
+    DGLM_PREC_BF16X3 = 2       /* split-BF16 (3 products) on tcgen05, FP32 accumulate */
+} dglm_precision;
+
+/* Solver description: the reference's compile-time common.h parameters
+ * (dglm_3d_launcher.py:152-205) as run-time values. */
+typedef struct {
+    int N;             /* polynomial order (NP, NFP follow) */
+    int physics;       /* dglm_physics; NVAR = 1 or 5 */
+    int K;             /* number of elements (datain dim.bin) */
+    int precision;     /* dglm_precision */
+    double cfl;        /* CFL */
+    double gamma;      /* GAMMA (Euler) */
+    double tau_scale;  /* TAU_SCALE */
+    double tmax;       /* TMAX: the last step is clipped to end at tmax */
+    int device;        /* CUDA device ordinal (DEVID); -1 keeps the current */
+} dglm_desc;
+
+/* Mesh and operator arrays (datain/*.bin), all HOST pointers. */
+typedef struct {
+    const double *WDr, *WDs, *WDt;        /* Np x Np */
+    const double *LIFT;                   /* Np x 4Nfp */
+    char matrix_order;                    /* 'c' or 'f' */
+    const double *rx, *ry, *rz, *sx, *sy, *sz, *tx, *ty, *tz;   /* K */
+    const double *Fscale, *nx, *ny, *nz;  /* K*4 */
+    const int *EtoB, *vmapF;              /* K*4 */
+    const int *vmapP;                     /* K*4*Nfp */
+    const int *Fmask;                     /* 4*Nfp */
+    const double *vx, *vy, *vz;           /* K*Np, advection only (NULL for Euler) */
+} dglm_mesh_arrays;
+
+typedef struct dglm_handle dglm_handle;
+
+const char *dglm_last_error(void);
+int dglm_abi_version(void);
+/* 1 when the library was built with kernels for order N, else 0. */
+int dglm_order_supported(int N);
+
+/* --- solver handle (replaces DataHost/DataDev + runRK + main) ------------ */
+dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out);
+dglm_status dglm_destroy(dglm_handle *h);
+dglm_status dglm_set_stream(dglm_handle *h, void *cuda_stream);
+/* Validates every index array on the host (0 <= vmapP < K*Np, 0 <= vmapF <
+ * 4K, 0 <= Fmask < Np) and all real arrays for NaN/Inf, then uploads. */
+dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *mesh);
+/* u: nvar pointers to K*Np doubles (host or device per on_device).  Resets
+ * t, tstep and the RK register k to zero and computes the face wave speeds
+ * of the new state.  The uploaded state is checked for NaN/Inf on the
+ * device (DGLM_ERR_NONFINITE).  Synchronises the handle's stream. */
+dglm_status dglm_set_state(dglm_handle *h, const double *const *u, int on_device);
+dglm_status dglm_get_state(dglm_handle *h, double *const *u, int on_device);
+/* Advances nsteps LSERK steps (runRK) on the handle's stream without host
+ * synchronisation; dt is computed on the device from the CFL condition and
+ * clipped at tmax; steps requested after t reaches tmax change nothing. */
+dglm_status dglm_step(dglm_handle *h, int nsteps);
+/* Same with a prescribed dt (dt > 0) instead of the CFL dt. */
+dglm_status dglm_step_fixed_dt(dglm_handle *h, int nsteps, double dt);
+/* One LSERK stage (0..4) of the current state with a prescribed dt and the
+ * handle's current tau, without the per-step dt/tau work (for timing the
+ * stage kernel on its own).  Asynchronous. */
+dglm_status dglm_stage(dglm_handle *h, int stage, double dt);
+/* Synchronises the stream and reports a device-side non-finite flag. */
+dglm_status dglm_sync(dglm_handle *h);
+/* Time, last dt and step counter (synchronises). */
+dglm_status dglm_get_time(dglm_handle *h, double *t, double *dt, int *tstep);
+/* dt of steps [first, first+count) taken since dglm_set_state (synchronises);
+ * the history keeps the most recent 65536 steps. */
+dglm_status dglm_get_dt_history(dglm_handle *h, int first, int count, double *dt_out);
+/* One right-hand side on device state u (nvar device pointers) into rhs
+ * (nvar device pointers), with maxv/tau taken from u as runRK does at the
+ * start of a step. */
+dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs);
+/* Number of kernels the last dglm_step call launched (for accounting). */
+long dglm_kernel_launches(dglm_handle *h);
+/* Device bytes held by the handle. */
+size_t dglm_device_bytes(dglm_handle *h);
+
+/* --- per-kernel entry points (reference kernels, caller-owned device arrays)
+ * Shapes as in the reference; nvar pointer tables are HOST arrays of device
+ * pointers.  N selects NP/NFP.  Each launches on `stream`. */
+
+/* euler_nopad_dglm.cu:7-76 / advec_nopad_dglm.cu:7-62.  u: nvar device
+ * pointers (Euler) or NULL with vx,vy,vz (advection). */
+dglm_status dglm_calc_maxv(int physics, int N, int nelem, double gamma, const int *Fmask,
+                           const double *Fscale, const double *const *u, const double *vx,
+                           const double *vy, const double *vz, double *maxv, double *maxv_fs,
+                           void *stream);
+/* euler_nopad_dglm.cu:79-96, on the device: dt = cfl/(2N+1)/max(maxv_fs),
+ * written to *dt_dev (device) -- no host round trip. */
+dglm_status dglm_calc_dt(int N, int nelem, double cfl, const double *maxv_fs, double *dt_dev,
+                         void *stream);
+/* euler_nopad_dglm.cu:99-112 */
+dglm_status dglm_update_tau(int nelem, double tau_scale, const int *vmapF, const double *maxv,
+                            double *tau, void *stream);
+/* euler_nopad_dglm.cu:115-135 */
+dglm_status dglm_update_ub(int N, int nvar, int nelem, const int *Fmask, const int *vmapP,
+                           const double *const *u, double *const *ub, void *stream);
+/* euler_nopad_dglm.cu:138-210 / advec_nopad_dglm.cu:120-165 */
+dglm_status dglm_calc_fluxLM(int physics, int N, int nelem, double gamma, const int *Fmask,
+                             const double *nx, const double *ny, const double *nz,
+                             const double *tau, const double *Fscale, const double *vx,
+                             const double *vy, const double *vz, const double *const *ub,
+                             const double *const *u, double *const *fluxLM, void *stream);
+/* euler_nopad_dglm.cu:213-266 / advec_nopad_dglm.cu:168-189.  geo: 9 device
+ * pointers rx, ry, rz, sx, sy, sz, tx, ty, tz. */
+dglm_status dglm_calc_fluxes(int physics, int N, int nelem, double gamma,
+                             const double *const *geo, const double *vx, const double *vy,
+                             const double *vz, const double *const *u, double *const *fluxR,
+                             double *const *fluxS, double *const *fluxT, void *stream);
+/* euler_nopad_dglm.cu:269-300 (the four cuBLAS GEMMs) as one kernel:
+ * utmp = WDr fluxR + WDs fluxS + WDt fluxT - LIFT fluxLM per variable. */
+dglm_status dglm_update_rhs(int N, int nvar, int nelem, const double *WDr, const double *WDs,
+                            const double *WDt, const double *LIFT, char matrix_order,
+                            const double *const *fluxR, const double *const *fluxS,
+                            const double *const *fluxT, const double *const *fluxLM,
+                            double *const *utmp, void *stream);
+/* euler_nopad_time.cu:15-29 */
+dglm_status dglm_lserk_stage(int N, int nvar, int nelem, double dt, double rka, double rkb,
+                             const double *const *utmp, double *const *k, double *const *u,
+                             void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGLM_H */

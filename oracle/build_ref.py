@@ -1,0 +1,130 @@
+"""Build recipe for ``oracle/_ref/``: the reference's own code, compiled from
+its sources where they lie under /root/reference (nothing is copied).
+
+Products (all git-ignored, they travel with the working tree):
+
+* ``_ref/libref_{euler,advec}_N{n}.so`` -- the reference CPU single-partition
+  solver (dim3/src/cpp/{euler,advec}_{data,dglm,time}.cpp, plus
+  utils/src/cpp/io.cpp), compiled the way its launcher does
+  (dglm_3d_launcher.py:392: ``g++ -O3 -std=c++11 -fopenmp``; ``-march`` is
+  pinned to x86-64-v3 instead of ``native`` so the library also runs on the
+  host of another machine), with the generated ``common.h`` written here.
+  ``ref_driver.cpp`` wraps its ``runRK`` in a fixed-step C entry point.
+  ``CFL``, ``GAMMA``, ``TAU_SCALE`` and ``TMAX`` become run-time globals so
+  one build serves every configuration of an order N; ``N``, ``NP``, ``NFP``,
+  ``NVAR`` stay compile-time as in the reference.
+* ``_ref/mesh_3d_cpp*.so``, ``_ref/uniform_3d_single_cpp*.so`` -- the
+  reference's pybind11 mesh cores rebuilt from dim3/src/cpp (used only to
+  generate golden fixtures in a container that holds the reference).
+
+Usage: ``python oracle/build_ref.py [--orders 1-6]``.  Exits quietly with a
+message when the reference tree is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+import sysconfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+REF = os.environ.get("DGLM_REFERENCE_ROOT", "/root/reference")
+CXXFLAGS = ["-O3", "-std=c++11", "-fopenmp", "-march=x86-64-v3", "-shared", "-fPIC"]
+
+COMMON_H = """#ifndef COMMON_H
+#define COMMON_H
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <fstream>
+#include <iostream>
+extern double ref_cfl, ref_gamma, ref_tau_scale, ref_tmax;
+extern std::string ref_datain, ref_dataout;
+#define REAL    double
+#define DATAIN  ref_datain
+#define DATAOUT ref_dataout
+#define PI     3.14159265358979323846
+#define TDIGIT 7
+#define N      {N}
+#define NP     {NP}
+#define NFP    {NFP}
+#define NFACE  4
+#define NROT   3
+#define NVAR   {NVAR}
+#define TMAX   ref_tmax
+#define CFL    ref_cfl
+#define GAMMA  ref_gamma
+#define TAU_SCALE ref_tau_scale
+#include "{REF}/utils/src/cpp/io.cpp"
+#include "{REF}/dim3/src/cpp/{P}_data.cpp"
+#include "{REF}/dim3/src/cpp/{P}_dglm.cpp"
+#include "{REF}/dim3/src/cpp/{P}_time.cpp"
+#endif
+"""
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(" ".join(cmd) + "\n" + r.stdout)
+
+
+def build_solver(phys: str, N: int, force=False) -> str:
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    Nfp = (N + 1) * (N + 2) // 2
+    nvar = 5 if phys == "euler" else 1
+    bdir = os.path.join(OUT, f"build_{phys}_N{N}")
+    os.makedirs(bdir, exist_ok=True)
+    so = os.path.join(OUT, f"libref_{phys}_N{N}.so")
+    drv = os.path.join(HERE, "ref_driver.cpp")
+    if not force and os.path.exists(so) and os.path.getmtime(so) > os.path.getmtime(drv):
+        return so
+    with open(os.path.join(bdir, "common.h"), "w") as f:
+        f.write(COMMON_H.format(N=N, NP=Np, NFP=Nfp, NVAR=nvar, REF=REF, P=phys))
+    flag = "-DREF_EULER" if phys == "euler" else "-DREF_ADVEC"
+    _run(["g++", *CXXFLAGS, flag, "-I", bdir, drv, "-o", so])
+    return so
+
+
+def build_mesh_cores() -> None:
+    import pybind11
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    inc = ["-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"]]
+    for name, src in (("mesh_3d_cpp", "mesh_3d_core.cpp"),
+                      ("uniform_3d_single_cpp", "uniform_3d_single_core.cpp")):
+        out = os.path.join(OUT, name + suffix)
+        if os.path.exists(out):
+            continue
+        _run(["g++", "-O3", "-shared", "-std=c++17", "-fPIC", *inc,
+              os.path.join(REF, "dim3/src/cpp", src), "-o", out])
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--orders", default="1-6")
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--no-mesh", action="store_true")
+    a = ap.parse_args(argv)
+    if not os.path.isdir(os.path.join(REF, "dim3/src/cpp")):
+        print(f"reference tree not found at {REF}; oracle/_ref not built")
+        return 0
+    lo, _, hi = a.orders.partition("-")
+    orders = range(int(lo), int(hi or lo) + 1)
+    os.makedirs(OUT, exist_ok=True)
+    for phys in ("euler", "advec"):
+        for N in orders:
+            build_solver(phys, N, force=a.force)
+    if not a.no_mesh:
+        try:
+            build_mesh_cores()
+        except Exception as e:          # pybind11 headers missing: fixtures only
+            print("mesh cores not built:", e)
+    print("oracle/_ref built:", sorted(os.listdir(OUT)))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
