@@ -20,6 +20,8 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OBJDIR = os.path.join(ROOT, "_build", "obj")
 LIB = os.path.join(PKG, "libdglm.so")
+MAIN_SRC = os.path.join(CSRC, "host", "dglm_main.cpp")
+MAIN = os.path.join(PKG, "dglm_main")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
@@ -75,6 +77,14 @@ def build(force=False, jobs=None, verbose=False):
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout)
         os.replace(tmp, LIB)
+    if force or not os.path.exists(MAIN) or \
+            os.path.getmtime(MAIN) < max(os.path.getmtime(LIB), os.path.getmtime(MAIN_SRC)):
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, MAIN_SRC, "-o", MAIN + ".tmp",
+               "-L", PKG, "-ldglm", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("dglm_main build failed:\n" + r.stdout)
+        os.replace(MAIN + ".tmp", MAIN)
     return LIB
 
 

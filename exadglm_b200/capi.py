@@ -24,7 +24,8 @@ EXPORTS = (
     "dglm_step", "dglm_step_fixed_dt", "dglm_stage", "dglm_sync", "dglm_get_time", "dglm_get_dt_history",
     "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
-    "dglm_update_rhs", "dglm_lserk_stage",
+    "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
+    "dglm_set_variant", "dglm_get_variant",
 )
 
 
@@ -76,6 +77,9 @@ def lib():
                                     C.POINTER(C.c_int)]
         L.dglm_get_dt_history.argtypes = [_P, C.c_int, C.c_int, _P]
         L.dglm_rhs.argtypes = [_P, _P, _P]
+        L.dglm_variant_describe.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
+        L.dglm_set_variant.argtypes = [_P, C.c_int]
+        L.dglm_get_variant.argtypes = [_P]
         L.dglm_kernel_launches.argtypes = [_P]
         L.dglm_kernel_launches.restype = C.c_long
         L.dglm_device_bytes.argtypes = [_P]
@@ -104,6 +108,18 @@ def ptr_table(ptrs):
     the C ABI expect."""
     arr = (C.c_void_p * len(ptrs))(*[C.c_void_p(int(p)) for p in ptrs])
     return arr
+
+
+def variants(physics, N):
+    """Descriptions of the compiled stage-kernel variants for (physics, N)."""
+    L = lib()
+    ph = EULER if physics == "euler" else ADVECTION
+    out = []
+    for i in range(L.dglm_variant_count(ph, N)):
+        buf = C.create_string_buffer(128)
+        check(L.dglm_variant_describe(ph, N, i, buf, 128))
+        out.append(buf.value.decode())
+    return out
 
 
 def _np_ptr(a):
@@ -208,6 +224,12 @@ class Solver:
 
     def set_stream(self, stream_ptr):
         check(self.L.dglm_set_stream(self.h, C.c_void_p(int(stream_ptr))))
+
+    def set_variant(self, v):
+        check(self.L.dglm_set_variant(self.h, int(v)))
+
+    def variant(self):
+        return int(self.L.dglm_get_variant(self.h))
 
     def kernel_launches(self):
         return int(self.L.dglm_kernel_launches(self.h))

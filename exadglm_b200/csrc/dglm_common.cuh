@@ -47,6 +47,8 @@ struct StageArgs {
   double *maxv;          // K*4 (written on the last stage)
   DevScalars *sc;
   long vs;
+  long gstride;          // elements between the 9 metric arrays and the 3
+                         // normal components (K rounded up to 64)
   int K;
   double gamma;
   double rka, rkb;
@@ -98,10 +100,29 @@ __device__ __forceinline__ unsigned long long warp_max_bits(unsigned long long b
 dglm_status set_error(dglm_status s, const std::string &msg);
 dglm_status cuda_check(cudaError_t e, const char *what);
 
+// contraction engines of the fused stage kernel
+enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2 };
+
+// One compiled tile shape of the fused stage kernel.
+struct StageVariantInfo {
+  int mode;      // MODE_SIMT, MODE_DMMA or MODE_PIPE (persistent, TMA-fed DMMA)
+  int E;         // elements per CTA
+  int R;         // SIMT rows per thread (8 = one m-tile for DMMA)
+  int CPT;       // SIMT columns per thread / DMMA n-tiles per warp
+  int WM;        // DMMA m-tiles per warp
+  int IP;        // SIMT: padded rows of the k-major operator copy
+  int MT;        // DMMA: m-tiles (8 rows each)
+  int KVP, KFP;  // DMMA: volume / lift k extents padded to 4
+  int threads;
+  size_t smem;
+};
+
 // fused FP64 stage launcher (dglm_stage_fp64.cu)
 bool stage_fp64_supported(int physics, int N);
-int stage_rows_padded(int physics, int N);  // IP: padded row count of AT
-cudaError_t launch_stage_fp64(int physics, int N, const StageArgs &a, cudaStream_t s);
+int stage_variant_count(int physics, int N);
+bool stage_variant_info(int physics, int N, int idx, StageVariantInfo *out);
+cudaError_t launch_stage_fp64(int physics, int N, int variant, const StageArgs &a,
+                              cudaStream_t s);
 cudaError_t launch_face_maxv(int physics, int N, const StageArgs &a, int parity_slot,
                              cudaStream_t s);
 cudaError_t launch_step_begin(int N, double cfl, double tmax, int frozen, DevScalars *sc,

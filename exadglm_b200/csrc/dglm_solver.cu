@@ -5,7 +5,9 @@
 // with no host synchronisation inside a step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -32,8 +34,12 @@ using namespace dglm;
 
 struct dglm_handle {
   dglm_desc d{};
-  int nvar = 0, Np = 0, Nfp = 0, NFF = 0, IP = 0;
+  int nvar = 0, Np = 0, Nfp = 0, NFF = 0;
+  int variant = 0;
+  StageVariantInfo vinfo{};
+  std::vector<double> Ahost;      // stacked [WDr WDs WDt -LIFT], Np x (3Np+NFF) row-major
   long vs = 0;                    // doubles between variables of a field
+  long Kp = 0;                    // K rounded up to a multiple of 64 (tile padding)
   int dev = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -129,6 +135,7 @@ StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
   a.maxv = h->maxv;
   a.sc = h->sc;
   a.vs = h->vs;
+  a.gstride = h->Kp;
   a.K = h->d.K;
   a.gamma = h->d.gamma;
   a.rka = s >= 0 ? RKA[s] : 0.0;
@@ -137,6 +144,58 @@ StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
   a.rhs_only = 0;
   a.dt_override = -1.0;
   return a;
+}
+
+// Doubles of the device operator copy for a variant's layout.
+size_t op_doubles(const StageVariantInfo &v, int Np, int NFF) {
+  if (v.mode == MODE_SIMT) return (size_t)(3 * Np + NFF) * v.IP;
+  return (size_t)(v.KVP / 4 + v.KFP / 4) * v.MT * 32;
+}
+
+size_t max_op_doubles(int physics, int N, int Np, int NFF) {
+  size_t m = 0;
+  StageVariantInfo v{};
+  for (int i = 0; i < stage_variant_count(physics, N); i++)
+    if (stage_variant_info(physics, N, i, &v)) m = std::max(m, op_doubles(v, Np, NFF));
+  return m;
+}
+
+// Builds the variant's device layout of A = [WDr WDs WDt -LIFT] (Np rows,
+// 3Np + NFF columns) from the host copy and uploads it.
+//   SIMT: k-major with padded rows, AT[k * IP + i] = A(i, k);
+//   DMMA: m8n8k4 A fragments, [kstep][mtile][lane] with row = 8*mtile +
+//         lane/4 and column 4*kstep + lane%4 inside the volume block
+//         (ksteps [0, KVP/4)) or the lift block (ksteps [KVP/4, ...)).
+dglm_status upload_operator_layout(dglm_handle *h) {
+  const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
+  const StageVariantInfo &v = h->vinfo;
+  std::vector<double> out(op_doubles(v, Np, NFF), 0.0);
+  auto A = [&](int i, int k) { return h->Ahost[(size_t)i * KA + k]; };
+  if (v.mode == MODE_SIMT) {
+    for (int k = 0; k < KA; k++)
+      for (int i = 0; i < Np; i++) out[(size_t)k * v.IP + i] = A(i, k);
+  } else {
+    const int kv4 = v.KVP / 4, kf4 = v.KFP / 4;
+    for (int ks = 0; ks < kv4 + kf4; ks++)
+      for (int mt = 0; mt < v.MT; mt++)
+        for (int lane = 0; lane < 32; lane++) {
+          const int row = mt * 8 + lane / 4;
+          int k;
+          bool ok;
+          if (ks < kv4) {
+            k = ks * 4 + lane % 4;
+            ok = k < KV;
+          } else {
+            const int kk = (ks - kv4) * 4 + lane % 4;
+            k = KV + kk;
+            ok = kk < NFF;
+          }
+          if (ok && row < Np) out[((size_t)ks * v.MT + mt) * 32 + lane] = A(row, k);
+        }
+  }
+  return cuda_check(cudaMemcpy(h->AT, out.data(), sizeof(double) * out.size(),
+                               cudaMemcpyHostToDevice),
+                    "operator upload");
 }
 
 // Issues one LSERK step starting from u[cur] (ends in u[cur^1]).
@@ -148,7 +207,7 @@ dglm_status issue_step(dglm_handle *h, int cur, cudaStream_t s) {
   for (int st = 0; st < 5 && e == cudaSuccess; st++) {
     const int in = (cur + st) & 1;
     StageArgs a = stage_args(h, h->u[in], h->u[in ^ 1], st);
-    e = launch_stage_fp64(h->d.physics, h->d.N, a, s);
+    e = launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, s);
   }
   if (e == cudaSuccess) e = launch_step_end(h->sc, s);
   return cuda_check(e, "step launch");
@@ -190,21 +249,25 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   h->Np = np_of(d.N);
   h->Nfp = nfp_of(d.N);
   h->NFF = 4 * h->Nfp;
-  h->IP = stage_rows_padded(d.physics, d.N);
-  const long n = (long)d.K * h->Np;
+  h->variant = 0;
+  stage_variant_info(d.physics, d.N, 0, &h->vinfo);
+  // per-element arrays are padded to whole 64-element tiles (zero-filled) so
+  // that every tile copy of the pipelined kernel is in bounds and aligned
+  h->Kp = ((long)d.K + 63) / 64 * 64;
+  const long n = h->Kp * h->Np;
   h->vs = (n + 31) / 32 * 32;  // 256-byte aligned variable blocks
   dglm_status st = DGLM_OK;
-  const long K = d.K;
+  const long K = h->Kp;
   auto chk = [&](dglm_status s) {
     if (st == DGLM_OK) st = s;
   };
-  chk(dalloc(h, &h->AT, (size_t)(3 * h->Np + h->NFF) * h->IP));
+  chk(dalloc(h, &h->AT, max_op_doubles(d.physics, d.N, h->Np, h->NFF)));
   chk(dalloc(h, &h->geo, (size_t)9 * K));
   chk(dalloc(h, &h->fscale, (size_t)4 * K));
   chk(dalloc(h, &h->nrm, (size_t)12 * K));
   chk(dalloc(h, &h->tau, (size_t)4 * K));
   chk(dalloc(h, &h->maxv, (size_t)4 * K));
-  chk(dalloc(h, &h->vmapP, (size_t)K * h->NFF));
+  chk(dalloc(h, &h->vmapP, (size_t)d.K * h->NFF));
   chk(dalloc(h, &h->vmapF, (size_t)4 * K));
   chk(dalloc(h, &h->Fmask, (size_t)h->NFF));
   if (d.physics == DGLM_ADVECTION) chk(dalloc(h, &h->vel, (size_t)3 * h->vs));
@@ -227,7 +290,10 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   // zero-padded tails stay zero for the whole life of the handle
   for (void *p : {(void *)h->u[0], (void *)h->u[1], (void *)h->kreg})
     cudaMemset(p, 0, sizeof(double) * h->nvar * h->vs);
-  cudaMemset(h->AT, 0, sizeof(double) * (3 * h->Np + h->NFF) * h->IP);
+  cudaMemset(h->geo, 0, sizeof(double) * 9 * K);
+  cudaMemset(h->nrm, 0, sizeof(double) * 12 * K);
+  for (double *p : {h->fscale, h->tau, h->maxv}) cudaMemset(p, 0, sizeof(double) * 4 * K);
+  if (h->vel) cudaMemset(h->vel, 0, sizeof(double) * 3 * h->vs);
   *out = h;
   return cuda_check(cudaDeviceSynchronize(), "dglm_create");
 }
@@ -256,7 +322,7 @@ dglm_status dglm_set_stream(dglm_handle *h, void *stream) {
 
 dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *m) {
   if (!h || !m) return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: NULL argument");
-  const long K = h->d.K, Np = h->Np, NFF = h->NFF, IP = h->IP;
+  const long K = h->d.K, Np = h->Np, NFF = h->NFF;
   const double *req_d[] = {m->WDr, m->WDs, m->WDt, m->LIFT, m->rx, m->ry, m->rz, m->sx,
                            m->sy,  m->sz,  m->tx,  m->ty,   m->tz, m->Fscale, m->nx, m->ny,
                            m->nz};
@@ -291,32 +357,35 @@ dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *m) {
         return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: non-finite velocity");
   }
 
-  // stacked operators, k-major with padded rows: AT[k][i]
+  // stacked operator A = [WDr WDs WDt -LIFT], row-major
   const bool cm = m->matrix_order == 'f';
-  std::vector<double> AT((size_t)(3 * Np + NFF) * IP, 0.0);
+  const long KA = 3 * Np + NFF;
+  h->Ahost.assign((size_t)Np * KA, 0.0);
   auto at = [&](const double *M, long i, long j, long cols) {
     return cm ? M[j * Np + i] : M[i * cols + j];
   };
   for (long i = 0; i < Np; i++) {
     for (long j = 0; j < Np; j++) {
-      AT[(size_t)(0 * Np + j) * IP + i] = at(m->WDr, i, j, Np);
-      AT[(size_t)(1 * Np + j) * IP + i] = at(m->WDs, i, j, Np);
-      AT[(size_t)(2 * Np + j) * IP + i] = at(m->WDt, i, j, Np);
+      h->Ahost[i * KA + j] = at(m->WDr, i, j, Np);
+      h->Ahost[i * KA + Np + j] = at(m->WDs, i, j, Np);
+      h->Ahost[i * KA + 2 * Np + j] = at(m->WDt, i, j, Np);
     }
-    for (long j = 0; j < NFF; j++) AT[(size_t)(3 * Np + j) * IP + i] = -at(m->LIFT, i, j, NFF);
+    for (long j = 0; j < NFF; j++) h->Ahost[i * KA + 3 * Np + j] = -at(m->LIFT, i, j, NFF);
   }
-  std::vector<double> geo((size_t)9 * K), nrm((size_t)12 * K);
+  const long Kp = h->Kp;
+  std::vector<double> geo((size_t)9 * Kp, 0.0), nrm((size_t)12 * Kp, 0.0);
   const double *g9[9] = {m->rx, m->ry, m->rz, m->sx, m->sy, m->sz, m->tx, m->ty, m->tz};
-  for (int q = 0; q < 9; q++) std::memcpy(&geo[(size_t)q * K], g9[q], sizeof(double) * K);
+  for (int q = 0; q < 9; q++) std::memcpy(&geo[(size_t)q * Kp], g9[q], sizeof(double) * K);
   std::memcpy(&nrm[0], m->nx, sizeof(double) * 4 * K);
-  std::memcpy(&nrm[(size_t)4 * K], m->ny, sizeof(double) * 4 * K);
-  std::memcpy(&nrm[(size_t)8 * K], m->nz, sizeof(double) * 4 * K);
+  std::memcpy(&nrm[(size_t)4 * Kp], m->ny, sizeof(double) * 4 * K);
+  std::memcpy(&nrm[(size_t)8 * Kp], m->nz, sizeof(double) * 4 * K);
 
   DeviceGuard g(h->dev);
   cudaStreamSynchronize(h->stream);
   const auto H2D = cudaMemcpyHostToDevice;
-  cudaError_t e = cudaMemcpy(h->AT, AT.data(), sizeof(double) * AT.size(), H2D);
-  if (e == cudaSuccess) e = cudaMemcpy(h->geo, geo.data(), sizeof(double) * geo.size(), H2D);
+  dglm_status os = upload_operator_layout(h);
+  if (os != DGLM_OK) return os;
+  cudaError_t e = cudaMemcpy(h->geo, geo.data(), sizeof(double) * geo.size(), H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->nrm, nrm.data(), sizeof(double) * nrm.size(), H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->fscale, m->Fscale, sizeof(double) * 4 * K, H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->vmapP, m->vmapP, sizeof(int) * K * NFF, H2D);
@@ -454,7 +523,7 @@ dglm_status dglm_stage(dglm_handle *h, int stage, double dt) {
   DeviceGuard g(h->dev);
   StageArgs a = stage_args(h, h->u[h->cur], h->u[h->cur ^ 1], stage);
   a.dt_override = dt;
-  cudaError_t e = launch_stage_fp64(h->d.physics, h->d.N, a, h->stream);
+  cudaError_t e = launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, h->stream);
   if (e != cudaSuccess) return cuda_check(e, "dglm_stage");
   h->cur ^= 1;
   return DGLM_OK;
@@ -508,11 +577,13 @@ dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs)
     const long K = h->d.K;
     st = dalloc(h, &h->rhs_in, (size_t)h->nvar * h->vs);
     if (st == DGLM_OK) st = dalloc(h, &h->rhs_out, (size_t)h->nvar * h->vs);
-    if (st == DGLM_OK) st = dalloc(h, &h->maxv_s, (size_t)4 * K);
-    if (st == DGLM_OK) st = dalloc(h, &h->tau_s, (size_t)4 * K);
+    if (st == DGLM_OK) st = dalloc(h, &h->maxv_s, (size_t)4 * h->Kp);
+    if (st == DGLM_OK) st = dalloc(h, &h->tau_s, (size_t)4 * h->Kp);
     if (st == DGLM_OK) st = dalloc(h, &h->sc_s, 1);
     if (st != DGLM_OK) return st;
     cudaMemset(h->rhs_in, 0, sizeof(double) * h->nvar * h->vs);
+    cudaMemset(h->maxv_s, 0, sizeof(double) * 4 * h->Kp);
+    cudaMemset(h->tau_s, 0, sizeof(double) * 4 * h->Kp);
   }
   cudaStream_t s = h->stream;
   const long n = (long)h->d.K * h->Np;
@@ -528,13 +599,44 @@ dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs)
   a.rhs_only = 1;
   if (e == cudaSuccess) e = launch_face_maxv(h->d.physics, h->d.N, a, 0, s);
   if (e == cudaSuccess) e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv_s, h->tau_s, s);
-  if (e == cudaSuccess) e = launch_stage_fp64(h->d.physics, h->d.N, a, s);
+  if (e == cudaSuccess) e = launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, s);
   for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
     e = cudaMemcpyAsync(rhs[v], h->rhs_out + (size_t)v * h->vs, sizeof(double) * n,
                         cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return cuda_check(e, "dglm_rhs");
 }
+
+int dglm_variant_count(int physics, int N) { return stage_variant_count(physics, N); }
+
+dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, size_t len) {
+  StageVariantInfo v{};
+  if (!buf || len == 0 || !stage_variant_info(physics, N, variant, &v))
+    return set_error(DGLM_ERR_INVALID, "dglm_variant_describe: no such variant");
+  if (v.mode == MODE_SIMT)
+    snprintf(buf, len, "simt E=%d R=%d CPT=%d threads=%d smem=%zu", v.E, v.R, v.CPT, v.threads,
+             v.smem);
+  else
+    snprintf(buf, len, "dmma E=%d WN=%d WM=%d threads=%d smem=%zu", v.E, v.CPT, v.WM,
+             v.threads, v.smem);
+  return DGLM_OK;
+}
+
+dglm_status dglm_set_variant(dglm_handle *h, int variant) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_set_variant: NULL handle");
+  StageVariantInfo v{};
+  if (!stage_variant_info(h->d.physics, h->d.N, variant, &v))
+    return set_error(DGLM_ERR_INVALID, "dglm_set_variant: no such variant");
+  DeviceGuard g(h->dev);
+  cudaStreamSynchronize(h->stream);
+  drop_graphs(h);
+  h->variant = variant;
+  h->vinfo = v;
+  if (h->mesh_ready) return upload_operator_layout(h);
+  return DGLM_OK;
+}
+
+int dglm_get_variant(dglm_handle *h) { return h ? h->variant : -1; }
 
 long dglm_kernel_launches(dglm_handle *h) { return h ? h->launches : 0; }
 size_t dglm_device_bytes(dglm_handle *h) { return h ? h->bytes : 0; }

@@ -6,14 +6,12 @@
 // four batched cuBLAS DGEMMs build utmp, lserk_stage updates k and u.  Here a
 // CTA owns a tile of E elements and does all of it on chip:
 //
-//   0. the tile's state u (all variables) is staged in shared memory with
-//      coalesced loads;
+//   0. the tile's state u (all variables), its metrics, face data and vmapP
+//      are staged in shared memory with coalesced loads;
 //   1. volume fluxes F, G, W at every node, combined with the element's affine
 //      metrics into fluxR/S/T (calc_fluxes, euler_dglm.cpp:186-251), go to a
-//      shared "column" buffer B with one column per (variable, element);
-//   2. acc += [WDr WDs WDt] * [fluxR; fluxS; fluxT]: a register-tiled FP64
-//      contraction, R output rows x CPT columns per thread, operators read
-//      through L1 from a k-major stacked copy;
+//      shared column buffer B, one column per (variable, element);
+//   2. acc += [WDr WDs WDt] * [fluxR; fluxS; fluxT];
 //   3. the trace average ub = (u- + u+)/2 (update_ub, euler_dglm.cpp:87-107)
 //      with u+ gathered through vmapP, and the face flux
 //      (n.F(ub) - tau (ub - u-)) Fscale (calc_fluxLM, :110-183) replace B;
@@ -23,9 +21,21 @@
 //      per-face wave speed of the new state (calc_maxv, euler_dglm.cpp:6-50)
 //      and a device-wide max of maxv*Fscale for the next dt are fused in.
 //
+// Two contraction engines share this skeleton:
+//   SIMT  register-tiled DFMA, R rows x CPT columns per thread, operators in
+//         a k-major stacked copy read through L1;
+//   DMMA  FP64 tensor-core mma.sync.m8n8k4, operators pre-swizzled into A
+//         fragments (one coalesced 256-byte load per fragment), B fragments
+//         from shared memory, 8x8 accumulators in registers.
+//
 // u is ping-ponged between two buffers (u_in -> u_out) because neighbouring
 // tiles read u_in's face values while this tile writes its update.
+//
+// Shared layouts put the element index fastest ([..][e], row stride E+1)
+// so that every phase's per-lane accesses are consecutive or odd-strided.
 #include <cuda_runtime.h>
+
+#include <vector>
 
 #include "dglm_common.cuh"
 
@@ -33,198 +43,309 @@ namespace dglm {
 
 enum { ADV = 0, EUL = 1 };
 
-// Tile shape per (physics, N): E elements per CTA, R output rows per thread,
-// CPT columns per thread (Euler: the 5 variables of one element; advection:
-// CPT elements of the single variable).
-template <int PHYS, int N>
-struct Tile;
+// Euler flux with one reciprocal per node: v = m / rho, p = (gamma-1)(E -
+// m.v/2), H = E + p.  The reference's per-term divisions
+// (euler_dglm.cpp:152-168) agree with it to rounding.
+__device__ __forceinline__ void euler_flux_fast(double g, const double q[5], double F[5],
+                                                double G[5], double W[5]) {
+  const double ir = 1.0 / q[0];
+  const double vx = q[1] * ir, vy = q[2] * ir, vz = q[3] * ir;
+  const double p = (g - 1) * (q[4] - 0.5 * (q[1] * vx + q[2] * vy + q[3] * vz));
+  const double H = q[4] + p;
+  F[0] = q[1]; F[1] = q[1] * vx + p; F[2] = q[2] * vx; F[3] = q[3] * vx; F[4] = H * vx;
+  G[0] = q[2]; G[1] = q[1] * vy; G[2] = q[2] * vy + p; G[3] = q[3] * vy; G[4] = H * vy;
+  W[0] = q[3]; W[1] = q[1] * vz; W[2] = q[2] * vz; W[3] = q[3] * vz + p; W[4] = H * vz;
+}
 
-#define DGLM_TILE(P, NN, EE, RR, CC)             \
-  template <>                                    \
-  struct Tile<P, NN> {                           \
-    static constexpr int E = EE, R = RR, CPT = CC; \
-  };
-DGLM_TILE(EUL, 1, 128, 4, 5)
-DGLM_TILE(EUL, 2, 64, 5, 5)
-DGLM_TILE(EUL, 3, 32, 5, 5)
-DGLM_TILE(EUL, 4, 16, 5, 5)
-DGLM_TILE(EUL, 5, 8, 7, 5)
-DGLM_TILE(EUL, 6, 8, 7, 5)
-DGLM_TILE(EUL, 7, 4, 8, 5)
-DGLM_TILE(EUL, 8, 4, 8, 5)
-DGLM_TILE(ADV, 1, 256, 4, 4)
-DGLM_TILE(ADV, 2, 128, 5, 4)
-DGLM_TILE(ADV, 3, 64, 5, 4)
-DGLM_TILE(ADV, 4, 64, 5, 4)
-DGLM_TILE(ADV, 5, 32, 7, 4)
-DGLM_TILE(ADV, 6, 32, 7, 4)
-DGLM_TILE(ADV, 7, 16, 8, 4)
-DGLM_TILE(ADV, 8, 16, 8, 4)
-#undef DGLM_TILE
+// ---------------------------------------------------------------------------
+// configuration
+// ---------------------------------------------------------------------------
 
-template <int PHYS, int N>
+template <int PHYS, int N, int MODE, int E_, int R_, int CPT_, int WM_>
 struct Cfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
-  static constexpr int E = Tile<PHYS, N>::E, R = Tile<PHYS, N>::R, CPT = Tile<PHYS, N>::CPT;
-  static constexpr int G = (Np + R - 1) / R;       // row groups
-  static constexpr int IP = G * R;                 // padded rows of AT
-  static constexpr int NCOL = NV * E;              // columns of B
-  static constexpr int CG = NCOL / CPT;            // column groups
-  static constexpr int THREADS = CG * G;
-  static constexpr int BROWS = (3 * Np > NFF) ? 3 * Np : NFF;
-  static constexpr size_t SMEM =
-      sizeof(double) * ((size_t)NV * E * Np + (size_t)BROWS * NCOL) + sizeof(int) * NFF;
-  static_assert(NCOL % CPT == 0, "columns must split evenly");
-  static_assert(NV * E * Np <= BROWS * NCOL, "epilogue reuses B for the rhs");
+  static constexpr int E = E_, EP = E_ + 1;
+  static constexpr int NCOL = NV * E;
+  // SIMT tiling: R rows x CPT columns per thread
+  static constexpr int R = R_, CPT = CPT_;
+  static constexpr int G = (Np + R - 1) / R;
+  static constexpr int CG = NCOL / CPT;
+  // DMMA tiling: MT m-tiles of 8 rows, NT n-tiles of 8 columns; each warp
+  // owns WM m-tiles x WN n-tiles
+  static constexpr int MT = (Np + 7) / 8, NT = NCOL / 8;
+  static constexpr int WM = WM_ > MT ? MT : WM_;
+  static constexpr int WN = CPT_;
+  static constexpr int MGROUPS = (MT + WM - 1) / WM;
+  static constexpr int WARPS_D = MODE == MODE_DMMA ? MGROUPS * (NT / WN) : 0;
+  static constexpr int THREADS = MODE == MODE_SIMT ? CG * G : 32 * WARPS_D;
+  static constexpr int KV = 3 * Np, KVP = (KV + 3) / 4 * 4;    // volume k (padded to 4)
+  static constexpr int KF = NFF, KFP = (KF + 3) / 4 * 4;
+  static constexpr int IP = MODE == MODE_SIMT ? G * R : 8 * MT;     // padded rows
+  static constexpr int BLD = MODE == MODE_SIMT ? NCOL : NCOL + 4;   // B row stride
+  static constexpr int BROWS = KVP > KFP ? KVP : KFP;
+  // shared memory
+  static constexpr int S_U = NV * Np * EP;
+  static constexpr int S_B = BROWS * BLD;
+  static constexpr int S_GEO = 9 * E;
+  static constexpr int S_FACE = 5 * 4 * E;                     // nx ny nz fs tau
+  static constexpr int VMLD = NFF + 1;                         // vmapP row stride (ints)
+  static constexpr size_t SMEM = sizeof(double) * (S_U + S_B + S_GEO + S_FACE) +
+                                 sizeof(int) * ((size_t)E * VMLD + NFF);
+  static_assert(NCOL % CPT_ == 0, "columns must split evenly");
+  static_assert(S_B >= NV * Np * EP, "epilogue reuses B for the rhs");
+  static_assert(MODE == MODE_SIMT || NCOL % 8 == 0, "DMMA needs whole n-tiles");
+  static_assert(MODE == MODE_SIMT || NT % WN == 0, "DMMA n-tiles must split over warps");
+  static_assert(THREADS <= 1024, "block too large");
 };
 
-template <int PHYS, int N>
-__global__ void __launch_bounds__(Cfg<PHYS, N>::THREADS)
+// ---------------------------------------------------------------------------
+// contraction engines: acc += A[:, k range] * B[rows of the range, :]
+// ---------------------------------------------------------------------------
+
+template <class C, int KL>
+__device__ __forceinline__ void contract_simt(const double *__restrict__ AT, int kofs,
+                                              const double *sB, double (&acc)[C::R][C::CPT],
+                                              int tid) {
+  const int cg = tid % C::CG, rg = tid / C::CG;
+  const double *Ab = AT + (long)kofs * C::IP + rg * C::R;
+#pragma unroll 3
+  for (int k = 0; k < KL; k++) {
+    double bv[C::CPT], av[C::R];
+#pragma unroll
+    for (int j = 0; j < C::CPT; j++) bv[j] = sB[k * C::BLD + cg + j * C::CG];
+#pragma unroll
+    for (int r = 0; r < C::R; r++) av[r] = __ldg(Ab + (long)k * C::IP + r);
+#pragma unroll
+    for (int r = 0; r < C::R; r++)
+#pragma unroll
+      for (int j = 0; j < C::CPT; j++) acc[r][j] = fma(av[r], bv[j], acc[r][j]);
+  }
+}
+
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+// A fragments are stored [kstep][mtile][lane] in the lane order of the
+// m8n8k4 A operand (row = lane/4, col = lane%4): one coalesced load each.
+// B fragments (row = lane%4, col = lane/4) come from sB.
+template <class C, int KSTEPS>
+__device__ __forceinline__ void contract_dmma(const double *__restrict__ Afrag, int kstep0,
+                                              const double *sB,
+                                              double (&acc)[C::WM][C::WN][2], int warp,
+                                              int lane) {
+  const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
+  const int m0 = mg * C::WM, n0 = ng * C::WN;
+  const double *Ab = Afrag + ((long)kstep0 * C::MT + m0) * 32 + lane;
+  const double *Bb = sB + (lane & 3) * C::BLD + n0 * 8 + (lane >> 2);
+#pragma unroll 2
+  for (int ks = 0; ks < KSTEPS; ks++) {
+    double av[C::WM], bv[C::WN];
+#pragma unroll
+    for (int i = 0; i < C::WM; i++)
+      av[i] = (m0 + i < C::MT) ? __ldg(Ab + ((long)ks * C::MT + i) * 32) : 0.0;
+#pragma unroll
+    for (int j = 0; j < C::WN; j++) bv[j] = Bb[ks * 4 * C::BLD + j * 8];
+#pragma unroll
+    for (int i = 0; i < C::WM; i++)
+#pragma unroll
+      for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the stage kernel
+// ---------------------------------------------------------------------------
+
+template <int PHYS, int N, int MODE, int E_, int R_, int CPT_, int WM_>
+__global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>::THREADS)
     stage_fp64_kernel(const StageArgs a) {
-  using C = Cfg<PHYS, N>;
-  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, R = C::R,
-                CPT = C::CPT, CG = C::CG, NCOL = C::NCOL, IP = C::IP;
+  using C = Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>;
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+                BLD = C::BLD, T = C::THREADS;
+  constexpr bool SIMT = MODE == MODE_SIMT;
+  constexpr int AR = SIMT ? C::R : 1, AC = SIMT ? C::CPT : 1;     // SIMT accumulators
+  constexpr int DM = SIMT ? 1 : C::WM, DN = SIMT ? 1 : C::WN;     // DMMA accumulators
   extern __shared__ __align__(16) double smem[];
-  double *sU = smem;                              // [NV][E][Np]
-  double *sB = sU + NV * E * Np;                  // [BROWS][NCOL], col = v*E + e
-  int *sFm = reinterpret_cast<int *>(sB + C::BROWS * NCOL);
+  double *sU = smem;                    // [v][i][EP]
+  double *sB = sU + C::S_U;             // [k][BLD], col = v*E + e
+  double *sGeo = sB + C::S_B;           // [9][E]
+  double *sFace = sGeo + C::S_GEO;      // [5][4][E]: nx ny nz fs tau
+  int *sVm = reinterpret_cast<int *>(sFace + C::S_FACE);   // [E][VMLD]
+  int *sFm = sVm + E * C::VMLD;         // [NFF]
 
   const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
   const long e0 = (long)blockIdx.x * E;
   const int ne = (int)min((long)E, (long)a.K - e0);
   const long vs = a.vs;
 
-  for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
-  // 0. stage the tile's state
+  // 0. staging
+  for (int i = tid; i < NFF; i += T) sFm[i] = a.Fmask[i];
   for (int v = 0; v < NV; v++) {
     const double *src = a.u_in + v * vs + e0 * Np;
-    for (int i = tid; i < E * Np; i += C::THREADS)
-      sU[v * E * Np + i] = (i < ne * Np) ? src[i] : (v == 0 ? 1.0 : 0.0);
+    for (int g = tid; g < E * Np; g += T) {
+      const int e = g / Np, i = g - e * Np;
+      sU[(v * Np + i) * EP + e] = (g < ne * Np) ? src[g] : (v == 0 ? 1.0 : 0.0);
+    }
+  }
+  for (int g = tid; g < 9 * E; g += T) {
+    const int m = g / E, e = g - m * E;
+    sGeo[g] = e < ne ? __ldg(a.geo + (long)m * a.gstride + e0 + e) : 0.0;
+  }
+  for (int g = tid; g < 4 * E; g += T) {
+    const int e = g >> 2, f = g & 3;      // consecutive g: consecutive faces in HBM
+    const long gf = (e0 + e) * 4 + f;
+    const bool ok = e < ne;
+    sFace[(0 * 4 + f) * E + e] = ok ? __ldg(a.nrm + gf) : 0.0;
+    sFace[(1 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 4L * a.gstride + gf) : 0.0;
+    sFace[(2 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 8L * a.gstride + gf) : 0.0;
+    sFace[(3 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf) : 0.0;
+    sFace[(4 * 4 + f) * E + e] = ok ? __ldg(a.tau + gf) : 0.0;
+  }
+  for (int g = tid; g < E * NFF; g += T) {
+    const int e = g / NFF, fj = g - e * NFF;
+    sVm[e * C::VMLD + fj] = g < ne * NFF ? __ldg(a.vmapP + e0 * NFF + g) : 0;
   }
   __syncthreads();
 
   // 1. volume fluxes -> B rows [0, 3Np)
-  for (int it = tid; it < E * Np; it += C::THREADS) {
-    const int e = it / Np, i = it % Np;
-    double g[9];
-    if (e < ne) {
-#pragma unroll
-      for (int m = 0; m < 9; m++) g[m] = __ldg(a.geo + (long)m * a.K + e0 + e);
-    } else {
-#pragma unroll
-      for (int m = 0; m < 9; m++) g[m] = 0.0;
-    }
+  for (int it = tid; it < E * Np; it += T) {
+    const int i = it / E, e = it - i * E;
+    const double *g = sGeo + e;
+    const double rx = g[0], ry = g[E], rz = g[2 * E], sx = g[3 * E], sy = g[4 * E],
+                 sz = g[5 * E], tx = g[6 * E], ty = g[7 * E], tz = g[8 * E];
     if (PHYS == EUL) {
       double q[5], F[5], Gf[5], W[5];
 #pragma unroll
-      for (int v = 0; v < 5; v++) q[v] = sU[v * E * Np + e * Np + i];
-      euler_flux(a.gamma, q, F, Gf, W);
+      for (int v = 0; v < 5; v++) q[v] = sU[(v * Np + i) * EP + e];
+      euler_flux_fast(a.gamma, q, F, Gf, W);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const int col = v * E + e;
-        sB[(0 * Np + i) * NCOL + col] = g[0] * F[v] + g[1] * Gf[v] + g[2] * W[v];
-        sB[(1 * Np + i) * NCOL + col] = g[3] * F[v] + g[4] * Gf[v] + g[5] * W[v];
-        sB[(2 * Np + i) * NCOL + col] = g[6] * F[v] + g[7] * Gf[v] + g[8] * W[v];
+        sB[(0 * Np + i) * BLD + col] = rx * F[v] + ry * Gf[v] + rz * W[v];
+        sB[(1 * Np + i) * BLD + col] = sx * F[v] + sy * Gf[v] + sz * W[v];
+        sB[(2 * Np + i) * BLD + col] = tx * F[v] + ty * Gf[v] + tz * W[v];
       }
     } else {
       const long n = (e < ne) ? (e0 + e) * Np + i : 0;
-      const double uu = sU[e * Np + i];
+      const double uu = sU[i * EP + e];
       const double F = __ldg(a.vel + n) * uu, Gf = __ldg(a.vel + vs + n) * uu,
                    W = __ldg(a.vel + 2 * vs + n) * uu;
-      sB[(0 * Np + i) * NCOL + e] = g[0] * F + g[1] * Gf + g[2] * W;
-      sB[(1 * Np + i) * NCOL + e] = g[3] * F + g[4] * Gf + g[5] * W;
-      sB[(2 * Np + i) * NCOL + e] = g[6] * F + g[7] * Gf + g[8] * W;
+      sB[(0 * Np + i) * BLD + e] = rx * F + ry * Gf + rz * W;
+      sB[(1 * Np + i) * BLD + e] = sx * F + sy * Gf + sz * W;
+      sB[(2 * Np + i) * BLD + e] = tx * F + ty * Gf + tz * W;
     }
+  }
+  if (!SIMT) {   // zero the k padding rows of the volume block
+    for (int g = tid; g < (C::KVP - C::KV) * BLD; g += T) sB[C::KV * BLD + g] = 0.0;
   }
   __syncthreads();
 
   // 2. volume contraction
-  const int cg = tid % CG, rg = tid / CG;
-  double acc[R][CPT];
+  double accS[AR][AC];
+  double accD[DM][DN][2];
 #pragma unroll
-  for (int r = 0; r < R; r++)
+  for (int r = 0; r < AR; r++)
 #pragma unroll
-    for (int j = 0; j < CPT; j++) acc[r][j] = 0.0;
-
-  const double *Ab = a.AT + rg * R;
-#pragma unroll 3
-  for (int k = 0; k < 3 * Np; k++) {
-    double bv[CPT], av[R];
+    for (int j = 0; j < AC; j++) accS[r][j] = 0.0;
 #pragma unroll
-    for (int j = 0; j < CPT; j++) bv[j] = sB[k * NCOL + cg + j * CG];
+  for (int i = 0; i < DM; i++)
 #pragma unroll
-    for (int r = 0; r < R; r++) av[r] = __ldg(Ab + (long)k * IP + r);
-#pragma unroll
-    for (int r = 0; r < R; r++)
-#pragma unroll
-      for (int j = 0; j < CPT; j++) acc[r][j] = fma(av[r], bv[j], acc[r][j]);
+    for (int j = 0; j < DN; j++) accD[i][j][0] = accD[i][j][1] = 0.0;
+  if constexpr (SIMT) {
+    contract_simt<C, C::KV>(a.AT, 0, sB, accS, tid);
+  } else {
+    if (warp < C::WARPS_D) contract_dmma<C, C::KVP / 4>(a.AT, 0, sB, accD, warp, lane);
   }
   __syncthreads();
 
   // 3. face traces and fluxes -> B rows [0, NFF)
-  for (int it = tid; it < E * NFF; it += C::THREADS) {
-    const int e = it / NFF, fj = it % NFF, f = fj / Nfp;
+  for (int it = tid; it < E * NFF; it += T) {
+    const int fj = it / E, e = it - fj * E, f = fj / Nfp;
     const int nodeM = sFm[fj];
     if (e >= ne) {
 #pragma unroll
-      for (int v = 0; v < NV; v++) sB[fj * NCOL + v * E + e] = 0.0;
+      for (int v = 0; v < NV; v++) sB[fj * BLD + v * E + e] = 0.0;
       continue;
     }
-    const long gf = (e0 + e) * 4 + f;
-    const long idxP = __ldg(a.vmapP + (e0 + e) * NFF + fj);
-    const double nx = __ldg(a.nrm + gf), ny = __ldg(a.nrm + 4L * a.K + gf),
-                 nz = __ldg(a.nrm + 8L * a.K + gf);
-    const double fs = __ldg(a.fscale + gf), tau = __ldg(a.tau + gf);
+    const long idxP = sVm[e * C::VMLD + fj];
+    const double nx = sFace[(0 * 4 + f) * E + e], ny = sFace[(1 * 4 + f) * E + e],
+                 nz = sFace[(2 * 4 + f) * E + e], fs = sFace[(3 * 4 + f) * E + e],
+                 tau = sFace[(4 * 4 + f) * E + e];
     if (PHYS == EUL) {
       double qm[5], qb[5], F[5], Gf[5], W[5];
 #pragma unroll
       for (int v = 0; v < 5; v++) {
-        qm[v] = sU[v * E * Np + e * Np + nodeM];
+        qm[v] = sU[(v * Np + nodeM) * EP + e];
         qb[v] = 0.5 * (qm[v] + __ldg(a.u_in + v * vs + idxP));
       }
-      euler_flux(a.gamma, qb, F, Gf, W);
+      euler_flux_fast(a.gamma, qb, F, Gf, W);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];
-        sB[fj * NCOL + v * E + e] = (nd - tau * (qb[v] - qm[v])) * fs;
+        sB[fj * BLD + v * E + e] = (nd - tau * (qb[v] - qm[v])) * fs;
       }
     } else {
-      const double um = sU[e * Np + nodeM];
+      const double um = sU[nodeM * EP + e];
       const double ub = 0.5 * (um + __ldg(a.u_in + idxP));
       const long nM = (e0 + e) * Np + nodeM;
       const double F = __ldg(a.vel + nM) * ub, Gf = __ldg(a.vel + vs + nM) * ub,
                    W = __ldg(a.vel + 2 * vs + nM) * ub;
       const double nd = nx * F + ny * Gf + nz * W;
-      sB[fj * NCOL + e] = (nd - tau * (ub - um)) * fs;
+      sB[fj * BLD + e] = (nd - tau * (ub - um)) * fs;
     }
   }
-  __syncthreads();
-
-  // 4. lift contraction (AT rows [3Np, 3Np+NFF) hold -LIFT^T)
-  const double *Al = a.AT + (long)3 * Np * IP + rg * R;
-#pragma unroll 3
-  for (int k = 0; k < NFF; k++) {
-    double bv[CPT], av[R];
-#pragma unroll
-    for (int j = 0; j < CPT; j++) bv[j] = sB[k * NCOL + cg + j * CG];
-#pragma unroll
-    for (int r = 0; r < R; r++) av[r] = __ldg(Al + (long)k * IP + r);
-#pragma unroll
-    for (int r = 0; r < R; r++)
-#pragma unroll
-      for (int j = 0; j < CPT; j++) acc[r][j] = fma(av[r], bv[j], acc[r][j]);
+  if (!SIMT) {
+    for (int g = tid; g < (C::KFP - C::KF) * BLD; g += T) sB[C::KF * BLD + g] = 0.0;
   }
   __syncthreads();
 
-  // 5. epilogue through shared memory: rhs as [v][e][i] in B
+  // 4. lift contraction (A columns [3Np, 3Np+NFF) hold -LIFT)
+  if constexpr (SIMT) {
+    contract_simt<C, C::KF>(a.AT, C::KV, sB, accS, tid);
+  } else {
+    if (warp < C::WARPS_D) contract_dmma<C, C::KFP / 4>(a.AT, C::KVP / 4, sB, accD, warp, lane);
+  }
+  __syncthreads();
+
+  // 5. epilogue through shared memory: rhs as [v][i][EP] in B
   double *sR = sB;
+  if constexpr (SIMT) {
+    const int cg = tid % C::CG, rg = tid / C::CG;
 #pragma unroll
-  for (int r = 0; r < R; r++) {
-    const int i = rg * R + r;
-    if (i < Np) {
+    for (int r = 0; r < AR; r++) {
+      const int i = rg * C::R + r;
+      if (i < Np) {
 #pragma unroll
-      for (int j = 0; j < CPT; j++) sR[(cg + j * CG) * Np + i] = acc[r][j];
+        for (int j = 0; j < AC; j++) {
+          const int col = cg + j * C::CG, v = col / E, e = col - v * E;
+          sR[(v * Np + i) * EP + e] = accS[r][j];
+        }
+      }
+    }
+  } else {
+    if (warp < C::WARPS_D) {
+      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
+#pragma unroll
+      for (int ii = 0; ii < DM; ii++) {
+        const int i = (mg * C::WM + ii) * 8 + (lane >> 2);
+        if (i < Np) {
+#pragma unroll
+          for (int jj = 0; jj < DN; jj++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int col = (ng * C::WN + jj) * 8 + (lane & 3) * 2 + h;
+              const int v = col / E, e = col - v * E;
+              sR[(v * Np + i) * EP + e] = accD[ii][jj][h];
+            }
+          }
+        }
+      }
     }
   }
   __syncthreads();
@@ -232,16 +353,18 @@ __global__ void __launch_bounds__(Cfg<PHYS, N>::THREADS)
   const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
   for (int v = 0; v < NV; v++) {
     const long base = v * vs + e0 * Np;
-    for (int i = tid; i < ne * Np; i += C::THREADS) {
-      const double rhs = sR[v * E * Np + i];
+    for (int g = tid; g < ne * Np; g += T) {
+      const int e = g / Np, i = g - e * Np;
+      const int s = (v * Np + i) * EP + e;
+      const double rhs = sR[s];
       if (a.rhs_only) {
-        a.u_out[base + i] = rhs;
+        a.u_out[base + g] = rhs;
       } else {
-        const double kn = a.rka * a.kreg[base + i] + dt * rhs;
-        const double un = sU[v * E * Np + i] + a.rkb * kn;
-        a.kreg[base + i] = kn;
-        a.u_out[base + i] = un;
-        sU[v * E * Np + i] = un;
+        const double kn = a.rka * a.kreg[base + g] + dt * rhs;
+        const double un = sU[s] + a.rkb * kn;
+        a.kreg[base + g] = kn;
+        a.u_out[base + g] = un;
+        sU[s] = un;
       }
     }
   }
@@ -251,19 +374,22 @@ __global__ void __launch_bounds__(Cfg<PHYS, N>::THREADS)
   // fused calc_maxv on the new state (Euler): per face max |v|^2 and c^2
   __shared__ unsigned long long sMax[32];
   unsigned long long local = 0ull;
-  for (int it = tid; it < ne * 4; it += C::THREADS) {
-    const int e = it / 4, f = it % 4;
+  for (int it = tid; it < 4 * E; it += T) {
+    const int f = it / E, e = it - f * E;
+    if (e >= ne) continue;
     double mv2 = 0.0, mc2 = 0.0;
     bool bad = false;
     for (int j = 0; j < Nfp; j++) {
-      const int nd = e * Np + sFm[f * Nfp + j];
-      const double u1 = sU[nd], u2 = sU[E * Np + nd], u3 = sU[2 * E * Np + nd],
-                   u4 = sU[3 * E * Np + nd], u5 = sU[4 * E * Np + nd];
-      const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
+      const int nd = sFm[f * Nfp + j];
+      const double u1 = sU[(0 * Np + nd) * EP + e], u2 = sU[(1 * Np + nd) * EP + e],
+                   u3 = sU[(2 * Np + nd) * EP + e], u4 = sU[(3 * Np + nd) * EP + e],
+                   u5 = sU[(4 * Np + nd) * EP + e];
+      const double ir = 1.0 / u1;
+      const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
       const double v2 = vx * vx + vy * vy + vz * vz;
       mv2 = v2 > mv2 ? v2 : mv2;
       const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-      const double c2 = fabs(a.gamma * pres / u1);
+      const double c2 = fabs(a.gamma * pres * ir);
       mc2 = c2 > mc2 ? c2 : mc2;
       bad |= (v2 != v2) || (c2 != c2);
     }
@@ -271,18 +397,20 @@ __global__ void __launch_bounds__(Cfg<PHYS, N>::THREADS)
     double mv = sqrt(mv2) + sqrt(mc2);
     if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
     a.maxv[gf] = mv;
-    const unsigned long long b = dbits(mv * __ldg(a.fscale + gf));
+    const unsigned long long b = dbits(mv * sFace[(3 * 4 + f) * E + e]);
     local = b > local ? b : local;
   }
   local = warp_max_bits(local);
   if ((tid & 31) == 0) sMax[tid >> 5] = local;
   __syncthreads();
   if (tid < 32) {
-    unsigned long long v = tid < (C::THREADS + 31) / 32 ? sMax[tid] : 0ull;
+    unsigned long long v = tid < (T + 31) / 32 ? sMax[tid] : 0ull;
     v = warp_max_bits(v);
     if (tid == 0) atomicMax(&a.sc->acc[a.sc->parity ^ 1], v);
   }
 }
+
+#include "dglm_stage_pipe.cuh"
 
 // Standalone calc_maxv (initial state, advection velocity): maxv per face and
 // a device-wide max of maxv*Fscale into sc->acc[slot].
@@ -383,19 +511,154 @@ __global__ void tau_kernel(int K, double tau_scale, const int *__restrict__ vmap
 }
 
 // ---------------------------------------------------------------------------
-// dispatch
+// variants and dispatch
 // ---------------------------------------------------------------------------
 
-template <int PHYS, int N>
-static cudaError_t launch_one(const StageArgs &a, cudaStream_t s) {
-  using C = Cfg<PHYS, N>;
-  // set per call: the attribute belongs to the current device's context
-  cudaError_t e = cudaFuncSetAttribute(stage_fp64_kernel<PHYS, N>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+struct Variant {
+  StageVariantInfo info;
+  cudaError_t (*launch)(const StageArgs &, cudaStream_t);
+};
+
+template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM>
+static cudaError_t launch_v(const StageArgs &a, cudaStream_t s) {
+  using C = Cfg<PHYS, N, MODE, E, R, CPT, WM>;
+  auto k = stage_fp64_kernel<PHYS, N, MODE, E, R, CPT, WM>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)C::SMEM);
   if (e != cudaSuccess) return e;
   const int blocks = (a.K + C::E - 1) / C::E;
-  stage_fp64_kernel<PHYS, N><<<blocks, C::THREADS, C::SMEM, s>>>(a);
+  k<<<blocks, C::THREADS, C::SMEM, s>>>(a);
   return cudaGetLastError();
+}
+
+static int sm_count() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 148;
+}
+
+template <int PHYS, int N, int E, int WN, int WM, bool AS>
+static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
+  using C = PCfg<PHYS, N, E, WN, WM, AS>;
+  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int ntiles = (a.K + E - 1) / E;
+  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  k<<<grid, C::THREADS, C::SMEM, s>>>(a, ntiles);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E, int WN, int WM, bool AS>
+static Variant make_pipe() {
+  using C = PCfg<PHYS, N, E, WN, WM, AS>;
+  StageVariantInfo i{};
+  i.mode = MODE_PIPE;
+  i.E = E;
+  i.R = 8;
+  i.CPT = WN;
+  i.WM = C::WM;
+  i.IP = 8 * C::MT;
+  i.MT = C::MT;
+  i.KVP = C::KVP;
+  i.KFP = C::KFP;
+  i.threads = C::THREADS;
+  i.smem = C::SMEM;
+  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS>};
+}
+
+template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM>
+static Variant make_v() {
+  using C = Cfg<PHYS, N, MODE, E, R, CPT, WM>;
+  StageVariantInfo i{};
+  i.mode = MODE;
+  i.E = E;
+  i.R = MODE == MODE_SIMT ? R : 8;
+  i.CPT = CPT;
+  i.WM = C::WM;
+  i.IP = C::IP;
+  i.MT = C::MT;
+  i.KVP = C::KVP;
+  i.KFP = C::KFP;
+  i.threads = C::THREADS;
+  i.smem = C::SMEM;
+  return Variant{i, &launch_v<PHYS, N, MODE, E, R, CPT, WM>};
+}
+
+// Candidate tile shapes per (physics, N); entry 0 is the default, the others
+// are alternatives the tuner may pick.  SIMT(E, R rows, CPT columns per
+// thread); DMMA(E, WN n-tiles, WM m-tiles per warp).
+template <int PHYS, int N>
+static const std::vector<Variant> &variants();
+
+#define V_SIMT(P, NN, E, R, C) make_v<P, NN, MODE_SIMT, E, R, C, 1>()
+#define V_DMMA(P, NN, E, WN, WM) make_v<P, NN, MODE_DMMA, E, 1, WN, WM>()
+#define V_PIPE(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS>()
+#define DGLM_VARIANTS(P, NN, ...)                        \
+  template <>                                            \
+  const std::vector<Variant> &variants<P, NN>() {        \
+    static const std::vector<Variant> v = {__VA_ARGS__}; \
+    return v;                                            \
+  }
+
+DGLM_VARIANTS(EUL, 1, V_SIMT(EUL, 1, 128, 4, 5), V_DMMA(EUL, 1, 64, 4, 1))
+DGLM_VARIANTS(EUL, 2, V_SIMT(EUL, 2, 64, 5, 5), V_DMMA(EUL, 2, 32, 4, 2))
+DGLM_VARIANTS(EUL, 3, V_DMMA(EUL, 3, 16, 2, 3), V_SIMT(EUL, 3, 32, 5, 5),
+              V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true))
+DGLM_VARIANTS(EUL, 4, V_DMMA(EUL, 4, 8, 1, 5), V_SIMT(EUL, 4, 16, 5, 5),
+              V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5), V_DMMA(EUL, 4, 16, 2, 5),
+              V_PIPE(EUL, 4, 8, 1, 5, true), V_PIPE(EUL, 4, 8, 1, 5, false),
+              V_PIPE(EUL, 4, 8, 1, 3, true))
+DGLM_VARIANTS(EUL, 5, V_DMMA(EUL, 5, 8, 1, 7), V_SIMT(EUL, 5, 8, 7, 5),
+              V_PIPE(EUL, 5, 8, 1, 7, false))
+DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5))
+DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
+DGLM_VARIANTS(EUL, 8, V_DMMA(EUL, 8, 8, 1, 7), V_SIMT(EUL, 8, 4, 8, 5))
+DGLM_VARIANTS(ADV, 1, V_SIMT(ADV, 1, 256, 4, 4), V_DMMA(ADV, 1, 64, 2, 1))
+DGLM_VARIANTS(ADV, 2, V_SIMT(ADV, 2, 128, 5, 4), V_DMMA(ADV, 2, 64, 2, 2))
+DGLM_VARIANTS(ADV, 3, V_SIMT(ADV, 3, 64, 5, 4), V_DMMA(ADV, 3, 64, 2, 3),
+              V_PIPE(ADV, 3, 32, 1, 3, true))
+DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5))
+DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7))
+DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6))
+DGLM_VARIANTS(ADV, 7, V_SIMT(ADV, 7, 16, 8, 4), V_DMMA(ADV, 7, 16, 1, 5))
+DGLM_VARIANTS(ADV, 8, V_SIMT(ADV, 8, 16, 8, 4), V_DMMA(ADV, 8, 16, 1, 7))
+
+static const std::vector<Variant> *variant_list(int physics, int N) {
+#define CASE(P, NN) \
+  case NN: return &variants<P, NN>();
+  if (physics == DGLM_EULER) {
+    switch (N) { CASE(EUL, 1) CASE(EUL, 2) CASE(EUL, 3) CASE(EUL, 4)
+                 CASE(EUL, 5) CASE(EUL, 6) CASE(EUL, 7) CASE(EUL, 8) }
+  } else if (physics == DGLM_ADVECTION) {
+    switch (N) { CASE(ADV, 1) CASE(ADV, 2) CASE(ADV, 3) CASE(ADV, 4)
+                 CASE(ADV, 5) CASE(ADV, 6) CASE(ADV, 7) CASE(ADV, 8) }
+  }
+#undef CASE
+  return nullptr;
+}
+
+bool stage_fp64_supported(int physics, int N) { return variant_list(physics, N) != nullptr; }
+
+int stage_variant_count(int physics, int N) {
+  auto *v = variant_list(physics, N);
+  return v ? (int)v->size() : 0;
+}
+
+bool stage_variant_info(int physics, int N, int idx, StageVariantInfo *out) {
+  auto *v = variant_list(physics, N);
+  if (!v || idx < 0 || idx >= (int)v->size()) return false;
+  *out = (*v)[idx].info;
+  return true;
+}
+
+cudaError_t launch_stage_fp64(int physics, int N, int variant, const StageArgs &a,
+                              cudaStream_t s) {
+  auto *v = variant_list(physics, N);
+  if (!v || variant < 0 || variant >= (int)v->size()) return cudaErrorInvalidValue;
+  return (*v)[variant].launch(a, s);
 }
 
 template <int PHYS, int N>
@@ -407,60 +670,19 @@ static cudaError_t launch_maxv_one(const StageArgs &a, int slot, cudaStream_t s)
   return cudaGetLastError();
 }
 
-#define DGLM_DISPATCH(FN, PHYS, N, ...)                        \
-  switch (N) {                                                 \
-    case 1: return FN<PHYS, 1>(__VA_ARGS__);                   \
-    case 2: return FN<PHYS, 2>(__VA_ARGS__);                   \
-    case 3: return FN<PHYS, 3>(__VA_ARGS__);                   \
-    case 4: return FN<PHYS, 4>(__VA_ARGS__);                   \
-    case 5: return FN<PHYS, 5>(__VA_ARGS__);                   \
-    case 6: return FN<PHYS, 6>(__VA_ARGS__);                   \
-    case 7: return FN<PHYS, 7>(__VA_ARGS__);                   \
-    case 8: return FN<PHYS, 8>(__VA_ARGS__);                   \
-    default: return cudaErrorInvalidValue;                     \
-  }
-
-bool stage_fp64_supported(int physics, int N) {
-  return (physics == DGLM_EULER || physics == DGLM_ADVECTION) && N >= 1 && N <= kMaxOrder;
-}
-
-template <int PHYS, int N>
-static int ip_of() { return Cfg<PHYS, N>::IP; }
-
-int stage_rows_padded(int physics, int N) {
-  if (physics == DGLM_EULER) {
-    switch (N) {
-      case 1: return ip_of<EUL, 1>(); case 2: return ip_of<EUL, 2>();
-      case 3: return ip_of<EUL, 3>(); case 4: return ip_of<EUL, 4>();
-      case 5: return ip_of<EUL, 5>(); case 6: return ip_of<EUL, 6>();
-      case 7: return ip_of<EUL, 7>(); case 8: return ip_of<EUL, 8>();
-    }
-  } else {
-    switch (N) {
-      case 1: return ip_of<ADV, 1>(); case 2: return ip_of<ADV, 2>();
-      case 3: return ip_of<ADV, 3>(); case 4: return ip_of<ADV, 4>();
-      case 5: return ip_of<ADV, 5>(); case 6: return ip_of<ADV, 6>();
-      case 7: return ip_of<ADV, 7>(); case 8: return ip_of<ADV, 8>();
-    }
-  }
-  return -1;
-}
-
-cudaError_t launch_stage_fp64(int physics, int N, const StageArgs &a, cudaStream_t s) {
-  if (physics == DGLM_EULER) {
-    DGLM_DISPATCH(launch_one, EUL, N, a, s)
-  } else {
-    DGLM_DISPATCH(launch_one, ADV, N, a, s)
-  }
-}
-
 cudaError_t launch_face_maxv(int physics, int N, const StageArgs &a, int slot,
                              cudaStream_t s) {
+#define CASE(P, NN) \
+  case NN: return launch_maxv_one<P, NN>(a, slot, s);
   if (physics == DGLM_EULER) {
-    DGLM_DISPATCH(launch_maxv_one, EUL, N, a, slot, s)
+    switch (N) { CASE(EUL, 1) CASE(EUL, 2) CASE(EUL, 3) CASE(EUL, 4)
+                 CASE(EUL, 5) CASE(EUL, 6) CASE(EUL, 7) CASE(EUL, 8) }
   } else {
-    DGLM_DISPATCH(launch_maxv_one, ADV, N, a, slot, s)
+    switch (N) { CASE(ADV, 1) CASE(ADV, 2) CASE(ADV, 3) CASE(ADV, 4)
+                 CASE(ADV, 5) CASE(ADV, 6) CASE(ADV, 7) CASE(ADV, 8) }
   }
+#undef CASE
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_step_begin(int N, double cfl, double tmax, int frozen, DevScalars *sc,

@@ -1,0 +1,416 @@
+// Persistent, warp-specialised FP64 stage kernel (included by
+// dglm_stage_fp64.cu, which defines EUL/ADV, euler_flux_fast and
+// dmma_8x8x4).
+//
+// One CTA per SM walks the element tiles t = blockIdx.x, +gridDim.x, ...
+// with a two-deep shared-memory pipeline:
+//
+//   producer warp   TMA bulk copies (cp.async.bulk, mbarrier complete_tx) of
+//                   the next tile's state u, RK register k, metrics, face
+//                   data (and advection velocity) -- all contiguous per tile
+//                   -- plus cp.async gathers of the neighbour traces
+//                   u[vmapP] straight into a [v][face node][e] layout;
+//   consumer warps  volume flux -> DMMA volume contraction -> face flux ->
+//                   DMMA lift contraction -> LSERK epilogue with coalesced
+//                   stores; then release the buffer to the producer.
+//
+// The stacked operator's m8n8k4 A fragments are loaded into shared memory
+// once per CTA (orders whose FP64 operators do not fit read them through L1).
+// Every mbarrier wait is bounded by a clock limit; on expiry the CTA sets
+// flag bit 2 in the device scalars and leaves after its copies settle.
+// This header is included inside namespace dglm.
+#pragma once
+
+constexpr long long kWaitCycles = 2000000000LL;   // ~1 s at the B200 clock
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *b, unsigned tx) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(tx)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the completion of the phase with the given parity
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity) {
+  if (mbar_try_wait(b, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(b, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
+                                         unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long *b) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(b))
+               : "memory");
+}
+__device__ __forceinline__ void consumer_sync(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+// AND of a predicate over the consumer threads (named barrier 2)
+__device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, 2, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)v), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM>
+struct PCfg {
+  static constexpr int NV = PHYS == EUL ? 5 : 1;
+  static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
+  static constexpr int E = E_, EP = E_ + 1, NCOL = NV * E;
+  static constexpr int MT = (Np + 7) / 8, NT = NCOL / 8;
+  static constexpr int WN = WN_, WM = WM_ > MT ? MT : WM_;
+  static constexpr int MGROUPS = (MT + WM - 1) / WM;
+  static constexpr int NWC = MGROUPS * (NT / WN);      // consumer warps
+  static constexpr int TC = 32 * NWC;                   // consumer threads
+  static constexpr int THREADS = TC + 32;               // + producer warp
+  static constexpr int KV = 3 * Np, KVP = (KV + 3) / 4 * 4;
+  static constexpr int KF = NFF, KFP = (KF + 3) / 4 * 4;
+  static constexpr int KS = KVP / 4 + KFP / 4;
+  static constexpr int BLD = NCOL + 4, BROWS = KVP > KFP ? KVP : KFP;
+  // shared memory segments, in doubles
+  static constexpr int S_AF = ASMEM ? KS * MT * 32 : 0;
+  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
+  static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
+  static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
+  static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
+  static constexpr int S_B = BROWS * BLD > NV * Np * EP ? BROWS * BLD : NV * Np * EP;
+  static constexpr int S_MISC = 8 + NFF / 2 + 1 + 40;   // barriers, Fmask, reduction
+  static constexpr size_t SMEM = sizeof(double) * ((size_t)S_AF + 2 * S_BUF + S_B + S_MISC);
+  // bytes the producer's bulk copies deliver per tile
+  static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE + S_VEL);
+  static_assert(NCOL % 8 == 0 && NT % WN == 0, "n-tiles must split over the warps");
+  static_assert((E * Np * 8) % 16 == 0 && (E * 8) % 16 == 0, "bulk copies need 16-byte sizes");
+  static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
+};
+
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM>
+__global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1)
+    stage_pipe_kernel(const StageArgs a, int ntiles) {
+  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM>;
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+                BLD = C::BLD, TC = C::TC;
+  extern __shared__ __align__(16) double smem[];
+  double *sAF = smem;
+  double *sBuf0 = sAF + C::S_AF;
+  double *sB = sBuf0 + 2 * C::S_BUF;
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(sB + C::S_B);
+  unsigned long long *full = bars, *empty = bars + 2, *abar = bars + 4;
+  int *sFm = reinterpret_cast<int *>(bars + 8);
+  unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long vs = a.vs, gs = a.gstride;
+
+  if (tid == 0) {
+    mbar_init(&full[0], 33);
+    mbar_init(&full[1], 33);
+    mbar_init(&empty[0], C::NWC);
+    mbar_init(&empty[1], C::NWC);
+    mbar_init(abar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+
+  auto buf = [&](int b) { return sBuf0 + b * C::S_BUF; };
+
+  // ------------------------------------------------------------- producer
+  if (warp == C::NWC) {
+    if (ASMEM && lane == 0) {
+      mbar_arrive_expect_tx(abar, 8u * C::S_AF);
+      bulk_g2s(sAF, a.AT, 8u * C::S_AF, abar);
+    }
+    int it = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+      const int b = it & 1;
+      if (it >= 2 && !mbar_wait(&empty[b], ((it >> 1) - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      const long e0 = (long)t * E;
+      const int ne = (int)min((long)E, (long)a.K - e0);
+      double *B = buf(b);
+      double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
+      double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
+      if (lane == 0) {
+        mbar_arrive_expect_tx(&full[b], C::TX);
+        for (int v = 0; v < NV; v++) {
+          bulk_g2s(bU + v * E * Np, a.u_in + v * vs + e0 * Np, 8u * E * Np, &full[b]);
+          bulk_g2s(bK + v * E * Np, a.kreg + v * vs + e0 * Np, 8u * E * Np, &full[b]);
+        }
+        for (int m = 0; m < 9; m++) bulk_g2s(bG + m * E, a.geo + m * gs + e0, 8u * E, &full[b]);
+        for (int q = 0; q < 3; q++)
+          bulk_g2s(bF + q * 4 * E, a.nrm + q * 4 * gs + 4 * e0, 32u * E, &full[b]);
+        bulk_g2s(bF + 3 * 4 * E, a.fscale + 4 * e0, 32u * E, &full[b]);
+        bulk_g2s(bF + 4 * 4 * E, a.tau + 4 * e0, 32u * E, &full[b]);
+        if (PHYS != EUL)
+          for (int q = 0; q < 3; q++)
+            bulk_g2s(bV + q * E * Np, a.vel + q * vs + e0 * Np, 8u * E * Np, &full[b]);
+      }
+      // neighbour traces u+ = u[vmapP] into [v][fj][e]
+      for (int idx = lane; idx < ne * NFF; idx += 32) {
+        const long vm = __ldg(a.vmapP + e0 * NFF + idx);
+        const int e = idx / NFF, fj = idx - e * NFF;
+#pragma unroll
+        for (int v = 0; v < NV; v++) cp_async8(bUP + (v * NFF + fj) * E + e, a.u_in + v * vs + vm);
+      }
+      cp_async_arrive_noinc(&full[b]);
+    }
+    if (!ok) atomicOr(&a.sc->flags, 4);
+    // let the copies of the last two tiles settle before this warp leaves
+    for (int j = (it > 2 ? it - 2 : 0); j < it; j++) mbar_wait(&full[j & 1], (j >> 1) & 1);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    return;
+  }
+
+  // ------------------------------------------------------------ consumers
+  double acc[C::WM][C::WN][2];
+  const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
+  unsigned long long vmax = 0ull;
+  bool ok = true;
+  if (ASMEM) ok = consumer_all(mbar_wait(abar, 0), TC);
+  const double *Afrag = ASMEM ? sAF : a.AT;
+  int it = 0;
+  for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, it++) {
+    const int b = it & 1;
+    if (!consumer_all(mbar_wait(&full[b], (it >> 1) & 1), TC)) {
+      ok = false;
+      break;
+    }
+    const long e0 = (long)t * E;
+    const int ne = (int)min((long)E, (long)a.K - e0);
+    double *B = buf(b);
+    double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
+    double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
+
+    // 1. volume fluxes -> sB rows [0, 3Np), zero padding rows
+    for (int itm = tid; itm < E * Np; itm += TC) {
+      const int i = itm / E, e = itm - i * E;
+      const double *g = bG + e;
+      const double rx = g[0], ry = g[E], rz = g[2 * E], sx = g[3 * E], sy = g[4 * E],
+                   sz = g[5 * E], tx = g[6 * E], ty = g[7 * E], tz = g[8 * E];
+      if (PHYS == EUL) {
+        double q[5], F[5], Gf[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
+        euler_flux_fast(a.gamma, q, F, Gf, W);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const int col = v * E + e;
+          sB[(0 * Np + i) * BLD + col] = rx * F[v] + ry * Gf[v] + rz * W[v];
+          sB[(1 * Np + i) * BLD + col] = sx * F[v] + sy * Gf[v] + sz * W[v];
+          sB[(2 * Np + i) * BLD + col] = tx * F[v] + ty * Gf[v] + tz * W[v];
+        }
+      } else {
+        const double uu = bU[e * Np + i];
+        const double F = bV[e * Np + i] * uu, Gf = bV[E * Np + e * Np + i] * uu,
+                     W = bV[2 * E * Np + e * Np + i] * uu;
+        sB[(0 * Np + i) * BLD + e] = rx * F + ry * Gf + rz * W;
+        sB[(1 * Np + i) * BLD + e] = sx * F + sy * Gf + sz * W;
+        sB[(2 * Np + i) * BLD + e] = tx * F + ty * Gf + tz * W;
+      }
+    }
+    for (int g = tid; g < (C::KVP - C::KV) * BLD; g += TC) sB[C::KV * BLD + g] = 0.0;
+    consumer_sync(TC);
+
+    // 2. volume contraction
+#pragma unroll
+    for (int i = 0; i < C::WM; i++)
+#pragma unroll
+      for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    {
+      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
+      const int m0 = mg * C::WM, n0 = ng * C::WN;
+      const double *Ab = Afrag + (long)m0 * 32 + lane;
+      const double *Bb = sB + (lane & 3) * BLD + n0 * 8 + (lane >> 2);
+#pragma unroll 2
+      for (int ks = 0; ks < C::KVP / 4; ks++) {
+        double av[C::WM], bv[C::WN];
+#pragma unroll
+        for (int i = 0; i < C::WM; i++)
+          av[i] = (m0 + i < C::MT) ? Ab[((long)ks * C::MT + i) * 32] : 0.0;
+#pragma unroll
+        for (int j = 0; j < C::WN; j++) bv[j] = Bb[ks * 4 * BLD + j * 8];
+#pragma unroll
+        for (int i = 0; i < C::WM; i++)
+#pragma unroll
+          for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
+      }
+    }
+    consumer_sync(TC);
+
+    // 3. face fluxes -> sB rows [0, NFF)
+    for (int itm = tid; itm < E * NFF; itm += TC) {
+      const int fj = itm / E, e = itm - fj * E, f = fj / Nfp;
+      const int nodeM = sFm[fj];
+      // face arrays arrive in their global order: [array][e][f]
+      const double nx = bF[0 * 4 * E + e * 4 + f], ny = bF[1 * 4 * E + e * 4 + f],
+                   nz = bF[2 * 4 * E + e * 4 + f], fs = bF[3 * 4 * E + e * 4 + f],
+                   tau = bF[4 * 4 * E + e * 4 + f];
+      if (PHYS == EUL) {
+        double qm[5], qb[5], F[5], Gf[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          qm[v] = bU[v * E * Np + e * Np + nodeM];
+          qb[v] = 0.5 * (qm[v] + bUP[(v * NFF + fj) * E + e]);
+        }
+        euler_flux_fast(a.gamma, qb, F, Gf, W);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];
+          sB[fj * BLD + v * E + e] = (nd - tau * (qb[v] - qm[v])) * fs;
+        }
+      } else {
+        const double um = bU[e * Np + nodeM];
+        const double ub = 0.5 * (um + bUP[fj * E + e]);
+        const double F = bV[e * Np + nodeM] * ub, Gf = bV[E * Np + e * Np + nodeM] * ub,
+                     W = bV[2 * E * Np + e * Np + nodeM] * ub;
+        const double nd = nx * F + ny * Gf + nz * W;
+        sB[fj * BLD + e] = (nd - tau * (ub - um)) * fs;
+      }
+    }
+    for (int g = tid; g < (C::KFP - C::KF) * BLD; g += TC) sB[C::KF * BLD + g] = 0.0;
+    consumer_sync(TC);
+
+    // 4. lift contraction
+    {
+      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
+      const int m0 = mg * C::WM, n0 = ng * C::WN;
+      const double *Ab = Afrag + ((long)(C::KVP / 4) * C::MT + m0) * 32 + lane;
+      const double *Bb = sB + (lane & 3) * BLD + n0 * 8 + (lane >> 2);
+#pragma unroll 2
+      for (int ks = 0; ks < C::KFP / 4; ks++) {
+        double av[C::WM], bv[C::WN];
+#pragma unroll
+        for (int i = 0; i < C::WM; i++)
+          av[i] = (m0 + i < C::MT) ? Ab[((long)ks * C::MT + i) * 32] : 0.0;
+#pragma unroll
+        for (int j = 0; j < C::WN; j++) bv[j] = Bb[ks * 4 * BLD + j * 8];
+#pragma unroll
+        for (int i = 0; i < C::WM; i++)
+#pragma unroll
+          for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
+      }
+    }
+    consumer_sync(TC);
+
+    // 5. epilogue: rhs -> sB as [v][i][EP], then the coalesced LSERK update
+    {
+      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
+#pragma unroll
+      for (int ii = 0; ii < C::WM; ii++) {
+        const int i = (mg * C::WM + ii) * 8 + (lane >> 2);
+        if (i < Np) {
+#pragma unroll
+          for (int jj = 0; jj < C::WN; jj++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int col = (ng * C::WN + jj) * 8 + (lane & 3) * 2 + h;
+              const int v = col / E, e = col - v * E;
+              sB[(v * Np + i) * EP + e] = acc[ii][jj][h];
+            }
+        }
+      }
+    }
+    consumer_sync(TC);
+    for (int v = 0; v < NV; v++) {
+      const long base = v * vs + e0 * Np;
+      for (int g = tid; g < ne * Np; g += TC) {
+        const int e = g / Np, i = g - e * Np;
+        const double rhs = sB[(v * Np + i) * EP + e];
+        if (a.rhs_only) {
+          a.u_out[base + g] = rhs;
+        } else {
+          const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
+          const double un = bU[v * E * Np + g] + a.rkb * kn;
+          a.kreg[base + g] = kn;
+          a.u_out[base + g] = un;
+          bU[v * E * Np + g] = un;
+        }
+      }
+    }
+    if (PHYS == EUL && a.last_stage && !a.rhs_only) {
+      consumer_sync(TC);
+      // fused calc_maxv on the new state
+      for (int itm = tid; itm < 4 * E; itm += TC) {
+        const int f = itm / E, e = itm - f * E;
+        if (e >= ne) continue;
+        double mv2 = 0.0, mc2 = 0.0;
+        bool bad = false;
+        for (int j = 0; j < Nfp; j++) {
+          const int nd = e * Np + sFm[f * Nfp + j];
+          const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
+                       u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
+          const double ir = 1.0 / u1;
+          const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
+          const double v2 = vx * vx + vy * vy + vz * vz;
+          mv2 = v2 > mv2 ? v2 : mv2;
+          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
+          const double c2 = fabs(a.gamma * pres * ir);
+          mc2 = c2 > mc2 ? c2 : mc2;
+          bad |= (v2 != v2) || (c2 != c2);
+        }
+        double mv = sqrt(mv2) + sqrt(mc2);
+        if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+        a.maxv[(e0 + e) * 4 + f] = mv;
+        const unsigned long long bits = dbits(mv * bF[3 * 4 * E + e * 4 + f]);
+        vmax = bits > vmax ? bits : vmax;
+      }
+    }
+    // release the buffer (generic-proxy writes into it precede the next TMA)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[b]);
+  }
+  if (!ok && tid == 0) atomicOr(&a.sc->flags, 4);
+  if (PHYS == EUL && a.last_stage && !a.rhs_only) {
+    vmax = warp_max_bits(vmax);
+    if (lane == 0) sMax[warp] = vmax;
+    consumer_sync(TC);
+    if (tid < 32) {
+      unsigned long long v = tid < C::NWC ? sMax[tid] : 0ull;
+      v = warp_max_bits(v);
+      if (tid == 0) atomicMax(&a.sc->acc[a.sc->parity ^ 1], v);
+    }
+  }
+}

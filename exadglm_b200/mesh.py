@@ -242,6 +242,21 @@ class Mesh3D:
             vmapF[ee, ff] = e2 * 4 + f2
         return vmapM.astype(np.int32), vmapP.astype(np.int32), vmapF.astype(np.int32)
 
+    def calc_spatial_h(self, verbose=0):
+        """min and max over elements of the inscribed-sphere diameter
+        6 V / (total face area) (mesh_3d_core.cpp:444-465)."""
+        V = self.box.VXYZ[self.box.EtoV.astype(np.int64)]            # (K,4,3)
+        vol = np.abs(np.einsum("ki,ki->k", V[:, 1] - V[:, 0],
+                               np.cross(V[:, 2] - V[:, 0], V[:, 3] - V[:, 0]))) / 6
+        area = np.zeros(len(V))
+        for f in FACE_VERTS:
+            a, b, c = V[:, f[0]], V[:, f[1]], V[:, f[2]]
+            area += 0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1)
+        h = 6 * vol / area
+        if verbose >= 1:
+            print(f"min(h) ={h.min():1.5f}, max(h) ={h.max():1.5f}")
+        return h.min(), h.max()
+
     # -- arrays in the datain layout --------------------------------------
     def datain_arrays(self):
         """Dict of every mesh array the solver reads, named as the

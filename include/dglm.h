@@ -133,6 +133,14 @@ dglm_status dglm_get_dt_history(dglm_handle *h, int first, int count, double *dt
  * (nvar device pointers), with maxv/tau taken from u as runRK does at the
  * start of a step. */
 dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs);
+/* Tile shapes ("variants") of the fused stage kernel compiled for (physics,
+ * N); variant 0 is the default.  dglm_variant_describe writes a one-line
+ * description such as "dmma E=16 WN=2 WM=5 threads=160 smem=104000". */
+int dglm_variant_count(int physics, int N);
+dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, size_t len);
+/* Selects the variant used by the handle (rebuilds the operator layout). */
+dglm_status dglm_set_variant(dglm_handle *h, int variant);
+int dglm_get_variant(dglm_handle *h);
 /* Number of kernels the last dglm_step call launched (for accounting). */
 long dglm_kernel_launches(dglm_handle *h);
 /* Device bytes held by the handle. */

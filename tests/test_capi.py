@@ -1,0 +1,93 @@
+"""C ABI host logic (no GPU needed): libdglm.so loads, exports every function
+include/dglm.h declares, and rejects bad arguments with status codes before
+touching a device."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from exadglm_b200 import capi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "dglm.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dglm_[A-Za-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(names) == set(capi.EXPORTS)
+
+
+def test_abi_version_and_orders():
+    L = capi.lib()
+    assert L.dglm_abi_version() == 1
+    assert all(L.dglm_order_supported(n) for n in range(1, 9))
+    assert not L.dglm_order_supported(0) and not L.dglm_order_supported(9)
+
+
+def test_variants_are_described():
+    for phys in ("euler", "advection"):
+        for N in range(1, 9):
+            v = capi.variants(phys, N)
+            assert len(v) >= 2
+            assert all(d.startswith(("simt", "dmma")) for d in v)
+
+
+def _desc(**kw):
+    d = capi.Desc()
+    d.N, d.physics, d.K, d.precision = 4, capi.EULER, 48, capi.PREC_FP64
+    d.cfl, d.gamma, d.tau_scale, d.tmax, d.device = 0.4, 1.4, 1.2, 1.0, 0
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return d
+
+
+@pytest.mark.parametrize("kw,status", [
+    ({"N": 0}, capi.ERR_UNSUPPORTED), ({"N": 9}, capi.ERR_UNSUPPORTED),
+    ({"physics": 7}, capi.ERR_INVALID), ({"K": 0}, capi.ERR_INVALID),
+    ({"cfl": -1.0}, capi.ERR_INVALID), ({"gamma": 1.0}, capi.ERR_INVALID),
+    ({"tmax": 0.0}, capi.ERR_INVALID),
+])
+def test_create_rejects_bad_descriptions(kw, status):
+    L = capi.lib()
+    h = C.c_void_p()
+    assert L.dglm_create(C.byref(_desc(**kw)), C.byref(h)) == status
+    assert not h.value
+    assert L.dglm_last_error()
+
+
+def test_null_arguments():
+    L = capi.lib()
+    assert L.dglm_create(None, None) == capi.ERR_INVALID
+    assert L.dglm_step(None, 1) == capi.ERR_INVALID
+    assert L.dglm_set_state(None, None, 0) == capi.ERR_INVALID
+    assert L.dglm_destroy(None) == capi.OK
+
+
+def test_per_kernel_entry_points_validate_before_launch():
+    L = capi.lib()
+    null = C.c_void_p(0)
+    # bad order / nvar / NULL pointers are rejected without a launch
+    assert L.dglm_update_ub(0, 5, 10, null, null, null, null, null) == capi.ERR_INVALID
+    assert L.dglm_update_ub(4, 3, 10, null, null, null, null, null) == capi.ERR_INVALID
+    assert L.dglm_lserk_stage(4, 5, 10, 0.1, 0.0, 0.1, null, null, null, null) == capi.ERR_INVALID
+    assert L.dglm_update_rhs(4, 5, 10, null, null, null, null, b"x", null, null, null, null,
+                             null, null) == capi.ERR_INVALID
+    assert L.dglm_calc_dt(4, 0, 0.4, null, null, null) == capi.ERR_INVALID
+
+
+def test_library_fails_loudly_when_missing(monkeypatch):
+    monkeypatch.setattr(capi, "LIB_PATH", "/nonexistent/libdglm.so")
+    monkeypatch.setattr(capi, "_lib", None)
+    with pytest.raises(RuntimeError, match="missing"):
+        capi.lib()

@@ -118,3 +118,19 @@ def test_state_roundtrip_and_restart():
     s.step(4)
     assert rel(s.get_state(), end) < 1e-14
     s.close()
+
+
+@pytest.mark.parametrize("phys,N", [("euler", 4), ("euler", 3), ("euler", 6), ("advection", 3),
+                                    ("advection", 5)])
+def test_every_variant_matches_oracle(phys, N):
+    """Each compiled tile shape (SIMT and FP64 tensor-core DMMA engines) gives
+    the oracle's answer."""
+    from exadglm_b200.capi import variants
+    prob = make(phys, N)
+    uo, _, _, _ = oracle.Oracle(prob).run(3)
+    for v in range(len(variants(phys, N))):
+        s = Solver(prob)
+        s.set_variant(v)
+        s.step(3)
+        assert rel(s.get_state(), uo) < TOL_STATE, (v, variants(phys, N)[v])
+        s.close()

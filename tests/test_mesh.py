@@ -1,0 +1,82 @@
+"""Mesh arrays against the reference Mesh3D (tests/golden/mesh.npz, made from
+the reference's own mesh code with its C++ cores rebuilt from source) and
+the geometric properties its tests check (dim3/tests/test_uniform_3d_single.py,
+test_mesh_3d_common.py, test_mesh_3d_serial_uniform_pbc.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from exadglm_b200.mesh import Mesh3D, UniformBox, uniform_mesh
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "mesh.npz"))
+CASES = {"pbc": {"x": "pbc", "y": "pbc", "z": "pbc"},
+         "mixed": {"x": "bc1", "y": "pbc", "z": "bc2"}}
+
+
+def build(tag):
+    nx, ny, nz = (int(v) for v in GOLD[f"{tag}_dims"])
+    return Mesh3D(int(GOLD[f"{tag}_N"]), UniformBox(nx, ny, nz, bc=CASES[tag]))
+
+
+@pytest.mark.parametrize("tag", ["pbc", "mixed"])
+def test_index_arrays_identical(tag):
+    m = build(tag)
+    for name in ("EtoV", "vmapM", "vmapP", "vmapF", "EtoB"):
+        np.testing.assert_array_equal(getattr(m, name), GOLD[f"{tag}_{name}"], err_msg=name)
+    # EtoE agrees wherever the reference has a neighbour
+    ref = GOLD[f"{tag}_EtoE"]
+    np.testing.assert_array_equal(m.EtoE[ref >= 0], ref[ref >= 0])
+
+
+@pytest.mark.parametrize("tag", ["pbc", "mixed"])
+def test_geometry_matches(tag):
+    m = build(tag)
+    for name in ("PX", "PY", "PZ", "J", "rx", "ry", "rz", "sx", "sy", "sz", "tx", "ty", "tz",
+                 "NX", "NY", "NZ", "sJ", "Fscale"):
+        np.testing.assert_allclose(getattr(m, name), GOLD[f"{tag}_{name}"], rtol=0,
+                                   atol=1e-15 * max(1.0, np.abs(GOLD[f"{tag}_{name}"]).max()),
+                                   err_msg=name)
+
+
+@pytest.mark.parametrize("N,n", [(1, 2), (3, 3), (4, 4)])
+def test_vmapP_involution_and_coincidence(N, n):
+    """vmapP points to a coincident node (mod the period) and is an
+    involution on a periodic mesh."""
+    m = uniform_mesh(N, n)
+    vM, vP = m.vmapM.ravel(), m.vmapP.ravel()
+    x = np.stack([m.PX.ravel(), m.PY.ravel(), m.PZ.ravel()], axis=1)
+    d = x[vM] - x[vP]
+    d -= np.round(d)                      # unit period
+    assert np.abs(d).max() < 1e-12
+    # per face pair: if node j of face (e,f) maps to position j' of the
+    # neighbour face (e',f'), then j' maps back to j
+    K, Nfp = m.Nelem, m.Nfp
+    VM, VP = m.vmapM.reshape(K * 4, Nfp), m.vmapP.reshape(K * 4, Nfp)
+    nb = m.vmapF.ravel()
+    pos = np.argmax(VM[nb][:, None, :] == VP[:, :, None], axis=2)   # (4K, Nfp) -> j'
+    back = VP[nb][np.arange(4 * K)[:, None], pos]
+    np.testing.assert_array_equal(back, VM)
+    F = m.vmapF.ravel()
+    np.testing.assert_array_equal(F[F], np.arange(F.size))
+
+
+def test_volume_and_normals():
+    m = uniform_mesh(3, 3)
+    assert (m.J * 4.0 / 3.0).sum() == pytest.approx(1.0, rel=1e-14)   # unit cube
+    n = np.stack([m.NX, m.NY, m.NZ], axis=-1)
+    np.testing.assert_allclose(np.linalg.norm(n, axis=-1), 1.0, rtol=1e-15)
+    # neighbouring faces have opposite normals
+    F = m.vmapF.ravel()
+    nf = n.reshape(-1, 3)
+    np.testing.assert_allclose(nf + nf[F], 0.0, atol=1e-14)
+
+
+def test_element_counts():
+    b = UniformBox(7, 7, 7)
+    assert b.Nelem == 1296 and b.EtoV.shape == (1296, 4)
+
+
+def test_rejects_degenerate_periodic_axis():
+    with pytest.raises(ValueError):
+        UniformBox(2, 4, 4)
