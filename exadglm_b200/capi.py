@@ -110,8 +110,19 @@ def ptr_table(ptrs):
     return arr
 
 
-def variants(physics, N):
-    """Descriptions of the compiled stage-kernel variants for (physics, N)."""
+def variant_precision(desc):
+    """Precision mode of a variant from its description."""
+    if desc.startswith("tcgen05-tf32x3"):
+        return "tf32x3"
+    if desc.startswith("tcgen05-bf16x3"):
+        return "bf16x3"
+    return "fp64"
+
+
+def variants(physics, N, precision=None):
+    """Descriptions of the compiled stage-kernel variants for (physics, N),
+    indexed by variant number; with `precision`, the indices of that mode
+    only are returned as (index, description) pairs."""
     L = lib()
     ph = EULER if physics == "euler" else ADVECTION
     out = []
@@ -119,7 +130,9 @@ def variants(physics, N):
         buf = C.create_string_buffer(128)
         check(L.dglm_variant_describe(ph, N, i, buf, 128))
         out.append(buf.value.decode())
-    return out
+    if precision is None:
+        return out
+    return [(i, d) for i, d in enumerate(out) if variant_precision(d) == precision]
 
 
 def _np_ptr(a):
@@ -132,13 +145,18 @@ class Solver:
     ``state`` arrays are numpy (nvar, K*Np) on the host, or lists of device
     pointers for the on-device variants."""
 
-    def __init__(self, problem, precision="fp64", device=0, matrix_order="c", arrays=None):
+    def __init__(self, problem, precision="fp64", device=0, matrix_order="c", arrays=None,
+                 variant=None):
+        """variant: stage-kernel tile shape; None takes the tuned choice for
+        this device from exadglm_b200/tuned.json when present, a negative
+        value the library default (the first variant of the precision)."""
         self.p = problem
         L = lib()
         d = Desc()
         d.N, d.K = problem.N, problem.K
         d.physics = EULER if problem.physics == "euler" else ADVECTION
         d.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        self.precision = {v: k for k, v in PRECISIONS.items()}[d.precision]
         d.cfl, d.gamma, d.tau_scale, d.tmax = problem.cfl, problem.gamma, problem.tau_scale, \
             problem.tmax
         d.device = device
@@ -169,6 +187,11 @@ class Solver:
         if problem.vel is not None:
             m.vx, m.vy, m.vz = (f64(n, problem.vel[i]) for i, n in enumerate(("vx", "vy", "vz")))
         check(L.dglm_upload_mesh(h, C.byref(m)))
+        if variant is None:
+            from .tune import cached_variant
+            variant = cached_variant(problem.physics, problem.N, self.precision, device)
+        if variant is not None and variant >= 0:
+            self.set_variant(variant)
         self.set_state(problem.u0)
 
     # -- state ------------------------------------------------------------

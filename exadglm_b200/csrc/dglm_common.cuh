@@ -101,7 +101,7 @@ dglm_status set_error(dglm_status s, const std::string &msg);
 dglm_status cuda_check(cudaError_t e, const char *what);
 
 // contraction engines of the fused stage kernel
-enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2 };
+enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3 };
 
 // One compiled tile shape of the fused stage kernel.
 struct StageVariantInfo {
@@ -115,6 +115,10 @@ struct StageVariantInfo {
   int KVP, KFP;  // DMMA: volume / lift k extents padded to 4
   int threads;
   size_t smem;
+  int prec;      // dglm_precision of the contraction (0 FP64, 1 TF32x3, 2 BF16x3)
+  int npad;      // MIXED: MMA N (output nodes, padded)
+  int kva, kfa;  // MIXED: volume / lift K extents of the operand images
+  int bimg;      // MIXED: bytes of the operator image (hi then lo)
 };
 
 // fused FP64 stage launcher (dglm_stage_fp64.cu)

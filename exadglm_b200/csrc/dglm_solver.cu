@@ -149,6 +149,7 @@ StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
 // Doubles of the device operator copy for a variant's layout.
 size_t op_doubles(const StageVariantInfo &v, int Np, int NFF) {
   if (v.mode == MODE_SIMT) return (size_t)(3 * Np + NFF) * v.IP;
+  if (v.mode == MODE_MIXED) return ((size_t)v.bimg + 7) / 8;
   return (size_t)(v.KVP / 4 + v.KFP / 4) * v.MT * 32;
 }
 
@@ -160,6 +161,63 @@ size_t max_op_doubles(int physics, int N, int Np, int NFF) {
   return m;
 }
 
+// Round-to-nearest (ties away) of a float to TF32 (10 mantissa bits), as
+// cvt.rna.tf32.f32 does on the device.
+uint32_t tf32_rna(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+  return u;
+}
+float f32_of(uint32_t u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+// Round-to-nearest-even of a float to bfloat16.
+uint16_t bf16_rne(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+// Operator image of a mixed-precision variant: B = A^T blocks (volume: the
+// 3Np columns of [WDr WDs WDt], lift: the NFF columns of -LIFT), each
+// npad rows x (kva | kfa) K, K-major in 8-row x 16-byte core matrices,
+// split into hi and lo parts: [hi vol][hi lift][lo vol][lo lift].
+std::vector<unsigned char> mixed_image(const dglm_handle *h, const StageVariantInfo &v) {
+  const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
+  const bool tf = v.prec == DGLM_PREC_TF32X3;
+  const int S = tf ? 4 : 2, T = 16 / S;
+  const int bv = v.npad * v.kva * S, bf = v.npad * v.kfa * S;
+  std::vector<unsigned char> img((size_t)v.bimg, 0);
+  auto put = [&](size_t base, int sbo, int r, int k, double x) {
+    const size_t off = base + (size_t)(r / 8) * sbo + (size_t)(k / T) * 128 + (r % 8) * 16 +
+                       (k % T) * S;
+    const size_t lo_base = (size_t)bv + bf;   // lo part follows the hi part
+    if (tf) {
+      const uint32_t hi = tf32_rna((float)x);
+      const uint32_t lo = tf32_rna((float)(x - (double)f32_of(hi)));
+      std::memcpy(&img[off], &hi, 4);
+      std::memcpy(&img[off + lo_base], &lo, 4);
+    } else {
+      const uint16_t hi = bf16_rne((float)x);
+      const uint32_t hb = (uint32_t)hi << 16;
+      const uint16_t lo = bf16_rne((float)(x - (double)f32_of(hb)));
+      std::memcpy(&img[off], &hi, 2);
+      std::memcpy(&img[off + lo_base], &lo, 2);
+    }
+  };
+  for (int n = 0; n < Np; n++) {
+    for (int k = 0; k < KV; k++) put(0, v.kva / T * 128, n, k, h->Ahost[(size_t)n * KA + k]);
+    for (int k = 0; k < NFF; k++)
+      put((size_t)bv, v.kfa / T * 128, n, k, h->Ahost[(size_t)n * KA + KV + k]);
+  }
+  return img;
+}
+
 // Builds the variant's device layout of A = [WDr WDs WDt -LIFT] (Np rows,
 // 3Np + NFF columns) from the host copy and uploads it.
 //   SIMT: k-major with padded rows, AT[k * IP + i] = A(i, k);
@@ -169,6 +227,11 @@ size_t max_op_doubles(int physics, int N, int Np, int NFF) {
 dglm_status upload_operator_layout(dglm_handle *h) {
   const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
   const StageVariantInfo &v = h->vinfo;
+  if (v.mode == MODE_MIXED) {
+    std::vector<unsigned char> img = mixed_image(h, v);
+    return cuda_check(cudaMemcpy(h->AT, img.data(), img.size(), cudaMemcpyHostToDevice),
+                      "operator upload");
+  }
   std::vector<double> out(op_doubles(v, Np, NFF), 0.0);
   auto A = [&](int i, int k) { return h->Ahost[(size_t)i * KA + k]; };
   if (v.mode == MODE_SIMT) {
@@ -231,8 +294,18 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
     return set_error(DGLM_ERR_UNSUPPORTED,
                      "dglm_create: order N=" + std::to_string(d.N) + " is not built (1..8)");
   if (d.K <= 0) return set_error(DGLM_ERR_INVALID, "dglm_create: K must be positive");
-  if (d.precision != DGLM_PREC_FP64)
-    return set_error(DGLM_ERR_UNSUPPORTED, "dglm_create: precision mode not built");
+  if (d.precision != DGLM_PREC_FP64 && d.precision != DGLM_PREC_TF32X3 &&
+      d.precision != DGLM_PREC_BF16X3)
+    return set_error(DGLM_ERR_INVALID, "dglm_create: unknown precision");
+  int first = -1;
+  {
+    StageVariantInfo v{};
+    for (int i = 0; i < stage_variant_count(d.physics, d.N) && first < 0; i++)
+      if (stage_variant_info(d.physics, d.N, i, &v) && v.prec == d.precision) first = i;
+  }
+  if (first < 0)
+    return set_error(DGLM_ERR_UNSUPPORTED,
+                     "dglm_create: precision mode not built for this physics and order");
   if (!(d.cfl > 0) || !(d.tau_scale >= 0) || !(d.tmax > 0) ||
       (d.physics == DGLM_EULER && !(d.gamma > 1)))
     return set_error(DGLM_ERR_INVALID, "dglm_create: cfl/gamma/tau_scale/tmax out of range");
@@ -249,8 +322,8 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   h->Np = np_of(d.N);
   h->Nfp = nfp_of(d.N);
   h->NFF = 4 * h->Nfp;
-  h->variant = 0;
-  stage_variant_info(d.physics, d.N, 0, &h->vinfo);
+  h->variant = first;
+  stage_variant_info(d.physics, d.N, first, &h->vinfo);
   // per-element arrays are padded to whole 64-element tiles (zero-filled) so
   // that every tile copy of the pipelined kernel is in bounds and aligned
   h->Kp = ((long)d.K + 63) / 64 * 64;
@@ -616,9 +689,13 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
   if (v.mode == MODE_SIMT)
     snprintf(buf, len, "simt E=%d R=%d CPT=%d threads=%d smem=%zu", v.E, v.R, v.CPT, v.threads,
              v.smem);
-  else
-    snprintf(buf, len, "dmma E=%d WN=%d WM=%d threads=%d smem=%zu", v.E, v.CPT, v.WM,
+  else if (v.mode == MODE_MIXED)
+    snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
+             v.prec == DGLM_PREC_TF32X3 ? "tcgen05-tf32x3" : "tcgen05-bf16x3", v.E, v.npad,
              v.threads, v.smem);
+  else
+    snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu",
+             v.mode == MODE_PIPE ? "pipe-dmma" : "dmma", v.E, v.CPT, v.WM, v.threads, v.smem);
   return DGLM_OK;
 }
 
@@ -627,6 +704,8 @@ dglm_status dglm_set_variant(dglm_handle *h, int variant) {
   StageVariantInfo v{};
   if (!stage_variant_info(h->d.physics, h->d.N, variant, &v))
     return set_error(DGLM_ERR_INVALID, "dglm_set_variant: no such variant");
+  if (v.prec != h->d.precision)
+    return set_error(DGLM_ERR_INVALID, "dglm_set_variant: variant is of another precision");
   DeviceGuard g(h->dev);
   cudaStreamSynchronize(h->stream);
   drop_graphs(h);

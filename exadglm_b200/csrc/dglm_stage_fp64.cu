@@ -411,6 +411,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>::THREADS
 }
 
 #include "dglm_stage_pipe.cuh"
+#include "dglm_stage_mixed.cuh"
 
 // Standalone calc_maxv (initial state, advection velocity): maxv per face and
 // a device-wide max of maxv*Fscale into sc->acc[slot].
@@ -569,6 +570,35 @@ static Variant make_pipe() {
   return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS>};
 }
 
+template <int PHYS, int N, int E, int PREC>
+static cudaError_t launch_mixed(const StageArgs &a, cudaStream_t s) {
+  using C = MCfg<PHYS, N, E, PREC>;
+  auto k = stage_mixed_kernel<PHYS, N, E, PREC>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int ntiles = (a.K + E - 1) / E;
+  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  k<<<grid, C::THREADS, C::SMEM, s>>>(a, ntiles);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E, int PREC>
+static Variant make_mixed() {
+  using C = MCfg<PHYS, N, E, PREC>;
+  StageVariantInfo i{};
+  i.mode = MODE_MIXED;
+  i.E = E;
+  i.threads = C::THREADS;
+  i.smem = C::SMEM;
+  i.prec = PREC == PREC_TF32 ? DGLM_PREC_TF32X3 : DGLM_PREC_BF16X3;
+  i.npad = C::NPAD;
+  i.kva = C::KVA;
+  i.kfa = C::KFA;
+  i.bimg = C::BIMG;
+  return Variant{i, &launch_mixed<PHYS, N, E, PREC>};
+}
+
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM>
 static Variant make_v() {
   using C = Cfg<PHYS, N, MODE, E, R, CPT, WM>;
@@ -596,6 +626,8 @@ static const std::vector<Variant> &variants();
 #define V_SIMT(P, NN, E, R, C) make_v<P, NN, MODE_SIMT, E, R, C, 1>()
 #define V_DMMA(P, NN, E, WN, WM) make_v<P, NN, MODE_DMMA, E, 1, WN, WM>()
 #define V_PIPE(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS>()
+#define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
+#define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -607,19 +639,20 @@ DGLM_VARIANTS(EUL, 1, V_SIMT(EUL, 1, 128, 4, 5), V_DMMA(EUL, 1, 64, 4, 1))
 DGLM_VARIANTS(EUL, 2, V_SIMT(EUL, 2, 64, 5, 5), V_DMMA(EUL, 2, 32, 4, 2))
 DGLM_VARIANTS(EUL, 3, V_DMMA(EUL, 3, 16, 2, 3), V_SIMT(EUL, 3, 32, 5, 5),
               V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true))
-DGLM_VARIANTS(EUL, 4, V_DMMA(EUL, 4, 8, 1, 5), V_SIMT(EUL, 4, 16, 5, 5),
-              V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5), V_DMMA(EUL, 4, 16, 2, 5),
-              V_PIPE(EUL, 4, 8, 1, 5, true), V_PIPE(EUL, 4, 8, 1, 5, false),
-              V_PIPE(EUL, 4, 8, 1, 3, true))
-DGLM_VARIANTS(EUL, 5, V_DMMA(EUL, 5, 8, 1, 7), V_SIMT(EUL, 5, 8, 7, 5),
-              V_PIPE(EUL, 5, 8, 1, 7, false))
+DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
+              V_SIMT(EUL, 4, 16, 5, 5), V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5),
+              V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
+              V_PIPE(EUL, 4, 8, 1, 5, false), V_PIPE(EUL, 4, 8, 1, 3, true),
+              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8))
+DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
+              V_SIMT(EUL, 5, 8, 7, 5))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 DGLM_VARIANTS(EUL, 8, V_DMMA(EUL, 8, 8, 1, 7), V_SIMT(EUL, 8, 4, 8, 5))
 DGLM_VARIANTS(ADV, 1, V_SIMT(ADV, 1, 256, 4, 4), V_DMMA(ADV, 1, 64, 2, 1))
 DGLM_VARIANTS(ADV, 2, V_SIMT(ADV, 2, 128, 5, 4), V_DMMA(ADV, 2, 64, 2, 2))
-DGLM_VARIANTS(ADV, 3, V_SIMT(ADV, 3, 64, 5, 4), V_DMMA(ADV, 3, 64, 2, 3),
-              V_PIPE(ADV, 3, 32, 1, 3, true))
+DGLM_VARIANTS(ADV, 3, V_DMMA(ADV, 3, 64, 2, 3), V_SIMT(ADV, 3, 64, 5, 4),
+              V_PIPE(ADV, 3, 32, 1, 3, true), V_TF32(ADV, 3, 32), V_BF16(ADV, 3, 32))
 DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5))
 DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7))
 DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6))

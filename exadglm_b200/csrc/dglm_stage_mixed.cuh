@@ -1,0 +1,448 @@
+// Mixed-precision stage kernel on the 5th-generation tensor cores (included
+// by dglm_stage_fp64.cu after dglm_stage_pipe.cuh, inside namespace dglm).
+//
+// Same persistent, TMA-fed pipeline as stage_pipe_kernel; only the two
+// contractions change.  The volume block ([WDr WDs WDt] x [fluxR; fluxS;
+// fluxT]) and the lift block (-LIFT x fluxLM) run as tcgen05.mma with
+//   D[m][n] += A[m][k] * B[n][k],   m = (variable, element), n = output node,
+// A = the tile's fluxes, B = the operator, both K-major in shared memory in
+// the no-swizzle core-matrix layout (8 rows x 16 bytes), the accumulator D
+// (FP32) in tensor memory.  Every FP64 operand x is split as x = hi + lo
+// (hi = x rounded to TF32 or BF16, lo = the rounding error rounded again) and
+// the product is taken in three passes, hi*hi + hi*lo + lo*hi, accumulating
+// in FP32.  Fluxes, the LSERK state and update, metrics and face data stay
+// FP64; only the contraction operands and its accumulator are reduced.
+//
+// Per tile: flux phase writes the volume operand -> one thread issues the
+// volume MMAs and commits to an mbarrier -> once they have read the operand
+// the face phase overwrites it with the lift operand -> lift MMAs -> the
+// accumulator is read back with tcgen05.ld into the FP64 epilogue.  The K
+// range is spread over NACC tensor-memory accumulators (a slice of k-steps
+// each) that are summed in FP64 on read-back, so each FP32 running sum covers
+// only a slice of the terms.
+#pragma once
+
+#include <cuda_bf16.h>
+
+enum { PREC_BF16 = 1, PREC_TF32 = 2 };
+
+// ---- tcgen05 / TMEM helpers ------------------------------------------------
+__device__ __forceinline__ void tmem_alloc(unsigned *dst_smem, unsigned ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(unsigned long long *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+template <int PREC>
+__device__ __forceinline__ void tc_mma(unsigned dtmem, unsigned long long adesc,
+                                       unsigned long long bdesc, unsigned idesc, int accum) {
+  if (PREC == PREC_TF32)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+}
+// 32 lanes x 8 columns of 32-bit accumulator per warp
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float (&r)[8]) {
+  unsigned v[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7])
+      : "r"(taddr)
+      : "memory");
+  for (int i = 0; i < 8; i++) r[i] = __uint_as_float(v[i]);
+}
+__device__ __forceinline__ void tmem_ld_wait() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle, core matrices of 8
+// rows x 16 bytes; lbo = byte step between the two K core matrices of one
+// MMA, sbo = byte step between 8-row groups; version field 1 (sm_100)
+__device__ __forceinline__ unsigned long long smem_desc(unsigned saddr, unsigned lbo,
+                                                        unsigned sbo) {
+  return (unsigned long long)((saddr >> 4) & 0x3FFFu) |
+         ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// x = hi + lo with hi, lo in the operand format (stored as raw bits)
+__device__ __forceinline__ void split_tf32(double x, unsigned &hi, unsigned &lo) {
+  const float f = (float)x;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(f));
+  const float r = (float)(x - (double)__uint_as_float(hi));
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+__device__ __forceinline__ void split_bf16(double x, unsigned short &hi, unsigned short &lo) {
+  const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+  const __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+  hi = __bfloat16_as_ushort(h);
+  lo = __bfloat16_as_ushort(l);
+}
+
+template <int PHYS, int N, int E_, int PREC>
+struct MCfg {
+  static constexpr int NV = PHYS == EUL ? 5 : 1;
+  static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
+  static constexpr int E = E_, EP = E_ + 1, NCOL = NV * E;
+  static constexpr int M = NCOL <= 64 ? 64 : 128;            // MMA rows
+  static constexpr int NPAD = M == 64 ? (Np + 7) / 8 * 8 : (Np + 15) / 16 * 16;   // MMA N
+  // NACC accumulators, each summing the terms of a slice of K in FP32; the
+  // slices are added in FP64 when the tile is read back
+  static constexpr int S = PREC == PREC_TF32 ? 4 : 2;         // operand bytes
+  static constexpr int T = 16 / S;                              // elements per core row
+  static constexpr int KSTEP = 32 / S;                          // K per MMA
+  static constexpr int KV = 3 * Np, KVA = (KV + KSTEP - 1) / KSTEP * KSTEP;
+  static constexpr int KF = NFF, KFA = (KF + KSTEP - 1) / KSTEP * KSTEP;
+  static constexpr int KAM = KVA > KFA ? KVA : KFA;
+  static constexpr int KSV = KVA / KSTEP, KSF = KFA / KSTEP, KST = KSV + KSF;   // k-steps
+  // every accumulator receives at least one k-step, and they fit in 512 columns
+  static constexpr int NACC0 = NPAD * 8 <= 512 ? 8 : NPAD * 4 <= 512 ? 4 : 2;
+  static constexpr int NACC = NACC0 < KST ? NACC0 : KST;
+  static constexpr int TCOLS = NACC * NPAD <= 32 ? 32 : NACC * NPAD <= 64 ? 64
+                               : NACC * NPAD <= 128 ? 128 : NACC * NPAD <= 256 ? 256 : 512;
+  static constexpr int SBO_A = KAM / T * 128, SBO_BV = KVA / T * 128, SBO_BF = KFA / T * 128;
+  // byte sizes
+  static constexpr int A_BYTES = M * KAM * S;                   // one part (hi or lo)
+  static constexpr int BV_BYTES = NPAD * KVA * S, BF_BYTES = NPAD * KFA * S;
+  static constexpr int BIMG = 2 * (BV_BYTES + BF_BYTES);        // hi then lo
+  static constexpr int NWC = 8, TC = 32 * NWC, THREADS = TC + 32;
+  // FP64 pipeline buffers (as in PCfg)
+  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
+  static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
+  static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
+  static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
+  static constexpr int S_R = NV * Np * EP;
+  static constexpr size_t SMEM = (size_t)BIMG + 2 * A_BYTES +
+                                 sizeof(double) * (2 * (size_t)S_BUF + S_R) + 1024;
+  static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE + S_VEL);
+  // instruction descriptor: F32 accumulate, A/B format, K-major A and B, N, M
+  static constexpr unsigned IDESC = (1u << 4) | ((PREC == PREC_TF32 ? 2u : 1u) << 7) |
+                                    ((PREC == PREC_TF32 ? 2u : 1u) << 10) |
+                                    ((unsigned)(NPAD >> 3) << 17) | ((unsigned)(M >> 4) << 24);
+  static_assert(NCOL <= 128, "one MMA tile covers at most 128 columns");
+  static_assert(BIMG % 16 == 0 && A_BYTES % 16 == 0, "16-byte operand images");
+  static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
+  static_assert(NPAD <= 256, "MMA N limit");
+  static_assert(NACC * NPAD <= 512, "tensor memory has 512 columns");
+};
+
+// byte offset of element (r, k) in a K-major core-matrix image with 8-row
+// group stride sbo
+template <class C>
+__device__ __forceinline__ int core_off(int r, int k, int sbo) {
+  return (r >> 3) * sbo + (k / C::T) * 128 + (r & 7) * 16 + (k % C::T) * C::S;
+}
+
+template <class C, int PREC>
+__device__ __forceinline__ void put_split(unsigned char *Ahi, unsigned char *Alo, int r, int k,
+                                          double x) {
+  const int off = core_off<C>(r, k, C::SBO_A);
+  if (PREC == PREC_TF32) {
+    unsigned h, l;
+    split_tf32(x, h, l);
+    *reinterpret_cast<unsigned *>(Ahi + off) = h;
+    *reinterpret_cast<unsigned *>(Alo + off) = l;
+  } else {
+    unsigned short h, l;
+    split_bf16(x, h, l);
+    *reinterpret_cast<unsigned short *>(Ahi + off) = h;
+    *reinterpret_cast<unsigned short *>(Alo + off) = l;
+  }
+}
+
+template <int PHYS, int N, int E_, int PREC>
+__global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC>::THREADS, 1)
+    stage_mixed_kernel(const StageArgs a, int ntiles) {
+  using C = MCfg<PHYS, N, E_, PREC>;
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+                TC = C::TC;
+  extern __shared__ __align__(16) double smem[];
+  unsigned char *sBimg = reinterpret_cast<unsigned char *>(smem);
+  unsigned char *sAhi = sBimg + C::BIMG, *sAlo = sAhi + C::A_BYTES;
+  double *sBuf0 = reinterpret_cast<double *>(sAlo + C::A_BYTES);
+  double *sR = sBuf0 + 2 * C::S_BUF;
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(sR + C::S_R);
+  unsigned long long *full = bars, *empty = bars + 2, *abar = bars + 4, *mbar = bars + 5;
+  unsigned *sTmem = reinterpret_cast<unsigned *>(bars + 6);
+  int *sFm = reinterpret_cast<int *>(bars + 8);
+  unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long vs = a.vs;
+
+  if (tid == 0) {
+    mbar_init(&full[0], 33);
+    mbar_init(&full[1], 33);
+    mbar_init(&empty[0], C::NWC);
+    mbar_init(&empty[1], C::NWC);
+    mbar_init(abar, 1);
+    mbar_init(mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
+  // zero both operand parts once: padding rows and K columns stay zero
+  for (int i = tid; i < 2 * C::A_BYTES / 16; i += C::THREADS)
+    reinterpret_cast<uint4 *>(sAhi)[i] = make_uint4(0, 0, 0, 0);
+  if (warp == 0) tmem_alloc(sTmem, C::TCOLS);
+  tc_fence_before();
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = *sTmem;
+
+  if (warp == C::NWC) {
+    pipe_producer<C, PHYS>(a, ntiles, sBimg, sBuf0, full, empty, abar, C::BIMG, lane);
+    return;
+  }
+
+  const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
+  const unsigned aHi = smem_u32(sAhi), aLo = smem_u32(sAlo);
+  const unsigned bHiV = smem_u32(sBimg), bHiF = bHiV + C::BV_BYTES;
+  const unsigned bLoV = bHiF + C::BF_BYTES, bLoF = bLoV + C::BV_BYTES;
+  unsigned long long vmax = 0ull;
+  bool ok = consumer_all(mbar_wait(abar, 0), TC);
+  int it = 0, mma_phase = 0;
+  for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, it++) {
+    const int b = it & 1;
+    if (!consumer_all(mbar_wait(&full[b], (it >> 1) & 1), TC)) {
+      ok = false;
+      break;
+    }
+    const long e0 = (long)t * E;
+    const int ne = (int)min((long)E, (long)a.K - e0);
+    double *B = sBuf0 + b * C::S_BUF;
+    double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
+    double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
+
+    // 1. volume fluxes -> operand rows m = v*E + e, k = d*Np + i
+    for (int itm = tid; itm < E * Np; itm += TC) {
+      const int i = itm / E, e = itm - i * E;
+      const double *g = bG + e;
+      const double rx = g[0], ry = g[E], rz = g[2 * E], sx = g[3 * E], sy = g[4 * E],
+                   sz = g[5 * E], tx = g[6 * E], ty = g[7 * E], tz = g[8 * E];
+      if (PHYS == EUL) {
+        double q[5], F[5], Gf[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
+        euler_flux_fast(a.gamma, q, F, Gf, W);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const int m = v * E + e;
+          put_split<C, PREC>(sAhi, sAlo, m, i, rx * F[v] + ry * Gf[v] + rz * W[v]);
+          put_split<C, PREC>(sAhi, sAlo, m, Np + i, sx * F[v] + sy * Gf[v] + sz * W[v]);
+          put_split<C, PREC>(sAhi, sAlo, m, 2 * Np + i, tx * F[v] + ty * Gf[v] + tz * W[v]);
+        }
+      } else {
+        const double uu = bU[e * Np + i];
+        const double F = bV[e * Np + i] * uu, Gf = bV[E * Np + e * Np + i] * uu,
+                     W = bV[2 * E * Np + e * Np + i] * uu;
+        put_split<C, PREC>(sAhi, sAlo, e, i, rx * F + ry * Gf + rz * W);
+        put_split<C, PREC>(sAhi, sAlo, e, Np + i, sx * F + sy * Gf + sz * W);
+        put_split<C, PREC>(sAhi, sAlo, e, 2 * Np + i, tx * F + ty * Gf + tz * W);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    consumer_sync(TC);
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll 1
+      for (int ks = 0; ks < C::KSV; ks++) {
+        const unsigned ao = ks * 256;
+        const unsigned long long ah = smem_desc(aHi + ao, 128, C::SBO_A);
+        const unsigned long long al = smem_desc(aLo + ao, 128, C::SBO_A);
+        const unsigned long long bh = smem_desc(bHiV + ao, 128, C::SBO_BV);
+        const unsigned long long bl = smem_desc(bLoV + ao, 128, C::SBO_BV);
+        const int j = ks * C::NACC / C::KST;          // accumulator of this k-step
+        const int first = ks == (j * C::KST + C::NACC - 1) / C::NACC;
+        const unsigned d = tmem + j * C::NPAD;
+        tc_mma<PREC>(d, al, bh, C::IDESC, !first);
+        tc_mma<PREC>(d, ah, bl, C::IDESC, 1);
+        tc_mma<PREC>(d, ah, bh, C::IDESC, 1);
+      }
+      tc_commit(mbar);
+    }
+    // the volume MMAs must have read the operand before it is overwritten
+    if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
+      ok = false;
+      break;
+    }
+    mma_phase ^= 1;
+    tc_fence_after();
+
+    // 3. face fluxes -> operand rows m, k = fj
+    for (int itm = tid; itm < E * NFF; itm += TC) {
+      const int fj = itm / E, e = itm - fj * E, f = fj / Nfp;
+      const int nodeM = sFm[fj];
+      const double nx = bF[0 * 4 * E + e * 4 + f], ny = bF[1 * 4 * E + e * 4 + f],
+                   nz = bF[2 * 4 * E + e * 4 + f], fs = bF[3 * 4 * E + e * 4 + f],
+                   tau = bF[4 * 4 * E + e * 4 + f];
+      if (PHYS == EUL) {
+        double qm[5], qb[5], F[5], Gf[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          qm[v] = bU[v * E * Np + e * Np + nodeM];
+          qb[v] = 0.5 * (qm[v] + bUP[(v * NFF + fj) * E + e]);
+        }
+        euler_flux_fast(a.gamma, qb, F, Gf, W);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];
+          put_split<C, PREC>(sAhi, sAlo, v * E + e, fj, (nd - tau * (qb[v] - qm[v])) * fs);
+        }
+      } else {
+        const double um = bU[e * Np + nodeM];
+        const double ub = 0.5 * (um + bUP[fj * E + e]);
+        const double F = bV[e * Np + nodeM] * ub, Gf = bV[E * Np + e * Np + nodeM] * ub,
+                     W = bV[2 * E * Np + e * Np + nodeM] * ub;
+        const double nd = nx * F + ny * Gf + nz * W;
+        put_split<C, PREC>(sAhi, sAlo, e, fj, (nd - tau * (ub - um)) * fs);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    consumer_sync(TC);
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll 1
+      for (int ks = 0; ks < C::KSF; ks++) {
+        const unsigned ao = ks * 256;
+        const unsigned long long ah = smem_desc(aHi + ao, 128, C::SBO_A);
+        const unsigned long long al = smem_desc(aLo + ao, 128, C::SBO_A);
+        const unsigned long long bh = smem_desc(bHiF + ao, 128, C::SBO_BF);
+        const unsigned long long bl = smem_desc(bLoF + ao, 128, C::SBO_BF);
+        const int kg = C::KSV + ks;                   // global k-step
+        const int j = kg * C::NACC / C::KST;
+        const int first = kg == (j * C::KST + C::NACC - 1) / C::NACC;
+        const unsigned d = tmem + j * C::NPAD;
+        tc_mma<PREC>(d, al, bh, C::IDESC, !first);
+        tc_mma<PREC>(d, ah, bl, C::IDESC, 1);
+        tc_mma<PREC>(d, ah, bh, C::IDESC, 1);
+      }
+      tc_commit(mbar);
+    }
+    if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
+      ok = false;
+      break;
+    }
+    mma_phase ^= 1;
+    tc_fence_after();
+
+    // 5. accumulator -> sR as [v][i][EP] (row m lives in TMEM lane
+    //    (m % 16) + 32 (m / 16) for M = 64, lane m for M = 128)
+    if (warp < 4) {
+      const int m = C::M == 64 ? 16 * warp + lane : 32 * warp + lane;
+      const bool valid = (C::M == 64 ? lane < 16 : true) && m < C::NCOL;
+      const int v = m / E, e = m - (m / E) * E;
+#pragma unroll 1
+      for (int c0 = 0; c0 < C::NPAD; c0 += 8) {
+        double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        float r[C::NACC][8];
+#pragma unroll
+        for (int j = 0; j < C::NACC; j++)
+          tmem_ld8(tmem + ((unsigned)(32 * warp) << 16) + j * C::NPAD + c0, r[j]);
+        tmem_ld_wait();
+#pragma unroll
+        for (int j = 0; j < C::NACC; j++)
+#pragma unroll
+          for (int q = 0; q < 8; q++) sum[q] += (double)r[j][q];
+        if (valid) {
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+            if (c0 + q < Np) sR[(v * Np + c0 + q) * EP + e] = sum[q];
+        }
+      }
+    }
+    tc_fence_before();
+    consumer_sync(TC);
+    for (int v = 0; v < NV; v++) {
+      const long base = v * vs + e0 * Np;
+      for (int g = tid; g < ne * Np; g += TC) {
+        const int e = g / Np, i = g - e * Np;
+        const double rhs = sR[(v * Np + i) * EP + e];
+        if (a.rhs_only) {
+          a.u_out[base + g] = rhs;
+        } else {
+          const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
+          const double un = bU[v * E * Np + g] + a.rkb * kn;
+          a.kreg[base + g] = kn;
+          a.u_out[base + g] = un;
+          bU[v * E * Np + g] = un;
+        }
+      }
+    }
+    if (PHYS == EUL && a.last_stage && !a.rhs_only) {
+      consumer_sync(TC);
+      for (int itm = tid; itm < 4 * E; itm += TC) {
+        const int f = itm / E, e = itm - f * E;
+        if (e >= ne) continue;
+        double mv2 = 0.0, mc2 = 0.0;
+        bool bad = false;
+        for (int j = 0; j < Nfp; j++) {
+          const int nd = e * Np + sFm[f * Nfp + j];
+          const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
+                       u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
+          const double ir = 1.0 / u1;
+          const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
+          const double v2 = vx * vx + vy * vy + vz * vz;
+          mv2 = v2 > mv2 ? v2 : mv2;
+          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
+          const double c2 = fabs(a.gamma * pres * ir);
+          mc2 = c2 > mc2 ? c2 : mc2;
+          bad |= (v2 != v2) || (c2 != c2);
+        }
+        double mv = sqrt(mv2) + sqrt(mc2);
+        if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+        a.maxv[(e0 + e) * 4 + f] = mv;
+        const unsigned long long bits = dbits(mv * bF[3 * 4 * E + e * 4 + f]);
+        vmax = bits > vmax ? bits : vmax;
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[b]);
+  }
+  if (!ok && tid == 0) atomicOr(&a.sc->flags, 4);
+  if (PHYS == EUL && a.last_stage && !a.rhs_only) {
+    vmax = warp_max_bits(vmax);
+    if (lane == 0) sMax[warp] = vmax;
+    consumer_sync(TC);
+    if (tid < 32) {
+      unsigned long long v = tid < C::NWC ? sMax[tid] : 0ull;
+      v = warp_max_bits(v);
+      if (tid == 0) atomicMax(&a.sc->acc[a.sc->parity ^ 1], v);
+    }
+  }
+  // release tensor memory (warp 0 allocated it)
+  tc_fence_before();
+  consumer_sync(TC);
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, C::TCOLS);
+  }
+}

@@ -121,6 +121,78 @@ struct PCfg {
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
 };
 
+// Producer warp of the pipelined kernels: optional one-off bulk load of an
+// operator image into shared memory (abar), then per tile (two-deep ring)
+// TMA bulk copies of the tile's u, k, metrics, face data (and advection
+// velocity) and cp.async gathers of the neighbour traces.
+template <class C, int PHYS>
+__device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, void *op_smem,
+                                              double *sBuf0, unsigned long long *full,
+                                              unsigned long long *empty,
+                                              unsigned long long *abar, unsigned op_bytes,
+                                              int lane) {
+  constexpr int NV = C::NV, Np = C::Np, NFF = C::NFF, E = C::E;
+  const long vs = a.vs, gs = a.gstride;
+  if (op_bytes && lane == 0) {
+    mbar_arrive_expect_tx(abar, op_bytes);
+    bulk_g2s(op_smem, a.AT, op_bytes, abar);
+  }
+  int it = 0;
+  bool ok = true;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+    const int b = it & 1;
+    if (it >= 2 && !mbar_wait(&empty[b], ((it >> 1) - 1) & 1)) {
+      ok = false;
+      break;
+    }
+    const long e0 = (long)t * E;
+    const int ne = (int)min((long)E, (long)a.K - e0);
+    double *B = sBuf0 + b * C::S_BUF;
+    double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
+    double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&full[b], C::TX);
+      for (int v = 0; v < NV; v++) {
+        bulk_g2s(bU + v * E * Np, a.u_in + v * vs + e0 * Np, 8u * E * Np, &full[b]);
+        bulk_g2s(bK + v * E * Np, a.kreg + v * vs + e0 * Np, 8u * E * Np, &full[b]);
+      }
+      for (int m = 0; m < 9; m++) bulk_g2s(bG + m * E, a.geo + m * gs + e0, 8u * E, &full[b]);
+      for (int q = 0; q < 3; q++)
+        bulk_g2s(bF + q * 4 * E, a.nrm + q * 4 * gs + 4 * e0, 32u * E, &full[b]);
+      bulk_g2s(bF + 3 * 4 * E, a.fscale + 4 * e0, 32u * E, &full[b]);
+      bulk_g2s(bF + 4 * 4 * E, a.tau + 4 * e0, 32u * E, &full[b]);
+      if (PHYS != EUL)
+        for (int q = 0; q < 3; q++)
+          bulk_g2s(bV + q * E * Np, a.vel + q * vs + e0 * Np, 8u * E * Np, &full[b]);
+    }
+    // neighbour traces u+ = u[vmapP] into [v][fj][e]: all of this lane's
+    // vmapP loads are issued first, so their latency is paid once
+    constexpr int GPL = (E * NFF + 31) / 32;
+    int vmr[GPL];
+#pragma unroll
+    for (int j = 0; j < GPL; j++) {
+      const int idx = lane + 32 * j;
+      vmr[j] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < GPL; j++) {
+      const int idx = lane + 32 * j;
+      if (vmr[j] >= 0) {
+        const int e = idx / NFF, fj = idx - e * NFF;
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+          cp_async8(bUP + (v * NFF + fj) * E + e, a.u_in + v * vs + vmr[j]);
+      }
+    }
+    cp_async_arrive_noinc(&full[b]);
+  }
+  if (!ok) atomicOr(&a.sc->flags, 4);
+  // let the copies of the last two tiles settle before this warp leaves
+  for (int j = (it > 2 ? it - 2 : 0); j < it; j++) mbar_wait(&full[j & 1], (j >> 1) & 1);
+  if (op_bytes) mbar_wait(abar, 0);
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM>
 __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
@@ -137,7 +209,7 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long vs = a.vs, gs = a.gstride;
+  const long vs = a.vs;
 
   if (tid == 0) {
     mbar_init(&full[0], 33);
@@ -155,51 +227,7 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1
 
   // ------------------------------------------------------------- producer
   if (warp == C::NWC) {
-    if (ASMEM && lane == 0) {
-      mbar_arrive_expect_tx(abar, 8u * C::S_AF);
-      bulk_g2s(sAF, a.AT, 8u * C::S_AF, abar);
-    }
-    int it = 0;
-    bool ok = true;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
-      const int b = it & 1;
-      if (it >= 2 && !mbar_wait(&empty[b], ((it >> 1) - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      const long e0 = (long)t * E;
-      const int ne = (int)min((long)E, (long)a.K - e0);
-      double *B = buf(b);
-      double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
-      double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
-      if (lane == 0) {
-        mbar_arrive_expect_tx(&full[b], C::TX);
-        for (int v = 0; v < NV; v++) {
-          bulk_g2s(bU + v * E * Np, a.u_in + v * vs + e0 * Np, 8u * E * Np, &full[b]);
-          bulk_g2s(bK + v * E * Np, a.kreg + v * vs + e0 * Np, 8u * E * Np, &full[b]);
-        }
-        for (int m = 0; m < 9; m++) bulk_g2s(bG + m * E, a.geo + m * gs + e0, 8u * E, &full[b]);
-        for (int q = 0; q < 3; q++)
-          bulk_g2s(bF + q * 4 * E, a.nrm + q * 4 * gs + 4 * e0, 32u * E, &full[b]);
-        bulk_g2s(bF + 3 * 4 * E, a.fscale + 4 * e0, 32u * E, &full[b]);
-        bulk_g2s(bF + 4 * 4 * E, a.tau + 4 * e0, 32u * E, &full[b]);
-        if (PHYS != EUL)
-          for (int q = 0; q < 3; q++)
-            bulk_g2s(bV + q * E * Np, a.vel + q * vs + e0 * Np, 8u * E * Np, &full[b]);
-      }
-      // neighbour traces u+ = u[vmapP] into [v][fj][e]
-      for (int idx = lane; idx < ne * NFF; idx += 32) {
-        const long vm = __ldg(a.vmapP + e0 * NFF + idx);
-        const int e = idx / NFF, fj = idx - e * NFF;
-#pragma unroll
-        for (int v = 0; v < NV; v++) cp_async8(bUP + (v * NFF + fj) * E + e, a.u_in + v * vs + vm);
-      }
-      cp_async_arrive_noinc(&full[b]);
-    }
-    if (!ok) atomicOr(&a.sc->flags, 4);
-    // let the copies of the last two tiles settle before this warp leaves
-    for (int j = (it > 2 ? it - 2 : 0); j < it; j++) mbar_wait(&full[j & 1], (j >> 1) & 1);
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    pipe_producer<C, PHYS>(a, ntiles, sAF, sBuf0, full, empty, abar, 8u * C::S_AF, lane);
     return;
   }
 
