@@ -235,7 +235,7 @@ def main():
 
     import numpy as np
     import torch
-    from exadglm_b200.capi import Solver
+    from exadglm_b200.capi import Solver, variants
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -303,8 +303,9 @@ def main():
     achieved_gbs = B / (stage_ms * 1e-3) / 1e9
     achieved_tf = F / (stage_ms * 1e-3) / 1e12
     tag = f"euler_N{p.N}_K{p.K}_{a.precision}"
+    vdesc = variants("euler", p.N)[s.variant()]
     roof = {
-        "kernel": "stage_fp64_kernel<EUL,%d>" % p.N,
+        "kernel": vdesc,
         "bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": read_traffic(tag),
         "peak_source": f"{peak_kind} hbm_gbs (burst, kernel timed alone)",
