@@ -25,7 +25,8 @@ EXPORTS = (
     "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
-    "dglm_set_variant", "dglm_get_variant",
+    "dglm_set_variant", "dglm_get_variant", "dglm_adjoint_record", "dglm_adjoint_backward",
+    "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
 )
 
 
@@ -94,6 +95,11 @@ def lib():
         L.dglm_calc_fluxes.argtypes = [I, I, I, D, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         L.dglm_update_rhs.argtypes = [I, I, I, _P, _P, _P, _P, C.c_char, _P, _P, _P, _P, _P, _P]
         L.dglm_lserk_stage.argtypes = [I, I, I, D, D, D, _P, _P, _P, _P]
+        L.dglm_adjoint_record.argtypes = [_P, I, I]
+        L.dglm_adjoint_backward.argtypes = [_P, _P, _P, I]
+        L.dglm_adjoint_replay.argtypes = [_P]
+        L.dglm_adjoint_rhs.argtypes = [_P, _P, _P, _P]
+        L.dglm_adjoint_tape_bytes.argtypes = [_P, C.POINTER(C.c_size_t)]
         _lib = L
     return _lib
 
@@ -244,6 +250,37 @@ class Solver:
 
     def rhs_device(self, u_ptrs, rhs_ptrs):
         check(self.L.dglm_rhs(self.h, ptr_table(u_ptrs), ptr_table(rhs_ptrs)))
+
+    # -- discrete adjoint (FP64; dt and tau frozen at the recorded values) --
+    def adjoint_record(self, nsteps, checkpoint_every=50):
+        """nsteps CFL steps from the current state, recording the tape."""
+        check(self.L.dglm_adjoint_record(self.h, int(nsteps), int(checkpoint_every)))
+
+    def adjoint_backward(self, lam_T):
+        """(du_T/du_0)^T lam_T for the recorded run (numpy in, numpy out)."""
+        lam_T = np.ascontiguousarray(lam_T, dtype=np.float64).reshape(self.p.nvar, -1)
+        out = np.empty_like(lam_T)
+        check(self.L.dglm_adjoint_backward(
+            self.h, ptr_table([lam_T[v].ctypes.data for v in range(len(lam_T))]),
+            ptr_table([out[v].ctypes.data for v in range(len(out))]), 0))
+        return out
+
+    def adjoint_backward_device(self, lam_T_ptrs, lam_0_ptrs):
+        check(self.L.dglm_adjoint_backward(self.h, ptr_table(lam_T_ptrs), ptr_table(lam_0_ptrs),
+                                           1))
+
+    def adjoint_replay(self):
+        """The recorded run from the current state with recorded dt and tau."""
+        check(self.L.dglm_adjoint_replay(self.h))
+
+    def adjoint_rhs_device(self, u_ptrs, mu_ptrs, out_ptrs):
+        check(self.L.dglm_adjoint_rhs(self.h, ptr_table(u_ptrs), ptr_table(mu_ptrs),
+                                      ptr_table(out_ptrs)))
+
+    def adjoint_tape_bytes(self):
+        n = C.c_size_t()
+        check(self.L.dglm_adjoint_tape_bytes(self.h, C.byref(n)))
+        return int(n.value)
 
     def set_stream(self, stream_ptr):
         check(self.L.dglm_set_stream(self.h, C.c_void_p(int(stream_ptr))))

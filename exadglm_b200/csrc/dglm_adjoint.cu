@@ -1,0 +1,863 @@
+// Discrete adjoint of the DGLM right-hand side and of the LSERK step.
+//
+// The reference has no adjoint; this is the exact transpose of the
+// derivative of this library's own forward step with the step size dt and
+// the face penalty tau frozen at the values of the forward run (both are
+// non-smooth functions of u: a global max and a per-face max).
+//
+// One LSERK stage s maps (u, k) to
+//     k' = a_s k + dt R(u),   u' = u + b_s k'.
+// Its transpose, for adjoints (lam, lk) of (u', k'), is
+//     mu  = lk + b_s lam
+//     lk  = a_s mu
+//     lam = lam + dt R'(u)^T mu
+// and a step is the five stages in reverse order.  R = WD_d (geo.F) - LIFT
+// fluxLM, so with phi = -LIFT^T mu (a face-point field):
+//   volume: lam_j += sum_x A_x(u_j)^T G_x,  G_x = sum_d geo[d][x] (WD_d^T mu)_j
+//   faces:  for face point p with own node M(p) and partner node P(p)
+//           d fluxLM_p/du_M = fs (A_n(ub)/2 + tau/2),
+//           d fluxLM_p/du_P = fs (A_n(ub)/2 - tau/2).
+// The second term scatters to the neighbour.  On a conforming mesh the face
+// points pair up (mapP: the partner face point p' with vmapP[p'] == M(p), an
+// involution), so node M(p) gathers it from p' instead:
+//   lam_M += fs (A_n^T phi_p + tau phi_p)/2 + fs' (A_n'^T phi_p' - tau' phi_p')/2
+// with fs', n', tau' the partner face's values.  No atomics.
+//
+// Kernel layout.  phi of a stage is needed by the neighbours, so it is
+// produced one launch ahead: the launch for stage s reads phi_s (phi_in),
+// updates lam and lk, then forms mu of the next stage in reverse order and
+// writes phi of it (phi_out).  One launch per adjoint stage plus one
+// phi-only launch at the start of a sweep.
+//
+// A CTA owns E elements.  Both contractions are register-tiled DFMA over the
+// k = Np nodes with the output rows interleaved so that a thread ends with
+// everything one node needs: rows (3j + d) of [WD_r^T; WD_s^T; WD_t^T] for
+// RJ nodes j and all NV variables of one element, so the Euler Jacobian
+// transposes run in registers on the contraction's output.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dglm_common.cuh"
+#include "dglm_handle.cuh"
+
+namespace dglm {
+
+struct AdjArgs {
+  const double *AV;      // [Np][IPV]: AV[i*IPV + 3j + d] = WD_d(i, j)
+  const double *AL;      // [Np][IPL]: AL[i*IPL + fj] = -LIFT(i, fj)
+  const double *geo;     // 9 x gstride
+  const double *fscale;  // 4 K
+  const double *nrm;     // 3 x 4 gstride
+  const double *tau;     // 4 K (frozen)
+  const int *vmapP;      // K NFF
+  const int *vmapF;      // 4 K
+  const int *mapP;       // K NFF: partner face point
+  const int *Fmask;      // NFF
+  const double *vel;     // advection velocity, stride vs
+  const double *u;       // state at the stage's input
+  double *lam, *lk;      // adjoints of u and k (updated in place, own tile only)
+  const double *phi_in;  // phi of this stage, nvar x vsF
+  double *phi_out;       // phi of the next stage in reverse order
+  long vs, vsF, gstride;
+  int K;
+  double gamma, dt, rka, rkb, rkb_next;
+  int update;            // 1: apply the stage's transpose; 0: only form phi_out
+  int phi_next;          // 1: write phi_out
+};
+
+enum { A_ADV = 0, A_EUL = 1 };
+
+template <int PHYS, int N, int E_>
+struct ACfg {
+  static constexpr int NV = PHYS == A_EUL ? 5 : 1;
+  static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
+  static constexpr int E = E_, EP = E_ + 1;
+  static constexpr int RJ = (E * Np + 767) / 768;     // nodes per thread
+  static constexpr int G = (Np + RJ - 1) / RJ;        // row groups
+  static constexpr int T = E * G;                     // threads
+  static constexpr int RF = (NFF + G - 1) / G;        // lift rows per thread
+  static constexpr int IPV = 3 * G * RJ, IPL = G * RF;
+  static constexpr int BLD = NV * E;
+  static constexpr int VMLD = NFF + 1;
+  static constexpr int S_U = NV * Np * EP, S_MU = Np * BLD, S_FC = NV * NFF * EP;
+  static constexpr size_t SMEM =
+      sizeof(double) * (2 * S_U + S_MU + S_FC + 9 * E + 40 * E) +
+      sizeof(int) * (2 * E * VMLD + NFF + 4 * Np);
+  static_assert(T <= 1024, "block too large");
+};
+
+// Shared part of A_n(q)^T for the Euler flux with p = (gamma-1)(E - |m|^2/(2 rho)).
+struct JacPre {
+  double u[3], H, phi;
+};
+
+__device__ __forceinline__ JacPre jac_pre(double gm, const double q[5]) {
+  JacPre P;
+  const double ir = 1.0 / q[0];
+  P.u[0] = q[1] * ir;
+  P.u[1] = q[2] * ir;
+  P.u[2] = q[3] * ir;
+  const double q2 = P.u[0] * P.u[0] + P.u[1] * P.u[1] + P.u[2] * P.u[2];
+  const double p = (gm - 1) * (q[4] - 0.5 * q[0] * q2);
+  P.H = (q[4] + p) * ir;
+  P.phi = 0.5 * (gm - 1) * q2;
+  return P;
+}
+
+// w += s * A_n(q)^T g
+__device__ __forceinline__ void jac_t_add(const JacPre &P, double gm, double nx, double ny,
+                                          double nz, const double g[5], double s, double w[5]) {
+  const double un = P.u[0] * nx + P.u[1] * ny + P.u[2] * nz;
+  const double gu = g[1] * P.u[0] + g[2] * P.u[1] + g[3] * P.u[2];
+  const double gn = g[1] * nx + g[2] * ny + g[3] * nz;
+  const double n3[3] = {nx, ny, nz};
+  w[0] += s * (-un * gu + P.phi * gn + g[4] * un * (P.phi - P.H));
+#pragma unroll
+  for (int j = 0; j < 3; j++)
+    w[1 + j] += s * (g[0] * n3[j] + un * g[1 + j] + gu * n3[j] - (gm - 1) * gn * P.u[j] +
+                     g[4] * (P.H * n3[j] - (gm - 1) * un * P.u[j]));
+  w[4] += s * ((gm - 1) * gn + gm * un * g[4]);
+}
+
+template <int PHYS, int N, int E_>
+__global__ void __launch_bounds__(ACfg<PHYS, N, E_>::T)
+    adjoint_stage_kernel(const AdjArgs a) {
+  using C = ACfg<PHYS, N, E_>;
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+                BLD = C::BLD, T = C::T, RJ = C::RJ, RF = C::RF, VMLD = C::VMLD;
+  extern __shared__ __align__(16) double smem[];
+  double *sU = smem;                   // [v][i][EP] stage state, later lk'
+  double *sLam = sU + C::S_U;          // [v][i][EP]
+  double *sMu = sLam + C::S_U;         // [i][BLD], col = v*E + e
+  double *sFc = sMu + C::S_MU;         // [v][fj][EP] face terms, later phi'
+  double *sGeo = sFc + C::S_FC;        // [9][E]
+  double *sFace = sGeo + 9 * E;        // [10][4][E]: n fs tau, partner n fs tau
+  int *sVm = reinterpret_cast<int *>(sFace + 40 * E);   // [E][VMLD]
+  int *sMp = sVm + E * VMLD;           // [E][VMLD]
+  int *sFm = sMp + E * VMLD;           // [NFF]
+  int *sNF = sFm + NFF;                // [Np][4] face points of each node
+
+  const int tid = threadIdx.x;
+  const long e0 = (long)blockIdx.x * E;
+  const int ne = (int)min((long)E, (long)a.K - e0);
+  const long vs = a.vs, vsF = a.vsF;
+  const bool upd = a.update != 0;
+
+  // ---- staging ------------------------------------------------------------
+  for (int i = tid; i < NFF; i += T) sFm[i] = __ldg(a.Fmask + i);
+  for (int i = tid; i < Np; i += T) {
+    int c = 0;
+    for (int fj = 0; fj < NFF; fj++)
+      if (__ldg(a.Fmask + fj) == i && c < 4) sNF[i * 4 + c++] = fj;
+    for (; c < 4; c++) sNF[i * 4 + c] = -1;
+  }
+  const double bm = upd ? a.rkb : a.rkb_next;
+  for (int v = 0; v < NV; v++) {
+    const long base = v * vs + e0 * Np;
+    for (int g = tid; g < E * Np; g += T) {
+      const int e = g / Np, i = g - e * Np;
+      const bool ok = g < ne * Np;
+      const double lam = ok ? a.lam[base + g] : 0.0;
+      const double lk = ok ? a.lk[base + g] : 0.0;
+      sLam[(v * Np + i) * EP + e] = lam;
+      sMu[i * BLD + v * E + e] = lk + bm * lam;
+      if (upd) sU[(v * Np + i) * EP + e] = ok ? __ldg(a.u + base + g) : (v == 0 ? 1.0 : 0.0);
+    }
+  }
+  if (upd) {
+    for (int g = tid; g < 9 * E; g += T) {
+      const int m = g / E, e = g - m * E;
+      sGeo[g] = e < ne ? __ldg(a.geo + (long)m * a.gstride + e0 + e) : 0.0;
+    }
+    for (int g = tid; g < 4 * E; g += T) {
+      const int e = g >> 2, f = g & 3;
+      const bool ok = e < ne;
+      const long gf = (e0 + e) * 4 + f;
+      const long gf2 = ok ? __ldg(a.vmapF + gf) : 0;
+      const long gs = a.gstride;
+      sFace[(0 * 4 + f) * E + e] = ok ? __ldg(a.nrm + gf) : 0.0;
+      sFace[(1 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 4 * gs + gf) : 0.0;
+      sFace[(2 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 8 * gs + gf) : 0.0;
+      sFace[(3 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf) : 0.0;
+      sFace[(4 * 4 + f) * E + e] = ok ? __ldg(a.tau + gf) : 0.0;
+      sFace[(5 * 4 + f) * E + e] = ok ? __ldg(a.nrm + gf2) : 0.0;
+      sFace[(6 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 4 * gs + gf2) : 0.0;
+      sFace[(7 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 8 * gs + gf2) : 0.0;
+      sFace[(8 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf2) : 0.0;
+      sFace[(9 * 4 + f) * E + e] = ok ? __ldg(a.tau + gf2) : 0.0;
+    }
+    for (int g = tid; g < E * NFF; g += T) {
+      const int e = g / NFF, fj = g - e * NFF;
+      const bool ok = g < ne * NFF;
+      sVm[e * VMLD + fj] = ok ? __ldg(a.vmapP + e0 * NFF + g) : 0;
+      sMp[e * VMLD + fj] = ok ? __ldg(a.mapP + e0 * NFF + g) : 0;
+    }
+  }
+  __syncthreads();
+
+  const int cg = tid % E, rg = tid / E;
+  double acc[3 * RJ][NV];
+  if (upd) {
+    // ---- face terms -> sFc ------------------------------------------------
+    for (int it = tid; it < E * NFF; it += T) {
+      const int e = it / NFF, fj = it - e * NFF, f = fj / Nfp;
+      if (e >= ne) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) sFc[(v * NFF + fj) * EP + e] = 0.0;
+        continue;
+      }
+      const long p = (e0 + e) * NFF + fj;
+      const long iP = sVm[e * VMLD + fj], p2 = sMp[e * VMLD + fj];
+      const int nodeM = sFm[fj];
+      const double *F4 = sFace + f * E + e;
+      const double nx = F4[0], ny = F4[4 * E], nz = F4[8 * E], fs = F4[12 * E],
+                   ta = F4[16 * E], nx2 = F4[20 * E], ny2 = F4[24 * E], nz2 = F4[28 * E],
+                   fs2 = F4[32 * E], ta2 = F4[36 * E];
+      if (PHYS == A_EUL) {
+        double qb[5], g1[5], g2[5], w[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          qb[v] = 0.5 * (sU[(v * Np + nodeM) * EP + e] + __ldg(a.u + v * vs + iP));
+          g1[v] = a.phi_in[v * vsF + p];
+          g2[v] = a.phi_in[v * vsF + p2];
+          w[v] = 0.5 * (fs * ta * g1[v] - fs2 * ta2 * g2[v]);
+        }
+        const JacPre P = jac_pre(a.gamma, qb);
+        jac_t_add(P, a.gamma, nx, ny, nz, g1, 0.5 * fs, w);
+        jac_t_add(P, a.gamma, nx2, ny2, nz2, g2, 0.5 * fs2, w);
+#pragma unroll
+        for (int v = 0; v < 5; v++) sFc[(v * NFF + fj) * EP + e] = w[v];
+      } else {
+        const long nM = (e0 + e) * Np + nodeM;
+        const double an = nx * __ldg(a.vel + nM) + ny * __ldg(a.vel + vs + nM) +
+                          nz * __ldg(a.vel + 2 * vs + nM);
+        const double an2 = nx2 * __ldg(a.vel + iP) + ny2 * __ldg(a.vel + vs + iP) +
+                           nz2 * __ldg(a.vel + 2 * vs + iP);
+        const double g1 = a.phi_in[p], g2 = a.phi_in[p2];
+        sFc[fj * EP + e] = fs * (0.5 * an + 0.5 * ta) * g1 + fs2 * (0.5 * an2 - 0.5 * ta2) * g2;
+      }
+    }
+
+    // ---- nu = [WD_r^T; WD_s^T; WD_t^T] mu, rows 3j + d ---------------------
+#pragma unroll
+    for (int r = 0; r < 3 * RJ; r++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) acc[r][v] = 0.0;
+    const double *Ab = a.AV + rg * 3 * RJ;
+#pragma unroll 5
+    for (int k = 0; k < Np; k++) {
+      double bv[NV], av[3 * RJ];
+#pragma unroll
+      for (int v = 0; v < NV; v++) bv[v] = sMu[k * BLD + v * E + cg];
+#pragma unroll
+      for (int r = 0; r < 3 * RJ; r++) av[r] = __ldg(Ab + k * C::IPV + r);
+#pragma unroll
+      for (int r = 0; r < 3 * RJ; r++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[r][v] = fma(av[r], bv[v], acc[r][v]);
+    }
+  }
+  __syncthreads();
+
+  if (upd) {
+    // ---- combine: lam' = lam + dt (volume + face terms), lk' = a mu ---------
+    const double *gg = sGeo + cg;
+#pragma unroll
+    for (int r = 0; r < RJ; r++) {
+      const int j = rg * RJ + r;
+      if (j >= Np) continue;
+      double w[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) w[v] = 0.0;
+#pragma unroll
+      for (int x = 0; x < 3; x++) {
+        double Gx[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+          Gx[v] = gg[x * E] * acc[3 * r][v] + gg[(3 + x) * E] * acc[3 * r + 1][v] +
+                  gg[(6 + x) * E] * acc[3 * r + 2][v];
+        if (PHYS == A_EUL) {
+          double q[5];
+#pragma unroll
+          for (int v = 0; v < 5; v++) q[v] = sU[(v * Np + j) * EP + cg];
+          const JacPre P = jac_pre(a.gamma, q);
+          jac_t_add(P, a.gamma, x == 0, x == 1, x == 2, Gx, 1.0, w);
+        } else {
+          const long n = (cg < ne) ? (e0 + cg) * Np + j : 0;
+          w[0] += __ldg(a.vel + x * vs + n) * Gx[0];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int fj = sNF[j * 4 + c];
+        if (fj < 0) break;
+#pragma unroll
+        for (int v = 0; v < NV; v++) w[v] += sFc[(v * NFF + fj) * EP + cg];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        const int s = (v * Np + j) * EP + cg;
+        const double mu = sMu[j * BLD + v * E + cg];
+        const double lamn = sLam[s] + a.dt * w[v];
+        const double lkn = a.rka * mu;
+        sLam[s] = lamn;
+        sU[s] = lkn;
+        sMu[j * BLD + v * E + cg] = lkn + a.rkb_next * lamn;
+      }
+    }
+    __syncthreads();
+  }
+
+  if (a.phi_next) {
+    // ---- phi' = -LIFT^T mu' -> sFc ------------------------------------------
+    double acf[RF][NV];
+#pragma unroll
+    for (int r = 0; r < RF; r++)
+#pragma unroll
+      for (int v = 0; v < NV; v++) acf[r][v] = 0.0;
+    const double *Ab = a.AL + rg * RF;
+#pragma unroll 5
+    for (int k = 0; k < Np; k++) {
+      double bv[NV], av[RF];
+#pragma unroll
+      for (int v = 0; v < NV; v++) bv[v] = sMu[k * BLD + v * E + cg];
+#pragma unroll
+      for (int r = 0; r < RF; r++) av[r] = __ldg(Ab + k * C::IPL + r);
+#pragma unroll
+      for (int r = 0; r < RF; r++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) acf[r][v] = fma(av[r], bv[v], acf[r][v]);
+    }
+#pragma unroll
+    for (int r = 0; r < RF; r++) {
+      const int fj = rg * RF + r;
+      if (fj < NFF) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) sFc[(v * NFF + fj) * EP + cg] = acf[r][v];
+      }
+    }
+    __syncthreads();
+    for (int v = 0; v < NV; v++) {
+      const long base = v * vsF + e0 * NFF;
+      for (int g = tid; g < ne * NFF; g += T) {
+        const int e = g / NFF, fj = g - e * NFF;
+        a.phi_out[base + g] = sFc[(v * NFF + fj) * EP + e];
+      }
+    }
+  }
+
+  if (upd) {
+    for (int v = 0; v < NV; v++) {
+      const long base = v * vs + e0 * Np;
+      for (int g = tid; g < ne * Np; g += T) {
+        const int e = g / Np, i = g - e * Np;
+        const int s = (v * Np + i) * EP + e;
+        a.lam[base + g] = sLam[s];
+        a.lk[base + g] = sU[s];
+      }
+    }
+  }
+}
+
+// Partner face point of every face point (see the file comment); flags a
+// face point without exactly one partner or a pairing that is not an
+// involution.
+__global__ void adjoint_mapP_kernel(int K, int Np, int Nfp, const int *__restrict__ Fmask,
+                                    const int *__restrict__ vmapP,
+                                    const int *__restrict__ vmapF, int *__restrict__ mapP,
+                                    int *bad) {
+  const int NFF = 4 * Nfp;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= (long)K * NFF) return;
+  const long e = p / NFF;
+  const int fj = (int)(p - e * NFF), f = fj / Nfp;
+  const long target = e * Np + Fmask[fj];
+  const long gf2 = vmapF[e * 4 + f];
+  long found = p;
+  int cnt = 0;
+  for (int j2 = 0; j2 < Nfp; j2++)
+    if (vmapP[gf2 * Nfp + j2] == target) {
+      found = gf2 * Nfp + j2;
+      cnt++;
+    }
+  if (cnt != 1) atomicOr(bad, 1);
+  mapP[p] = (int)found;
+}
+
+__global__ void adjoint_mapP_check_kernel(long n, const int *__restrict__ mapP, int *bad) {
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p < n && mapP[mapP[p]] != p) atomicOr(bad, 2);
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+
+struct AdjVariant {
+  int E, T, IPV, IPL;
+  size_t smem;
+  cudaError_t (*launch)(const AdjArgs &, cudaStream_t);
+};
+
+template <int PHYS, int N, int E>
+cudaError_t launch_adj(const AdjArgs &a, cudaStream_t s) {
+  using C = ACfg<PHYS, N, E>;
+  auto k = adjoint_stage_kernel<PHYS, N, E>;
+  cudaError_t e =
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int blocks = (a.K + E - 1) / E;
+  k<<<blocks, C::T, C::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E>
+constexpr AdjVariant adj_variant() {
+  using C = ACfg<PHYS, N, E>;
+  return AdjVariant{E, C::T, C::IPV, C::IPL, C::SMEM, launch_adj<PHYS, N, E>};
+}
+
+bool adjoint_variant(int physics, int N, AdjVariant *out) {
+  static const AdjVariant eul[] = {adj_variant<A_EUL, 1, 16>(), adj_variant<A_EUL, 2, 16>(),
+                                   adj_variant<A_EUL, 3, 8>(),  adj_variant<A_EUL, 4, 8>(),
+                                   adj_variant<A_EUL, 5, 8>(),  adj_variant<A_EUL, 6, 4>()};
+  static const AdjVariant adv[] = {adj_variant<A_ADV, 1, 64>(), adj_variant<A_ADV, 2, 32>(),
+                                   adj_variant<A_ADV, 3, 32>(), adj_variant<A_ADV, 4, 32>(),
+                                   adj_variant<A_ADV, 5, 16>(), adj_variant<A_ADV, 6, 16>()};
+  if (N < 1 || N > 6) return false;
+  *out = physics == DGLM_EULER ? eul[N - 1] : adv[N - 1];
+  return true;
+}
+
+}  // namespace dglm
+
+using namespace dglm;
+
+// ---------------------------------------------------------------------------
+// the tape of a recorded forward run
+// ---------------------------------------------------------------------------
+
+struct AdjointTape {
+  AdjVariant var{};
+  long state = 0;            // doubles per stored state (nvar * vs)
+  long vsF = 0;              // doubles between variables of a face-point field
+  int nsteps = 0, every = 0, nseg = 0, cap_ckpt = 0, cap_steps = 0, cap_store = 0;
+  bool recorded = false;
+  std::vector<double> dt;    // dt of every recorded step
+  double *AV = nullptr, *AL = nullptr;
+  int *mapP = nullptr, *bad = nullptr;
+  double *lam = nullptr, *lk = nullptr, *phi[2] = {nullptr, nullptr}, *kbuf = nullptr;
+  double *dt_dev = nullptr;  // cap_steps
+  double *tau = nullptr;     // cap_steps x 4Kp (Euler) or 4Kp (advection)
+  double *ckpt = nullptr;    // cap_ckpt states
+  double *store = nullptr;   // cap_store states: stage inputs of one segment
+  std::vector<void *> fixed, sized;   // allocations: per mesh / per recording size
+  size_t bytes = 0, sized_bytes = 0;
+};
+
+namespace dglm {
+
+void free_tape(dglm_handle *h) {
+  if (!h->tape) return;
+  for (void *p : h->tape->fixed) cudaFree(p);
+  for (void *p : h->tape->sized) cudaFree(p);
+  delete h->tape;
+  h->tape = nullptr;
+}
+
+}  // namespace dglm
+
+namespace {
+
+template <typename T>
+dglm_status talloc(AdjointTape *t, std::vector<void *> &list, T **p, size_t count) {
+  const bool sized = &list == &t->sized;
+  void *q = nullptr;
+  const size_t n = std::max<size_t>(count * sizeof(T), 16);
+  cudaError_t e = cudaMalloc(&q, n);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(DGLM_ERR_NOMEM, std::string("adjoint: cudaMalloc of ") +
+                                         std::to_string(n) + " bytes failed: " +
+                                         cudaGetErrorString(e));
+  }
+  list.push_back(q);
+  t->bytes += n;
+  if (sized) t->sized_bytes += n;
+  *p = static_cast<T *>(q);
+  return DGLM_OK;
+}
+
+// Per-mesh part of the tape: transposed operators, the face-point pairing
+// and the adjoint fields.  Rebuilt after every mesh upload.
+dglm_status tape_setup(dglm_handle *h) {
+  if (h->d.precision != DGLM_PREC_FP64)
+    return set_error(DGLM_ERR_UNSUPPORTED,
+                     "adjoint: only FP64 handles (the adjoint is the transpose of the FP64 step)");
+  if (h->tape && h->tape->AV) return DGLM_OK;
+  free_tape(h);
+  AdjointTape *t = new AdjointTape();
+  h->tape = t;
+  if (!adjoint_variant(h->d.physics, h->d.N, &t->var))
+    return set_error(DGLM_ERR_UNSUPPORTED, "adjoint: order not built (1..6)");
+  const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF;
+  const long K = h->d.K;
+  t->state = (long)h->nvar * h->vs;
+  t->vsF = (h->Kp * NFF + 31) / 32 * 32;
+  dglm_status st = DGLM_OK;
+  auto chk = [&](dglm_status s) {
+    if (st == DGLM_OK) st = s;
+  };
+  chk(talloc(t, t->fixed, &t->AV, (size_t)Np * t->var.IPV));
+  chk(talloc(t, t->fixed, &t->AL, (size_t)Np * t->var.IPL));
+  chk(talloc(t, t->fixed, &t->mapP, (size_t)K * NFF));
+  chk(talloc(t, t->fixed, &t->bad, 1));
+  chk(talloc(t, t->fixed, &t->lam, (size_t)t->state));
+  chk(talloc(t, t->fixed, &t->lk, (size_t)t->state));
+  chk(talloc(t, t->fixed, &t->kbuf, (size_t)t->state));
+  chk(talloc(t, t->fixed, &t->phi[0], (size_t)h->nvar * t->vsF));
+  chk(talloc(t, t->fixed, &t->phi[1], (size_t)h->nvar * t->vsF));
+  if (st != DGLM_OK) {
+    free_tape(h);
+    return st;
+  }
+  std::vector<double> av((size_t)Np * t->var.IPV, 0.0), al((size_t)Np * t->var.IPL, 0.0);
+  for (int i = 0; i < Np; i++) {
+    for (int j = 0; j < Np; j++)
+      for (int d = 0; d < 3; d++)
+        av[(size_t)i * t->var.IPV + 3 * j + d] = h->Ahost[(size_t)i * KA + d * Np + j];
+    for (int fj = 0; fj < NFF; fj++)
+      al[(size_t)i * t->var.IPL + fj] = h->Ahost[(size_t)i * KA + 3 * Np + fj];
+  }
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->AV, av.data(), sizeof(double) * av.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->AL, al.data(), sizeof(double) * al.size(), cudaMemcpyHostToDevice);
+  for (double *p : {t->lam, t->lk, t->kbuf})
+    if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(double) * t->state);
+  for (double *p : t->phi)
+    if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(double) * h->nvar * t->vsF);
+  if (e == cudaSuccess) e = cudaMemset(t->bad, 0, sizeof(int));
+  const long nfp = K * NFF;
+  if (e == cudaSuccess) {
+    adjoint_mapP_kernel<<<(unsigned)((nfp + 255) / 256), 256, 0, s>>>(
+        (int)K, Np, h->Nfp, h->Fmask, h->vmapP, h->vmapF, t->mapP, t->bad);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    adjoint_mapP_check_kernel<<<(unsigned)((nfp + 255) / 256), 256, 0, s>>>(nfp, t->mapP,
+                                                                             t->bad);
+    e = cudaGetLastError();
+  }
+  int bad = 0;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpy(&bad, t->bad, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    free_tape(h);
+    return cuda_check(e, "adjoint setup");
+  }
+  if (bad) {
+    free_tape(h);
+    return set_error(DGLM_ERR_UNSUPPORTED,
+                     "adjoint: face points do not pair up one to one (non-conforming mesh)");
+  }
+  return DGLM_OK;
+}
+
+// Recording-size part: checkpoints, per-step tau and dt, one segment's store.
+dglm_status tape_size(dglm_handle *h, int nsteps, int every) {
+  AdjointTape *t = h->tape;
+  const int nseg = (nsteps + every - 1) / every;
+  const int seg_len = std::min(every, nsteps);
+  const bool euler = h->d.physics == DGLM_EULER;
+  if (nseg <= t->cap_ckpt && nsteps <= t->cap_steps && 5 * seg_len <= t->cap_store) return DGLM_OK;
+  cudaStreamSynchronize(h->stream);
+  for (void *p : t->sized) cudaFree(p);
+  t->sized.clear();
+  t->bytes -= t->sized_bytes;
+  t->sized_bytes = 0;
+  t->cap_ckpt = t->cap_steps = t->cap_store = 0;
+  dglm_status st = DGLM_OK;
+  auto chk = [&](dglm_status s) {
+    if (st == DGLM_OK) st = s;
+  };
+  chk(talloc(t, t->sized, &t->ckpt, (size_t)nseg * t->state));
+  chk(talloc(t, t->sized, &t->dt_dev, (size_t)nsteps));
+  chk(talloc(t, t->sized, &t->tau, (size_t)(euler ? nsteps : 1) * 4 * h->Kp));
+  // slot 0 of a segment is its checkpoint, slots 1..5*seg_len are stored here
+  chk(talloc(t, t->sized, &t->store, (size_t)5 * seg_len * t->state));
+  if (st != DGLM_OK) {
+    for (void *p : t->sized) cudaFree(p);
+    t->sized.clear();
+    t->bytes -= t->sized_bytes;
+    t->sized_bytes = 0;
+    return st;
+  }
+  // zero-filled so the padded tail elements of every stored state stay zero
+  cudaMemset(t->tau, 0, sizeof(double) * (euler ? nsteps : 1) * 4 * h->Kp);
+  cudaMemset(t->ckpt, 0, sizeof(double) * nseg * t->state);
+  cudaMemset(t->store, 0, sizeof(double) * 5 * seg_len * t->state);
+  t->cap_ckpt = nseg;
+  t->cap_steps = nsteps;
+  t->cap_store = 5 * seg_len;
+  return DGLM_OK;
+}
+
+const double *tau_of(const dglm_handle *h, int step) {
+  const AdjointTape *t = h->tape;
+  return h->d.physics == DGLM_EULER ? t->tau + (size_t)step * 4 * h->Kp : t->tau;
+}
+
+AdjArgs adj_args(dglm_handle *h) {
+  AdjointTape *t = h->tape;
+  AdjArgs a{};
+  a.AV = t->AV;
+  a.AL = t->AL;
+  a.geo = h->geo;
+  a.fscale = h->fscale;
+  a.nrm = h->nrm;
+  a.vmapP = h->vmapP;
+  a.vmapF = h->vmapF;
+  a.mapP = t->mapP;
+  a.Fmask = h->Fmask;
+  a.vel = h->vel;
+  a.lam = t->lam;
+  a.lk = t->lk;
+  a.vs = h->vs;
+  a.vsF = t->vsF;
+  a.gstride = h->Kp;
+  a.K = h->d.K;
+  a.gamma = h->d.gamma;
+  return a;
+}
+
+// Forward stage with recorded dt and tau (no wave-speed side effects).
+cudaError_t frozen_stage(dglm_handle *h, const double *u_in, double *u_out, double *k, int s,
+                         double dt, const double *tau, cudaStream_t cs) {
+  StageArgs a = stage_args(h, u_in, u_out, s);
+  a.kreg = k;
+  a.tau = tau;
+  a.dt_override = dt;
+  a.last_stage = 0;
+  return launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, cs);
+}
+
+dglm_status copy_fields(dglm_handle *h, double *dst, const double *const *src, int on_device,
+                        const char *what) {
+  const long n = (long)h->d.K * h->Np;
+  cudaError_t e = cudaSuccess;
+  for (int v = 0; v < h->nvar && e == cudaSuccess; v++) {
+    if (!src[v]) return set_error(DGLM_ERR_INVALID, std::string(what) + ": NULL pointer");
+    e = cudaMemcpyAsync(dst + (size_t)v * h->vs, src[v], sizeof(double) * n,
+                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                        h->stream);
+  }
+  return cuda_check(e, what);
+}
+
+dglm_status fetch_fields(dglm_handle *h, double *const *dst, const double *src, int on_device,
+                         const char *what) {
+  const long n = (long)h->d.K * h->Np;
+  cudaError_t e = cudaSuccess;
+  for (int v = 0; v < h->nvar && e == cudaSuccess; v++) {
+    if (!dst[v]) return set_error(DGLM_ERR_INVALID, std::string(what) + ": NULL pointer");
+    e = cudaMemcpyAsync(dst[v], src + (size_t)v * h->vs, sizeof(double) * n,
+                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                        h->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  return cuda_check(e, what);
+}
+
+}  // namespace
+
+extern "C" {
+
+dglm_status dglm_adjoint_record(dglm_handle *h, int nsteps, int checkpoint_every) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_adjoint_record: NULL handle");
+  if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_adjoint_record: set a state first");
+  if (nsteps <= 0 || checkpoint_every <= 0)
+    return set_error(DGLM_ERR_INVALID,
+                     "dglm_adjoint_record: nsteps and checkpoint_every must be positive");
+  DeviceGuard g(h->dev);
+  dglm_status st = tape_setup(h);
+  if (st == DGLM_OK) st = tape_size(h, nsteps, checkpoint_every);
+  if (st != DGLM_OK) return st;
+  AdjointTape *t = h->tape;
+  t->recorded = false;
+  cudaStream_t s = h->stream;
+  const double zero = 0.0;
+  cudaError_t e = cudaMemcpyAsync(&h->sc->dt_fixed, &zero, sizeof(double),
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record");
+  h->launches = 0;
+  const bool euler = h->d.physics == DGLM_EULER;
+  for (int i = 0; i < nsteps; i++) {
+    const size_t bytes = sizeof(double) * t->state;
+    if (i % checkpoint_every == 0) {
+      e = cudaMemcpyAsync(t->ckpt + (size_t)(i / checkpoint_every) * t->state, h->u[h->cur],
+                          bytes, cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record");
+    }
+    st = run_steps(h, 1);
+    if (st != DGLM_OK) return st;
+    if (euler || i == 0)
+      e = cudaMemcpyAsync(const_cast<double *>(tau_of(h, i)), h->tau,
+                          sizeof(double) * 4 * h->Kp, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(t->dt_dev + i, &h->sc->dt, sizeof(double), cudaMemcpyDeviceToDevice,
+                          s);
+    if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record");
+  }
+  t->dt.assign(nsteps, 0.0);
+  e = cudaMemcpyAsync(t->dt.data(), t->dt_dev, sizeof(double) * nsteps,
+                      cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record");
+  for (double d : t->dt)
+    if (!std::isfinite(d) || d < 0)
+      return set_error(DGLM_ERR_NONFINITE, "dglm_adjoint_record: non-finite dt recorded");
+  t->nsteps = nsteps;
+  t->every = checkpoint_every;
+  t->nseg = (nsteps + checkpoint_every - 1) / checkpoint_every;
+  t->recorded = true;
+  return DGLM_OK;
+}
+
+dglm_status dglm_adjoint_replay(dglm_handle *h) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_adjoint_replay: NULL handle");
+  if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_adjoint_replay: set a state first");
+  if (!h->tape || !h->tape->recorded)
+    return set_error(DGLM_ERR_STATE, "dglm_adjoint_replay: record a forward run first");
+  DeviceGuard g(h->dev);
+  AdjointTape *t = h->tape;
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaMemsetAsync(h->kreg, 0, sizeof(double) * t->state, s);
+  h->launches = 0;
+  for (int i = 0; i < t->nsteps && e == cudaSuccess; i++)
+    for (int st = 0; st < 5 && e == cudaSuccess; st++) {
+      e = frozen_stage(h, h->u[h->cur], h->u[h->cur ^ 1], h->kreg, st, t->dt[i], tau_of(h, i), s);
+      h->cur ^= 1;
+      h->launches++;
+    }
+  return cuda_check(e, "dglm_adjoint_replay");
+}
+
+dglm_status dglm_adjoint_backward(dglm_handle *h, const double *const *lam_T,
+                                  double *const *lam_0, int on_device) {
+  if (!h || !lam_T || !lam_0)
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_backward: NULL argument");
+  if (!h->tape || !h->tape->recorded)
+    return set_error(DGLM_ERR_STATE, "dglm_adjoint_backward: record a forward run first");
+  DeviceGuard g(h->dev);
+  AdjointTape *t = h->tape;
+  cudaStream_t s = h->stream;
+  dglm_status st = copy_fields(h, t->lam, lam_T, on_device, "dglm_adjoint_backward");
+  if (st != DGLM_OK) return st;
+  cudaError_t e = cudaMemsetAsync(t->lk, 0, sizeof(double) * t->state, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->kbuf, 0, sizeof(double) * t->state, s);
+  h->launches = 0;
+  AdjArgs a = adj_args(h);
+  int p = 0;
+  // phi of the first adjoint stage (stage 4 of the last step)
+  a.update = 0;
+  a.phi_next = 1;
+  a.rkb_next = RKB[4];
+  a.phi_out = t->phi[p];
+  if (e == cudaSuccess) e = t->var.launch(a, s);
+  h->launches++;
+  for (int seg = t->nseg - 1; seg >= 0 && e == cudaSuccess; seg--) {
+    const int s0 = seg * t->every, s1 = std::min(s0 + t->every, t->nsteps);
+    double *ck = t->ckpt + (size_t)seg * t->state;
+    auto slot = [&](int j) -> double * {
+      return j == 0 ? ck : t->store + (size_t)(j - 1) * t->state;
+    };
+    // recompute the segment's stage inputs from its checkpoint
+    for (int i = s0; i < s1 && e == cudaSuccess; i++)
+      for (int k = 0; k < 5 && e == cudaSuccess; k++) {
+        const int j = 5 * (i - s0) + k;
+        if (i == s1 - 1 && k == 4) break;   // the last stage's output is not needed
+        e = frozen_stage(h, slot(j), slot(j + 1), t->kbuf, k, t->dt[i], tau_of(h, i), s);
+        h->launches++;
+      }
+    // reverse sweep over the segment
+    for (int i = s1 - 1; i >= s0 && e == cudaSuccess; i--)
+      for (int k = 4; k >= 0 && e == cudaSuccess; k--) {
+        a.update = 1;
+        a.u = slot(5 * (i - s0) + k);
+        a.tau = tau_of(h, i);
+        a.dt = t->dt[i];
+        a.rka = RKA[k];
+        a.rkb = RKB[k];
+        const bool last = (i == 0 && k == 0);
+        a.phi_next = last ? 0 : 1;
+        a.rkb_next = k > 0 ? RKB[k - 1] : RKB[4];
+        a.phi_in = t->phi[p];
+        a.phi_out = t->phi[p ^ 1];
+        e = t->var.launch(a, s);
+        h->launches++;
+        p ^= 1;
+      }
+  }
+  if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_backward");
+  return fetch_fields(h, lam_0, t->lam, on_device, "dglm_adjoint_backward");
+}
+
+dglm_status dglm_adjoint_rhs(dglm_handle *h, const double *const *u, const double *const *mu,
+                             double *const *out) {
+  if (!h || !u || !mu || !out) return set_error(DGLM_ERR_INVALID, "dglm_adjoint_rhs: NULL argument");
+  if (!h->mesh_ready) return set_error(DGLM_ERR_STATE, "dglm_adjoint_rhs: upload the mesh first");
+  DeviceGuard g(h->dev);
+  dglm_status st = tape_setup(h);
+  if (st == DGLM_OK) st = ensure_rhs_scratch(h);
+  if (st != DGLM_OK) return st;
+  AdjointTape *t = h->tape;
+  cudaStream_t s = h->stream;
+  // tau of u, as dglm_rhs computes it
+  st = copy_fields(h, h->rhs_in, u, 1, "dglm_adjoint_rhs");
+  if (st == DGLM_OK) st = copy_fields(h, t->lk, mu, 1, "dglm_adjoint_rhs");
+  if (st != DGLM_OK) return st;
+  cudaError_t e = cudaMemsetAsync(h->sc_s, 0, sizeof(DevScalars), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->lam, 0, sizeof(double) * t->state, s);
+  StageArgs sa = stage_args(h, h->rhs_in, h->rhs_out, -1);
+  sa.maxv = h->maxv_s;
+  sa.tau = h->tau_s;
+  sa.sc = h->sc_s;
+  if (e == cudaSuccess) e = launch_face_maxv(h->d.physics, h->d.N, sa, 0, s);
+  if (e == cudaSuccess) e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv_s, h->tau_s, s);
+  AdjArgs a = adj_args(h);
+  a.u = h->rhs_in;
+  a.tau = h->tau_s;
+  // phi of mu (mu = lk + 0 lam), then lam = 0 + 1 * R'(u)^T mu
+  a.update = 0;
+  a.phi_next = 1;
+  a.rkb_next = 0.0;
+  a.phi_out = t->phi[0];
+  if (e == cudaSuccess) e = t->var.launch(a, s);
+  a.update = 1;
+  a.phi_next = 0;
+  a.dt = 1.0;
+  a.rka = 0.0;
+  a.rkb = 0.0;
+  a.phi_in = t->phi[0];
+  a.phi_out = t->phi[1];
+  if (e == cudaSuccess) e = t->var.launch(a, s);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_rhs");
+  return fetch_fields(h, out, t->lam, 1, "dglm_adjoint_rhs");
+}
+
+dglm_status dglm_adjoint_tape_bytes(dglm_handle *h, size_t *bytes) {
+  if (!h || !bytes) return set_error(DGLM_ERR_INVALID, "dglm_adjoint_tape_bytes: NULL argument");
+  *bytes = h->tape ? h->tape->bytes : 0;
+  return DGLM_OK;
+}
+
+}  // extern "C"

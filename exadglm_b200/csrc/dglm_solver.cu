@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "dglm_common.cuh"
+#include "dglm_handle.cuh"
 
 namespace dglm {
 
@@ -32,73 +33,7 @@ dglm_status cuda_check(cudaError_t e, const char *what) {
 
 using namespace dglm;
 
-struct dglm_handle {
-  dglm_desc d{};
-  int nvar = 0, Np = 0, Nfp = 0, NFF = 0;
-  int variant = 0;
-  StageVariantInfo vinfo{};
-  std::vector<double> Ahost;      // stacked [WDr WDs WDt -LIFT], Np x (3Np+NFF) row-major
-  long vs = 0;                    // doubles between variables of a field
-  long Kp = 0;                    // K rounded up to a multiple of 64 (tile padding)
-  int dev = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  // mesh, operators
-  double *AT = nullptr, *geo = nullptr, *fscale = nullptr, *nrm = nullptr;
-  double *tau = nullptr, *maxv = nullptr, *vel = nullptr;
-  int *vmapP = nullptr, *vmapF = nullptr, *Fmask = nullptr;
-  // state
-  double *u[2] = {nullptr, nullptr};
-  double *kreg = nullptr;
-  int cur = 0;
-  DevScalars *sc = nullptr;
-  double *dt_hist = nullptr;
-  // one-off right-hand side evaluation
-  double *rhs_in = nullptr, *rhs_out = nullptr, *maxv_s = nullptr, *tau_s = nullptr;
-  DevScalars *sc_s = nullptr;
-  bool mesh_ready = false, state_ready = false;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  long launches = 0;
-  size_t bytes = 0;
-  std::vector<void *> allocs;
-};
-
 namespace {
-
-// Carpenter & Kennedy 5-stage 4th-order 2N-storage coefficients
-// (euler_data.cpp:41-60).
-const double RKA[5] = {0.0, -567301805773.0 / 1357537059087.0,
-                       -2404267990393.0 / 2016746695238.0, -3550918686646.0 / 2091501179385.0,
-                       -1275806237668.0 / 842570457699.0};
-const double RKB[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
-                       1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
-                       2277821191437.0 / 14882151754819.0};
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (dev >= 0 && dev != prev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
-
-template <typename T>
-dglm_status dalloc(dglm_handle *h, T **p, size_t count) {
-  void *q = nullptr;
-  const size_t n = count * sizeof(T);
-  cudaError_t e = cudaMalloc(&q, n ? n : 16);
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return set_error(DGLM_ERR_NOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
-  }
-  h->allocs.push_back(q);
-  h->bytes += n;
-  *p = static_cast<T *>(q);
-  return DGLM_OK;
-}
 
 void drop_graphs(dglm_handle *h) {
   for (auto &g : h->graph) {
@@ -119,7 +54,9 @@ bool in_range(const int *a, size_t n, long lo, long hi) {
   return true;
 }
 
-StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
+}  // namespace
+
+StageArgs dglm::stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
   StageArgs a{};
   a.AT = h->AT;
   a.geo = h->geo;
@@ -145,6 +82,8 @@ StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s) {
   a.dt_override = -1.0;
   return a;
 }
+
+namespace {
 
 // Doubles of the device operator copy for a variant's layout.
 size_t op_doubles(const StageVariantInfo &v, int Np, int NFF) {
@@ -278,6 +217,22 @@ dglm_status issue_step(dglm_handle *h, int cur, cudaStream_t s) {
 
 }  // namespace
 
+// Scratch of the one-off right-hand-side evaluations (dglm_rhs,
+// dglm_adjoint_rhs), allocated on first use.
+dglm_status dglm::ensure_rhs_scratch(dglm_handle *h) {
+  if (h->rhs_in) return DGLM_OK;
+  dglm_status st = dalloc(h, &h->rhs_in, (size_t)h->nvar * h->vs);
+  if (st == DGLM_OK) st = dalloc(h, &h->rhs_out, (size_t)h->nvar * h->vs);
+  if (st == DGLM_OK) st = dalloc(h, &h->maxv_s, (size_t)4 * h->Kp);
+  if (st == DGLM_OK) st = dalloc(h, &h->tau_s, (size_t)4 * h->Kp);
+  if (st == DGLM_OK) st = dalloc(h, &h->sc_s, 1);
+  if (st != DGLM_OK) return st;
+  cudaError_t e = cudaMemset(h->rhs_in, 0, sizeof(double) * h->nvar * h->vs);
+  if (e == cudaSuccess) e = cudaMemset(h->maxv_s, 0, sizeof(double) * 4 * h->Kp);
+  if (e == cudaSuccess) e = cudaMemset(h->tau_s, 0, sizeof(double) * 4 * h->Kp);
+  return cuda_check(e, "rhs scratch");
+}
+
 extern "C" {
 
 const char *dglm_last_error(void) { return g_last_error.c_str(); }
@@ -376,6 +331,7 @@ dglm_status dglm_destroy(dglm_handle *h) {
   DeviceGuard g(h->dev);
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
+  free_tape(h);
   for (void *p : h->allocs) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -455,6 +411,7 @@ dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *m) {
 
   DeviceGuard g(h->dev);
   cudaStreamSynchronize(h->stream);
+  free_tape(h);   // the adjoint's operators and face pairing belong to the old mesh
   const auto H2D = cudaMemcpyHostToDevice;
   dglm_status os = upload_operator_layout(h);
   if (os != DGLM_OK) return os;
@@ -525,7 +482,9 @@ dglm_status dglm_get_state(dglm_handle *h, double *const *u, int on_device) {
   return cuda_check(e, "dglm_get_state");
 }
 
-static dglm_status run_steps(dglm_handle *h, int nsteps) {
+}  // extern "C"
+
+dglm_status dglm::run_steps(dglm_handle *h, int nsteps) {
   if (!h) return set_error(DGLM_ERR_INVALID, "dglm_step: NULL handle");
   if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_step: set a state first");
   if (nsteps < 0) return set_error(DGLM_ERR_INVALID, "dglm_step: negative step count");
@@ -560,6 +519,8 @@ static dglm_status run_steps(dglm_handle *h, int nsteps) {
   }
   return DGLM_OK;
 }
+
+extern "C" {
 
 dglm_status dglm_step(dglm_handle *h, int nsteps) {
   if (!h) return set_error(DGLM_ERR_INVALID, "dglm_step: NULL handle");
@@ -645,19 +606,8 @@ dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs)
   if (!h || !u || !rhs) return set_error(DGLM_ERR_INVALID, "dglm_rhs: NULL argument");
   if (!h->mesh_ready) return set_error(DGLM_ERR_STATE, "dglm_rhs: upload the mesh first");
   DeviceGuard g(h->dev);
-  dglm_status st = DGLM_OK;
-  if (!h->rhs_in) {
-    const long K = h->d.K;
-    st = dalloc(h, &h->rhs_in, (size_t)h->nvar * h->vs);
-    if (st == DGLM_OK) st = dalloc(h, &h->rhs_out, (size_t)h->nvar * h->vs);
-    if (st == DGLM_OK) st = dalloc(h, &h->maxv_s, (size_t)4 * h->Kp);
-    if (st == DGLM_OK) st = dalloc(h, &h->tau_s, (size_t)4 * h->Kp);
-    if (st == DGLM_OK) st = dalloc(h, &h->sc_s, 1);
-    if (st != DGLM_OK) return st;
-    cudaMemset(h->rhs_in, 0, sizeof(double) * h->nvar * h->vs);
-    cudaMemset(h->maxv_s, 0, sizeof(double) * 4 * h->Kp);
-    cudaMemset(h->tau_s, 0, sizeof(double) * 4 * h->Kp);
-  }
+  dglm_status st = ensure_rhs_scratch(h);
+  if (st != DGLM_OK) return st;
   cudaStream_t s = h->stream;
   const long n = (long)h->d.K * h->Np;
   cudaError_t e = cudaSuccess;

@@ -190,6 +190,35 @@ dglm_status dglm_lserk_stage(int N, int nvar, int nelem, double dt, double rka, 
                              const double *const *utmp, double *const *k, double *const *u,
                              void *stream);
 
+/* ---- discrete adjoint ----------------------------------------------------
+ * No counterpart in the reference (it has no adjoint).  Gradients of an
+ * objective of the final state with respect to the initial state, for FP64
+ * handles, with dt and the face penalty tau frozen at the values of the
+ * recorded forward run (both are non-smooth maxima of the state).
+ *
+ * dglm_adjoint_record: nsteps CFL steps (as dglm_step) from the current
+ * state, storing the state every checkpoint_every steps and each step's dt
+ * and tau on the device.  The state afterwards is the final state, as after
+ * dglm_step.  Device memory: (ceil(nsteps/every) + 5 min(every, nsteps))
+ * states plus nsteps x 4K doubles of tau (Euler).
+ * dglm_adjoint_backward: lam_0 = (du_T/du_0)^T lam_T for the recorded run.
+ * Each checkpoint segment is recomputed once (its 5 stage inputs per step
+ * kept), then swept in reverse: one launch per stage.  nvar pointers each,
+ * host or device (on_device).
+ * dglm_adjoint_replay: the recorded run again from the current state with
+ * the recorded dt and tau (for finite-difference checks); the simulated time
+ * is not advanced.
+ * dglm_adjoint_rhs: out = R'(u)^T mu on device fields, tau computed from u
+ * as dglm_rhs does.  Errors: DGLM_ERR_UNSUPPORTED for mixed precision, for
+ * N > 6, or for a mesh whose face points do not pair one to one. */
+dglm_status dglm_adjoint_record(dglm_handle *h, int nsteps, int checkpoint_every);
+dglm_status dglm_adjoint_backward(dglm_handle *h, const double *const *lam_T,
+                                  double *const *lam_0, int on_device);
+dglm_status dglm_adjoint_replay(dglm_handle *h);
+dglm_status dglm_adjoint_rhs(dglm_handle *h, const double *const *u, const double *const *mu,
+                             double *const *out);
+dglm_status dglm_adjoint_tape_bytes(dglm_handle *h, size_t *bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,10 @@ def lib():
         L.orc_run.argtypes = [P, P, P, P, C.c_int, C.c_double, P]
         L.orc_lserk_stage.argtypes = [P, C.c_double, C.c_double, C.c_double, P, P, P]
         L.orc_num_threads.restype = C.c_int
+        L.orc_run_record.argtypes = [P, P, P, C.c_int, P, P]
+        L.orc_run_frozen.argtypes = [P, P, P, C.c_int, P, P]
+        L.orc_rhs_adjoint.argtypes = [P, P, P, P, P]
+        L.orc_adjoint.argtypes = [P, P, C.c_int, P, P, P]
         _lib = L
     return _lib
 
@@ -136,6 +140,65 @@ class Oracle:
                                                    "fluxS", "fluxT", "utmp")])
         out["dt"] = dt
         return out
+
+    # ---- discrete adjoint (frozen dt and tau) ------------------------------
+
+    def run_record(self, nsteps, u=None):
+        """Forward run recording dt and tau per step.  Returns (u, dt_hist,
+        tau_hist[nsteps, 4K])."""
+        p = self.p
+        u = np.array(p.u0 if u is None else u, dtype=np.float64, order="C").reshape(p.nvar, -1)
+        k = np.zeros_like(u)
+        dt = np.zeros(nsteps)
+        tau = np.zeros((nsteps, 4 * p.K))
+        self.L.orc_run_record(self._m(), _ptr(u), _ptr(k), int(nsteps), _ptr(dt), _ptr(tau))
+        return u, dt, tau
+
+    def run_frozen(self, u, dt_hist, tau_hist):
+        """Forward run replaying recorded dt and tau (from k = 0)."""
+        p = self.p
+        u = np.array(u, dtype=np.float64, order="C").reshape(p.nvar, -1)
+        k = np.zeros_like(u)
+        dt = np.ascontiguousarray(dt_hist, dtype=np.float64)
+        tau = np.ascontiguousarray(tau_hist, dtype=np.float64)
+        self.L.orc_run_frozen(self._m(), _ptr(u), _ptr(k), len(dt), _ptr(dt), _ptr(tau))
+        return u
+
+    def rhs_frozen(self, u, tau):
+        """R(u) with the face penalty tau given (update_ub, calc_fluxLM,
+        calc_fluxes, update_rhs)."""
+        p = self.p
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(p.nvar, -1)
+        tau = np.ascontiguousarray(tau, dtype=np.float64)
+        nT, nV = p.nvar * p.K * 4 * p.Nfp, p.nvar * p.K * p.Np
+        ub, fLM = np.zeros(nT), np.zeros(nT)
+        fR, fS, fT, out = np.zeros(nV), np.zeros(nV), np.zeros(nV), np.zeros(nV)
+        L, m = self.L, self._m()
+        L.orc_update_ub(m, _ptr(u), _ptr(ub))
+        L.orc_calc_fluxLM(m, _ptr(u), _ptr(ub), _ptr(tau), _ptr(fLM))
+        L.orc_calc_fluxes(m, _ptr(u), _ptr(fR), _ptr(fS), _ptr(fT))
+        L.orc_update_rhs(m, _ptr(fR), _ptr(fS), _ptr(fT), _ptr(fLM), _ptr(out))
+        return out.reshape(p.nvar, -1)
+
+    def rhs_adjoint(self, u, tau, mu):
+        """R'(u)^T mu with tau frozen."""
+        p = self.p
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(p.nvar, -1)
+        mu = np.ascontiguousarray(mu, dtype=np.float64).reshape(p.nvar, -1)
+        tau = np.ascontiguousarray(tau, dtype=np.float64)
+        lam = np.zeros_like(u)
+        self.L.orc_rhs_adjoint(self._m(), _ptr(u), _ptr(tau), _ptr(mu), _ptr(lam))
+        return lam
+
+    def adjoint(self, u0, dt_hist, tau_hist, lam_T):
+        """dJ/du(0) from dJ/du(T) = lam_T for the frozen run from u0."""
+        p = self.p
+        u0 = np.ascontiguousarray(u0, dtype=np.float64).reshape(p.nvar, -1)
+        lam = np.array(lam_T, dtype=np.float64, order="C").reshape(p.nvar, -1)
+        dt = np.ascontiguousarray(dt_hist, dtype=np.float64)
+        tau = np.ascontiguousarray(tau_hist, dtype=np.float64)
+        self.L.orc_adjoint(self._m(), _ptr(u0), len(dt), _ptr(dt), _ptr(tau), _ptr(lam))
+        return lam
 
     @staticmethod
     def threads():

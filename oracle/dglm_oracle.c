@@ -307,3 +307,176 @@ int orc_num_threads(void) {
     return 1;
 #endif
 }
+
+/* ---------------------------------------------------------------------------
+ * Discrete adjoint (test infrastructure): the transpose of the derivative of
+ * runRK with dt and tau frozen (recorded in the forward run and replayed),
+ * for checking the GPU adjoint.  The reference has no adjoint; this is the
+ * exact derivative of the oracle's own step above.
+ * ------------------------------------------------------------------------- */
+
+/* w = A_n(q)^T g for the Euler flux in direction n (the Jacobian of
+ * F.n with p = (gamma-1)(E - |m|^2/(2 rho)), the reference's flux). */
+static void euler_jac_t(double gm, const double q[5], const double n[3], const double g[5],
+                        double w[5]) {
+    double ir = 1.0 / q[0], u[3] = {q[1] * ir, q[2] * ir, q[3] * ir};
+    double q2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    double p = (gm - 1) * (q[4] - 0.5 * q[0] * q2);
+    double H = (q[4] + p) * ir;
+    double un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+    double gu = g[1] * u[0] + g[2] * u[1] + g[3] * u[2];
+    double gn = g[1] * n[0] + g[2] * n[1] + g[3] * n[2];
+    double phi = 0.5 * (gm - 1) * q2;
+    w[0] = -un * gu + phi * gn + g[4] * un * (phi - H);
+    for (int j = 0; j < 3; j++)
+        w[1 + j] = g[0] * n[j] + un * g[1 + j] + gu * n[j] - (gm - 1) * gn * u[j] +
+                   g[4] * (H * n[j] - (gm - 1) * un * u[j]);
+    w[4] = (gm - 1) * gn + gm * un * g[4];
+}
+
+/* lam += R'(u)^T mu with tau frozen. */
+void orc_rhs_adjoint(const orc_mesh *m, const double *u, const double *tau, const double *mu,
+                     double *lam) {
+    const long K = m->K, Np = m->Np, Nfp = m->Nfp, NF = 4 * Nfp, n = K * Np;
+    const int nv = m->nvar;
+    double *nu = malloc(sizeof(double) * 3 * Np * nv), *phi = malloc(sizeof(double) * NF * nv);
+    for (long e = 0; e < K; e++) {
+        /* nu_d = WD_d^T mu, phi = -LIFT^T mu (per variable) */
+        for (int v = 0; v < nv; v++) {
+            const double *mv = mu + v * n + e * Np;
+            for (long j = 0; j < Np; j++) {
+                double a0 = 0, a1 = 0, a2 = 0;
+                for (long i = 0; i < Np; i++) {
+                    a0 += m->WDr[i * Np + j] * mv[i];
+                    a1 += m->WDs[i * Np + j] * mv[i];
+                    a2 += m->WDt[i * Np + j] * mv[i];
+                }
+                nu[(v * 3 + 0) * Np + j] = a0;
+                nu[(v * 3 + 1) * Np + j] = a1;
+                nu[(v * 3 + 2) * Np + j] = a2;
+            }
+            for (long f = 0; f < NF; f++) {
+                double s = 0;
+                for (long i = 0; i < Np; i++) s -= m->LIFT[i * NF + f] * mv[i];
+                phi[v * NF + f] = s;
+            }
+        }
+        /* volume: lam_j += sum_x A_x(u_j)^T G_x, G_x = r_x nu_r + s_x nu_s + t_x nu_t */
+        const double mt[3][3] = {{m->rx[e], m->ry[e], m->rz[e]},
+                                 {m->sx[e], m->sy[e], m->sz[e]},
+                                 {m->tx[e], m->ty[e], m->tz[e]}};
+        for (long j = 0; j < Np; j++) {
+            long idx = e * Np + j;
+            for (int x = 0; x < 3; x++) {
+                double G[5];
+                for (int v = 0; v < nv; v++)
+                    G[v] = mt[0][x] * nu[(v * 3 + 0) * Np + j] + mt[1][x] * nu[(v * 3 + 1) * Np + j] +
+                           mt[2][x] * nu[(v * 3 + 2) * Np + j];
+                if (m->physics == ORC_EULER) {
+                    double q[5], w[5], dir[3] = {0, 0, 0};
+                    dir[x] = 1;
+                    for (int v = 0; v < 5; v++) q[v] = u[v * n + idx];
+                    euler_jac_t(m->gamma, q, dir, G, w);
+                    for (int v = 0; v < 5; v++) lam[v * n + idx] += w[v];
+                } else {
+                    const double *vel = x == 0 ? m->vx : x == 1 ? m->vy : m->vz;
+                    lam[idx] += vel[idx] * G[0];
+                }
+            }
+        }
+        /* faces: d fluxLM/du- = fs (A_n(ub)/2 + tau/2), d fluxLM/du+ = fs (A_n(ub)/2 - tau/2) */
+        for (long fj = 0; fj < NF; fj++) {
+            long f = fj / Nfp, gf = e * 4 + f, idx = e * NF + fj;
+            long iM = e * Np + m->Fmask[fj], iP = m->vmapP[idx];
+            double fs = m->Fscale[gf], ta = tau[gf];
+            double nrm[3] = {m->nx[gf], m->ny[gf], m->nz[gf]};
+            if (m->physics == ORC_EULER) {
+                double qb[5], g[5], w[5];
+                for (int v = 0; v < 5; v++) {
+                    qb[v] = 0.5 * (u[v * n + iM] + u[v * n + iP]);
+                    g[v] = phi[v * NF + fj];
+                }
+                euler_jac_t(m->gamma, qb, nrm, g, w);
+                for (int v = 0; v < 5; v++) {
+                    lam[v * n + iM] += fs * (0.5 * w[v] + 0.5 * ta * g[v]);
+                    lam[v * n + iP] += fs * (0.5 * w[v] - 0.5 * ta * g[v]);
+                }
+            } else {
+                double an = nrm[0] * m->vx[iM] + nrm[1] * m->vy[iM] + nrm[2] * m->vz[iM];
+                double g = phi[fj];
+                lam[iM] += fs * (0.5 * an + 0.5 * ta) * g;
+                lam[iP] += fs * (0.5 * an - 0.5 * ta) * g;
+            }
+        }
+    }
+    free(nu);
+    free(phi);
+}
+
+/* One LSERK step from u with the given dt and tau (no tmax clipping);
+ * stage_in (5 states) receives the input state of every stage. */
+static void frozen_step(const orc_mesh *m, double *u, double *k, double dt, const double *tau,
+                        double *stage_in) {
+    const size_t nV = (size_t)m->nvar * m->K * m->Np, nT = (size_t)m->nvar * m->K * 4 * m->Nfp;
+    double *ub = xmalloc(nT * 8), *fLM = xmalloc(nT * 8), *fR = xmalloc(nV * 8),
+           *fS = xmalloc(nV * 8), *fT = xmalloc(nV * 8), *ut = xmalloc(nV * 8);
+    for (int s = 0; s < 5; s++) {
+        if (stage_in) memcpy(stage_in + s * nV, u, nV * 8);
+        orc_update_ub(m, u, ub);
+        orc_calc_fluxLM(m, u, ub, tau, fLM);
+        orc_calc_fluxes(m, u, fR, fS, fT);
+        orc_update_rhs(m, fR, fS, fT, fLM, ut);
+        orc_lserk_stage(m, dt, RKA[s], RKB[s], ut, k, u);
+    }
+    free(ub); free(fLM); free(fR); free(fS); free(fT); free(ut);
+}
+
+/* Forward run recording dt and tau of every step (tau_hist: nsteps x 4K). */
+int orc_run_record(const orc_mesh *m, double *u, double *k, int nsteps, double *dt_hist,
+                   double *tau_hist) {
+    const size_t nF = (size_t)m->K * 4;
+    double *maxv = xmalloc(nF * 8), *maxv_fs = xmalloc(nF * 8);
+    for (int st = 0; st < nsteps; st++) {
+        orc_calc_maxv(m, u, maxv, maxv_fs);
+        dt_hist[st] = orc_calc_dt(m, maxv_fs);
+        orc_update_tau(m, maxv, tau_hist + st * nF);
+        frozen_step(m, u, k, dt_hist[st], tau_hist + st * nF, NULL);
+    }
+    free(maxv); free(maxv_fs);
+    return nsteps;
+}
+
+/* Forward run replaying recorded dt and tau. */
+void orc_run_frozen(const orc_mesh *m, double *u, double *k, int nsteps, const double *dt_hist,
+                    const double *tau_hist) {
+    const size_t nF = (size_t)m->K * 4;
+    for (int st = 0; st < nsteps; st++) frozen_step(m, u, k, dt_hist[st], tau_hist + st * nF, NULL);
+}
+
+/* Reverse sweep: lam holds dJ/du(T) on entry and dJ/du(0) on return, for the
+ * frozen run of nsteps from u0. */
+void orc_adjoint(const orc_mesh *m, const double *u0, int nsteps, const double *dt_hist,
+                 const double *tau_hist, double *lam) {
+    const size_t nV = (size_t)m->nvar * m->K * m->Np, nF = (size_t)m->K * 4;
+    double *starts = xmalloc(nV * 8 * (size_t)nsteps), *u = xmalloc(nV * 8), *k = xmalloc(nV * 8);
+    double *stage_in = xmalloc(nV * 8 * 5), *lk = xmalloc(nV * 8), *mu = xmalloc(nV * 8);
+    memcpy(u, u0, nV * 8);
+    memset(k, 0, nV * 8);
+    for (int st = 0; st < nsteps; st++) {
+        memcpy(starts + st * nV, u, nV * 8);
+        frozen_step(m, u, k, dt_hist[st], tau_hist + st * nF, NULL);
+    }
+    for (int st = nsteps - 1; st >= 0; st--) {
+        memcpy(u, starts + st * nV, nV * 8);
+        memset(k, 0, nV * 8);      /* k is reset by rka[0] = 0 */
+        frozen_step(m, u, k, dt_hist[st], tau_hist + st * nF, stage_in);
+        memset(lk, 0, nV * 8);
+        for (int s = 4; s >= 0; s--) {
+            for (size_t i = 0; i < nV; i++) mu[i] = lk[i] + RKB[s] * lam[i];
+            for (size_t i = 0; i < nV; i++) lk[i] = RKA[s] * mu[i];
+            for (size_t i = 0; i < nV; i++) mu[i] *= dt_hist[st];
+            orc_rhs_adjoint(m, stage_in + s * nV, tau_hist + st * nF, mu, lam);
+        }
+    }
+    free(starts); free(u); free(k); free(stage_in); free(lk); free(mu);
+}

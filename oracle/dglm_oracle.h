@@ -40,6 +40,14 @@ double orc_rhs(const orc_mesh *m, const double *u, double *maxv, double *tau, do
 int orc_run(const orc_mesh *m, double *u, double *k, orc_clock *clk, int nsteps, double dt_fixed,
             double *dt_hist);
 int orc_num_threads(void);
+void orc_rhs_adjoint(const orc_mesh *m, const double *u, const double *tau, const double *mu,
+                     double *lam);
+int orc_run_record(const orc_mesh *m, double *u, double *k, int nsteps, double *dt_hist,
+                   double *tau_hist);
+void orc_run_frozen(const orc_mesh *m, double *u, double *k, int nsteps, const double *dt_hist,
+                    const double *tau_hist);
+void orc_adjoint(const orc_mesh *m, const double *u0, int nsteps, const double *dt_hist,
+                 const double *tau_hist, double *lam);
 
 #ifdef __cplusplus
 }

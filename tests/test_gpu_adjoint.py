@@ -1,0 +1,145 @@
+"""Discrete adjoint on the GPU (dglm_adjoint_*) against the oracle's adjoint
+and against central finite differences of the GPU's own frozen-dt/tau run.
+
+Tolerances: the adjoint right-hand side and the reverse sweep agree with the
+oracle to 1e-11 relative L2 (FP64, different summation order); the gradient
+of J = 1/2 ||rho(T) - rho_target||^2 matches central differences to 1e-6
+relative (best step over 1e-4 .. 1e-7); checkpoint spacing changes nothing
+(bit-identical, the recomputation is deterministic)."""
+import numpy as np
+import pytest
+
+import oracle
+from exadglm_b200 import problem as P
+from exadglm_b200.capi import DglmError, Solver
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-11
+SWEEP_TOL = 1e-10
+FD_TOL = 1e-6
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+def make(phys, N, n=3):
+    if phys == "euler":
+        return P.euler_sine(n=n, N=N, noise=1e-3, seed=N)
+    return P.advection_gaussian(n=n, N=N, width2=0.05)
+
+
+@pytest.mark.parametrize("phys", ["euler", "advection"])
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6])
+def test_adjoint_rhs_matches_oracle(phys, N):
+    import torch
+    prob = make(phys, N)
+    O = oracle.Oracle(prob)
+    rng = np.random.default_rng(N)
+    u0 = prob.u0.reshape(prob.nvar, -1)
+    mu = rng.standard_normal(u0.shape)
+    ref = O.rhs_adjoint(u0, O.rhs(u0)["tau"], mu)
+    s = Solver(prob, variant=-1)
+    ut = torch.tensor(u0, device="cuda")
+    mt = torch.tensor(mu, device="cuda")
+    out = torch.empty_like(ut)
+    nv = prob.nvar
+    s.adjoint_rhs_device([ut[v].data_ptr() for v in range(nv)],
+                         [mt[v].data_ptr() for v in range(nv)],
+                         [out[v].data_ptr() for v in range(nv)])
+    err = rel(out.cpu().numpy(), ref)
+    print(f"{phys} N={N}: adjoint rhs rel L2 {err:.2e}")
+    assert err < RHS_TOL, err
+    s.close()
+
+
+@pytest.mark.parametrize("phys,N", [("euler", 4), ("euler", 2), ("advection", 3)])
+def test_reverse_sweep_matches_oracle(phys, N):
+    prob = make(phys, N)
+    O = oracle.Oracle(prob)
+    rng = np.random.default_rng(11)
+    u0 = prob.u0.reshape(prob.nvar, -1)
+    nsteps = 7
+    _, dt, tau = O.run_record(nsteps, u0)
+    lamT = rng.standard_normal(u0.shape)
+    ref = O.adjoint(u0, dt, tau, lamT)
+    s = Solver(prob, variant=-1)
+    s.set_state(u0)
+    s.adjoint_record(nsteps, 3)
+    got = s.adjoint_backward(lamT)
+    err = rel(got, ref)
+    print(f"{phys} N={N}: {nsteps}-step adjoint rel L2 vs oracle {err:.2e}")
+    assert err < SWEEP_TOL, err
+    s.close()
+
+
+def test_checkpoint_spacing_and_replay_are_exact():
+    prob = make("euler", 3)
+    rng = np.random.default_rng(5)
+    u0 = prob.u0.reshape(prob.nvar, -1)
+    lamT = rng.standard_normal(u0.shape)
+    s = Solver(prob, variant=-1)
+    grads, finals = [], []
+    for every in (1, 4, 10, 50):
+        s.set_state(u0)
+        s.adjoint_record(10, every)
+        finals.append(s.get_state())
+        grads.append(s.adjoint_backward(lamT))
+    for g in grads[1:]:
+        assert np.array_equal(g, grads[0])
+    for f in finals[1:]:
+        assert np.array_equal(f, finals[0])
+    # replaying the recorded dt and tau from u0 reproduces the recorded run
+    s.set_state(u0)
+    s.adjoint_replay()
+    assert np.array_equal(s.get_state(), finals[0])
+    s.close()
+
+
+@pytest.mark.parametrize("phys,N", [("euler", 4), ("advection", 3)])
+def test_gradient_matches_finite_differences(phys, N):
+    import torch
+    from exadglm_b200.adjoint import density_misfit, evolve
+    prob = make(phys, N)
+    nv, n = prob.nvar, prob.K * prob.Np
+    nsteps = 20
+    s = Solver(prob, variant=-1)
+    u0 = torch.tensor(prob.u0.reshape(nv, -1), device="cuda")
+    rng = np.random.default_rng(3)
+    target = torch.tensor(prob.u0.reshape(nv, -1)[0] * (1 + 0.01 * rng.standard_normal(n)),
+                          device="cuda")
+    x = u0.clone().requires_grad_(True)
+    J = density_misfit(evolve(x, s, nsteps, checkpoint_every=6), target)
+    J.backward()
+    grad = x.grad.detach().cpu().numpy()
+
+    def J_replay(u):
+        s.set_state(u)
+        s.adjoint_replay()
+        uT = s.get_state()
+        d = uT[0] - target.cpu().numpy()
+        return 0.5 * float(np.dot(d, d))
+
+    base = prob.u0.reshape(nv, -1)
+    best = []
+    for k in range(4):
+        d = np.random.default_rng(100 + k).standard_normal(base.shape) * np.abs(base).max()
+        an = float(np.sum(grad * d))
+        errs = []
+        for h in (1e-4, 1e-5, 1e-6, 1e-7):
+            fd = (J_replay(base + h * d) - J_replay(base - h * d)) / (2 * h)
+            errs.append(abs(fd - an) / abs(an))
+        best.append(min(errs))
+        print(f"{phys} N={N} direction {k}: FD rel errors {['%.1e' % e for e in errs]}")
+    assert max(best) < FD_TOL, best
+    s.close()
+
+
+def test_mixed_precision_handle_has_no_adjoint():
+    prob = make("euler", 4)
+    s = Solver(prob, precision="tf32x3", variant=-1)
+    s.set_state(prob.u0)
+    with pytest.raises(DglmError):
+        s.adjoint_record(2, 1)
+    s.close()
