@@ -27,6 +27,7 @@ EXPORTS = (
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
     "dglm_set_variant", "dglm_get_variant", "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
+    "dglm_calc_maxv_dt_static",
 )
 
 
@@ -95,6 +96,8 @@ def lib():
         L.dglm_calc_fluxes.argtypes = [I, I, I, D, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         L.dglm_update_rhs.argtypes = [I, I, I, _P, _P, _P, _P, C.c_char, _P, _P, _P, _P, _P, _P]
         L.dglm_lserk_stage.argtypes = [I, I, I, D, D, D, _P, _P, _P, _P]
+        L.dglm_calc_maxv_dt_static.argtypes = [I, I, I, D, D, _P, _P, _P, _P, _P, _P, _P, _P,
+                                               _P]
         L.dglm_adjoint_record.argtypes = [_P, I, I]
         L.dglm_adjoint_backward.argtypes = [_P, _P, _P, I]
         L.dglm_adjoint_replay.argtypes = [_P]

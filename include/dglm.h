@@ -190,6 +190,27 @@ dglm_status dglm_lserk_stage(int N, int nvar, int nelem, double dt, double rka, 
                              const double *const *utmp, double *const *k, double *const *u,
                              void *stream);
 
+/* No counterpart in the reference.  calc_maxv followed by calc_dt (as
+ * dglm_calc_maxv + dglm_calc_dt) without the caller-owned maxv_fs array:
+ * writes maxv (4*nelem doubles) and dt (*dt_dev, device).  Allocates
+ * nothing: per-block partial maxima live in a 512 KiB file-scope device
+ * array, so nelem is limited to DGLM_MAXV_DT_STATIC_MAX_ELEMENTS (larger
+ * meshes: DGLM_ERR_INVALID).  For callers whose device memory is owned by
+ * another allocator (a framework's caching pool holding the HBM) or whose
+ * time loop must not call cudaMalloc/cudaFree (cudaFree synchronises the
+ * device and stalls work queued on other streams), and so cannot provide
+ * the 4*nelem-double intermediate.  Nothing in the scratch needs to start at
+ * zero.  The first call on a device looks the scratch up (and may load the
+ * module): make it before any stream capture.  Calls that overlap on one
+ * device (other streams, other host threads) share the scratch and race:
+ * serialise them. */
+#define DGLM_MAXV_DT_STATIC_MAX_ELEMENTS 4194304
+dglm_status dglm_calc_maxv_dt_static(int physics, int N, int nelem, double gamma, double cfl,
+                                     const int *Fmask, const double *Fscale,
+                                     const double *const *u, const double *vx,
+                                     const double *vy, const double *vz, double *maxv,
+                                     double *dt_dev, void *stream);
+
 /* ---- discrete adjoint ----------------------------------------------------
  * No counterpart in the reference (it has no adjoint).  Gradients of an
  * objective of the final state with respect to the initial state, for FP64
