@@ -51,6 +51,14 @@ def parse():
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint"], default=None,
+                    help="run one section alone (profiling); prints that section's object")
+    ap.add_argument("--accuracy-steps", type=int, default=200,
+                    help="steps of the mixed-vs-FP64 relative L2 comparison")
+    ap.add_argument("--adjoint-n", type=int, default=16,
+                    help="hexahedra per axis of the adjoint workload (K = 6 n^3)")
+    ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--adjoint-every", type=int, default=50, help="checkpoint spacing")
     return ap.parse_args()
 
 
@@ -228,6 +236,120 @@ def run_reference_arm(a):
     return 0
 
 
+def _events(stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return e0, e1
+
+
+def mixed_section(a, p, stream, fp64_ms_per_step):
+    """Mixed-precision stage kernels on the same workload: throughput, speed-up
+    over the FP64 path and relative L2 against FP64 after --accuracy-steps."""
+    import numpy as np
+    from exadglm_b200.capi import Solver, variants
+    S = a.accuracy_steps
+    ref = Solver(p, precision="fp64")
+    ref.set_stream(stream.cuda_stream)
+    ref.step(S)
+    ref.sync()
+    u64 = ref.get_state()
+    ref.close()
+    per_step = dof_stages_per_step(p)
+    out = {"accuracy_steps": S}
+    for prec in ("tf32x3", "bf16x3"):
+        try:
+            s = Solver(p, precision=prec)
+        except Exception as exc:        # precision not built for this order
+            out[prec] = {"unavailable": str(exc)}
+            continue
+        s.set_stream(stream.cuda_stream)
+        s.step(a.warmup)
+        s.sync()
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        s.step(a.steps)
+        e1.record(stream)
+        e1.synchronize()
+        s.sync()
+        ms = e0.elapsed_time(e1) / a.steps
+        s.set_state(p.u0)
+        s.step(S)
+        s.sync()
+        um = s.get_state()
+        per_field = [float(np.linalg.norm(um[v] - u64[v]) / np.linalg.norm(u64[v]))
+                     for v in range(p.nvar)]
+        out[prec] = {
+            "value": per_step / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "speedup_vs_fp64": fp64_ms_per_step / ms,
+            "rel_l2_vs_fp64": float(np.linalg.norm(um - u64) / np.linalg.norm(u64)),
+            "rel_l2_per_field": per_field,
+            "kernel": variants("euler", p.N)[s.variant()],
+        }
+        s.close()
+    return out
+
+
+def adjoint_section(a, stream):
+    """Discrete adjoint on the gradient-check workload: Euler N=4, K = 6 n^3,
+    J = 1/2 ||rho(T) - rho_target||^2 after --adjoint-steps steps, checkpoint
+    every --adjoint-every steps, dt and tau frozen.  The ratio is backward
+    (recomputation included) over a plain forward run, both per step, timed
+    with CUDA events on the solver's stream."""
+    import numpy as np
+    import torch
+    from exadglm_b200 import problem as P
+    from exadglm_b200.capi import Solver
+    pa = P.euler_sine(n=a.adjoint_n, N=4, noise=1e-3, seed=5)
+    pt = P.euler_sine(n=a.adjoint_n, N=4, v=(1.05, 0.45, 0.3), noise=1e-3, seed=5,
+                      mesh=pa.mesh)
+    T = a.adjoint_steps
+    s = Solver(pa)
+    s.set_stream(stream.cuda_stream)
+    s.set_state(pt.u0)
+    s.step(T)
+    s.sync()
+    rho_target = s.get_state()[0]
+    nv, n = pa.nvar, pa.K * pa.Np
+    s.set_state(pa.u0)
+    s.step(max(a.warmup, 3))
+    s.sync()
+
+    def timed(fn):
+        e0, e1 = _events(stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    s.set_state(pa.u0)
+    fwd = timed(lambda: s.step(T))
+    s.set_state(pa.u0)
+    rec = timed(lambda: s.adjoint_record(T, a.adjoint_every))
+    uT = s.get_state()
+    lam = torch.zeros((nv, n), dtype=torch.float64, device="cuda")
+    lam[0] = torch.from_numpy(uT[0] - rho_target).cuda()
+    grad = torch.empty_like(lam)
+    lp = [lam[v].data_ptr() for v in range(nv)]
+    gp = [grad[v].data_ptr() for v in range(nv)]
+    torch.cuda.synchronize()                      # lam is written on torch's stream
+    s.adjoint_backward_device(lp, gp)             # warm (first sweep sizes nothing new)
+    bwd = timed(lambda: s.adjoint_backward_device(lp, gp))
+    out = {
+        "workload": f"euler_sine N=4 K={pa.K} (n={a.adjoint_n}) + 1e-3 noise, "
+                    f"J = 1/2||rho(T)-rho_target||^2, T = {T} steps, checkpoint every "
+                    f"{a.adjoint_every}, dt and tau frozen",
+        "fwd_ms_per_step": fwd / T, "record_ms_per_step": rec / T, "bwd_ms_per_step": bwd / T,
+        "ratio_bwd_over_fwd": bwd / fwd, "ratio_bwd_over_record": bwd / rec,
+        "J": float(0.5 * np.dot(uT[0] - rho_target, uT[0] - rho_target)),
+        "grad_norm": float(torch.linalg.norm(grad).item()),
+        "tape_bytes": s.adjoint_tape_bytes(),
+    }
+    s.close()
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -260,8 +382,17 @@ def main():
         return float(t.item())
 
     p = build_problem(a)
-    s = Solver(p, precision=a.precision, device=local)
     stream = torch.cuda.Stream()
+    if a.only in ("mixed", "adjoint"):
+        res = (mixed_section(a, p, stream, float("nan")) if a.only == "mixed"
+               else adjoint_section(a, stream))
+        if rank == 0:
+            print(json.dumps({a.only: res}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+    s = Solver(p, precision=a.precision, device=local)
     s.set_stream(stream.cuda_stream)
     per_step = dof_stages_per_step(p)
 
@@ -352,6 +483,9 @@ def main():
                    "l2": "inputs larger than L2 (state 3 x 275 MB)"},
         "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
     }
+    if a.only is None and a.precision == "fp64":
+        line["mixed"] = mixed_section(a, p, stream, ms_max / a.steps)
+        line["adjoint"] = adjoint_section(a, stream)
     if rank == 0 and not a.no_cpu_baseline:
         sample_steps = 1
         rate, kind, cores, secs = cpu_reference_rate(p, sample_steps)

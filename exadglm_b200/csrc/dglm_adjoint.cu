@@ -540,11 +540,12 @@ dglm_status tape_setup(dglm_handle *h) {
     e = cudaMemcpy(t->AV, av.data(), sizeof(double) * av.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(t->AL, al.data(), sizeof(double) * al.size(), cudaMemcpyHostToDevice);
+  // every later use of these buffers is on the handle's stream: zero them there
   for (double *p : {t->lam, t->lk, t->kbuf})
-    if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(double) * t->state);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, sizeof(double) * t->state, s);
   for (double *p : t->phi)
-    if (e == cudaSuccess) e = cudaMemset(p, 0, sizeof(double) * h->nvar * t->vsF);
-  if (e == cudaSuccess) e = cudaMemset(t->bad, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, sizeof(double) * h->nvar * t->vsF, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->bad, 0, sizeof(int), s);
   const long nfp = K * NFF;
   if (e == cudaSuccess) {
     adjoint_mapP_kernel<<<(unsigned)((nfp + 255) / 256), 256, 0, s>>>(
@@ -600,10 +601,13 @@ dglm_status tape_size(dglm_handle *h, int nsteps, int every) {
     t->sized_bytes = 0;
     return st;
   }
-  // zero-filled so the padded tail elements of every stored state stay zero
-  cudaMemset(t->tau, 0, sizeof(double) * (euler ? nsteps : 1) * 4 * h->Kp);
-  cudaMemset(t->ckpt, 0, sizeof(double) * nseg * t->state);
-  cudaMemset(t->store, 0, sizeof(double) * 5 * seg_len * t->state);
+  // zero-filled (on the handle's stream, ordered before the recording that
+  // writes them) so the padded tail elements of every stored state stay zero
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaMemsetAsync(t->tau, 0, sizeof(double) * (euler ? nsteps : 1) * 4 * h->Kp, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->ckpt, 0, sizeof(double) * nseg * t->state, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->store, 0, sizeof(double) * 5 * seg_len * t->state, s);
+  if (e != cudaSuccess) return cuda_check(e, "adjoint tape");
   t->cap_ckpt = nseg;
   t->cap_steps = nsteps;
   t->cap_store = 5 * seg_len;

@@ -227,9 +227,11 @@ dglm_status dglm::ensure_rhs_scratch(dglm_handle *h) {
   if (st == DGLM_OK) st = dalloc(h, &h->tau_s, (size_t)4 * h->Kp);
   if (st == DGLM_OK) st = dalloc(h, &h->sc_s, 1);
   if (st != DGLM_OK) return st;
-  cudaError_t e = cudaMemset(h->rhs_in, 0, sizeof(double) * h->nvar * h->vs);
-  if (e == cudaSuccess) e = cudaMemset(h->maxv_s, 0, sizeof(double) * 4 * h->Kp);
-  if (e == cudaSuccess) e = cudaMemset(h->tau_s, 0, sizeof(double) * 4 * h->Kp);
+  // on the handle's stream, ordered before the copies that fill them
+  cudaStream_t s = h->stream;
+  cudaError_t e = cudaMemsetAsync(h->rhs_in, 0, sizeof(double) * h->nvar * h->vs, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->maxv_s, 0, sizeof(double) * 4 * h->Kp, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->tau_s, 0, sizeof(double) * 4 * h->Kp, s);
   return cuda_check(e, "rhs scratch");
 }
 
