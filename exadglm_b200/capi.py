@@ -27,7 +27,8 @@ EXPORTS = (
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
     "dglm_set_variant", "dglm_get_variant", "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
-    "dglm_calc_maxv_dt_static",
+    "dglm_calc_maxv_dt_static", "dglm_adjoint_variant_count", "dglm_adjoint_variant_describe",
+    "dglm_adjoint_set_variant",
 )
 
 
@@ -103,6 +104,8 @@ def lib():
         L.dglm_adjoint_replay.argtypes = [_P]
         L.dglm_adjoint_rhs.argtypes = [_P, _P, _P, _P]
         L.dglm_adjoint_tape_bytes.argtypes = [_P, C.POINTER(C.c_size_t)]
+        L.dglm_adjoint_variant_describe.argtypes = [I, I, I, C.c_char_p, C.c_size_t]
+        L.dglm_adjoint_set_variant.argtypes = [_P, I]
         _lib = L
     return _lib
 
@@ -142,6 +145,18 @@ def variants(physics, N, precision=None):
     if precision is None:
         return out
     return [(i, d) for i, d in enumerate(out) if variant_precision(d) == precision]
+
+
+def adjoint_variants(physics, N):
+    """Descriptions of the adjoint stage-kernel tile shapes for (physics, N)."""
+    L = lib()
+    ph = EULER if physics == "euler" else ADVECTION
+    out = []
+    for i in range(L.dglm_adjoint_variant_count(ph, N)):
+        buf = C.create_string_buffer(128)
+        check(L.dglm_adjoint_variant_describe(ph, N, i, buf, 128))
+        out.append(buf.value.decode())
+    return out
 
 
 def _np_ptr(a):
@@ -279,6 +294,9 @@ class Solver:
     def adjoint_rhs_device(self, u_ptrs, mu_ptrs, out_ptrs):
         check(self.L.dglm_adjoint_rhs(self.h, ptr_table(u_ptrs), ptr_table(mu_ptrs),
                                       ptr_table(out_ptrs)))
+
+    def adjoint_set_variant(self, v):
+        check(self.L.dglm_adjoint_set_variant(self.h, int(v)))
 
     def adjoint_tape_bytes(self):
         n = C.c_size_t()

@@ -38,6 +38,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -72,7 +73,7 @@ struct AdjArgs {
 
 enum { A_ADV = 0, A_EUL = 1 };
 
-template <int PHYS, int N, int E_>
+template <int PHYS, int N, int E_, int MINB_ = 1>
 struct ACfg {
   static constexpr int NV = PHYS == A_EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -124,8 +125,8 @@ __device__ __forceinline__ void jac_t_add(const JacPre &P, double gm, double nx,
   w[4] += s * ((gm - 1) * gn + gm * un * g[4]);
 }
 
-template <int PHYS, int N, int E_>
-__global__ void __launch_bounds__(ACfg<PHYS, N, E_>::T)
+template <int PHYS, int N, int E_, int MINB>
+__global__ void __launch_bounds__(ACfg<PHYS, N, E_>::T, MINB)
     adjoint_stage_kernel(const AdjArgs a) {
   using C = ACfg<PHYS, N, E_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
@@ -364,6 +365,301 @@ __global__ void __launch_bounds__(ACfg<PHYS, N, E_>::T)
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 tensor-core variant: the two contractions on mma.sync.m8n8k4.f64.
+//
+// Rows of the volume operator are (d*Np + j) of [WD_r^T; WD_s^T; WD_t^T]
+// (MTV m-tiles), rows of the lift operator are the face points of -LIFT^T
+// (MTL m-tiles); k runs over the Np nodes (padded to KP).  Both are stored
+// on the device as A fragments [kstep][mtile][lane] (row 8*mtile + lane/4,
+// k 4*kstep + lane%4), one coalesced 256-byte load each.  The B operand is
+// mu in shared memory, [k][v*E + e].  Warp w owns n-tile w % NT (8 columns)
+// and the m-tiles of group w / NT.  Results go through shared memory to the
+// element-local phases (Jacobians, faces, update), which use all threads.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void adj_dmma(double (&d)[2], double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
+template <int PHYS, int N, int E_, int MG_>
+struct DCfg {
+  static constexpr int NV = PHYS == A_EUL ? 5 : 1;
+  static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
+  static constexpr int E = E_, EP = E_ + 1, NCOL = NV * E, NT = NCOL / 8;
+  static constexpr int KP = (Np + 3) / 4 * 4, KS = KP / 4;
+  static constexpr int MTV = (3 * Np + 7) / 8, MTL = (NFF + 7) / 8;
+  static constexpr int MG = MG_;
+  static constexpr int WMV = (MTV + MG - 1) / MG, WML = (MTL + MG - 1) / MG;
+  static constexpr int WARPS = NT * MG, T = 32 * WARPS;
+  static constexpr int BLD = NCOL + 4;
+  static constexpr int VMLD = NFF + 1;
+  static constexpr int ROWS = 8 * (MTV > MTL ? MTV : MTL);
+  static constexpr int S_U = NV * Np * EP, S_B = KP * BLD, S_OUT = ROWS * NV * EP,
+                       S_FC = NV * NFF * EP;
+  static constexpr size_t SMEM =
+      sizeof(double) * (2 * S_U + S_B + S_OUT + S_FC + 9 * E + 40 * E) +
+      sizeof(int) * (2 * E * VMLD + NFF + 4 * Np);
+  static constexpr int AFV = KS * MTV * 32, AFL = KS * MTL * 32;   // fragment doubles
+  static_assert(NCOL % 8 == 0, "columns must fill whole n-tiles");
+  static_assert(T <= 1024, "block too large");
+};
+
+template <int PHYS, int N, int E_, int MG_, int MINB>
+__global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
+    adjoint_dmma_kernel(const AdjArgs a) {
+  using C = DCfg<PHYS, N, E_, MG_>;
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+                BLD = C::BLD, T = C::T, VMLD = C::VMLD, KP = C::KP;
+  extern __shared__ __align__(16) double smem[];
+  double *sU = smem;                   // [v][i][EP] stage state, later lk'
+  double *sLam = sU + C::S_U;          // [v][i][EP]
+  double *sB = sLam + C::S_U;          // [k][BLD] mu, col = v*E + e
+  double *sOut = sB + C::S_B;          // [row][v][EP] contraction results
+  double *sFc = sOut + C::S_OUT;       // [v][fj][EP] face terms
+  double *sGeo = sFc + C::S_FC;        // [9][E]
+  double *sFace = sGeo + 9 * E;        // [10][4][E]
+  int *sVm = reinterpret_cast<int *>(sFace + 40 * E);
+  int *sMp = sVm + E * VMLD;
+  int *sFm = sMp + E * VMLD;
+  int *sNF = sFm + NFF;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long e0 = (long)blockIdx.x * E;
+  const int ne = (int)min((long)E, (long)a.K - e0);
+  const long vs = a.vs, vsF = a.vsF;
+  const bool upd = a.update != 0;
+  const int ng = warp % C::NT, mg = warp / C::NT;
+
+  // ---- staging ------------------------------------------------------------
+  for (int i = tid; i < NFF; i += T) sFm[i] = __ldg(a.Fmask + i);
+  for (int i = tid; i < Np; i += T) {
+    int c = 0;
+    for (int fj = 0; fj < NFF; fj++)
+      if (__ldg(a.Fmask + fj) == i && c < 4) sNF[i * 4 + c++] = fj;
+    for (; c < 4; c++) sNF[i * 4 + c] = -1;
+  }
+  const double bm = upd ? a.rkb : a.rkb_next;
+  for (int v = 0; v < NV; v++) {
+    const long base = v * vs + e0 * Np;
+    for (int g = tid; g < E * Np; g += T) {
+      const int e = g / Np, i = g - e * Np;
+      const bool ok = g < ne * Np;
+      const double lam = ok ? a.lam[base + g] : 0.0;
+      const double lk = ok ? a.lk[base + g] : 0.0;
+      sLam[(v * Np + i) * EP + e] = lam;
+      sB[i * BLD + v * E + e] = lk + bm * lam;
+      if (upd) sU[(v * Np + i) * EP + e] = ok ? __ldg(a.u + base + g) : (v == 0 ? 1.0 : 0.0);
+    }
+  }
+  for (int g = tid; g < (KP - Np) * BLD; g += T) sB[Np * BLD + g] = 0.0;
+  if (upd) {
+    for (int g = tid; g < 9 * E; g += T) {
+      const int m = g / E, e = g - m * E;
+      sGeo[g] = e < ne ? __ldg(a.geo + (long)m * a.gstride + e0 + e) : 0.0;
+    }
+    for (int g = tid; g < 4 * E; g += T) {
+      const int e = g >> 2, f = g & 3;
+      const bool ok = e < ne;
+      const long gf = (e0 + e) * 4 + f;
+      const long gf2 = ok ? __ldg(a.vmapF + gf) : 0;
+      const long gs = a.gstride;
+      sFace[(0 * 4 + f) * E + e] = ok ? __ldg(a.nrm + gf) : 0.0;
+      sFace[(1 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 4 * gs + gf) : 0.0;
+      sFace[(2 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 8 * gs + gf) : 0.0;
+      sFace[(3 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf) : 0.0;
+      sFace[(4 * 4 + f) * E + e] = ok ? __ldg(a.tau + gf) : 0.0;
+      sFace[(5 * 4 + f) * E + e] = ok ? __ldg(a.nrm + gf2) : 0.0;
+      sFace[(6 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 4 * gs + gf2) : 0.0;
+      sFace[(7 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 8 * gs + gf2) : 0.0;
+      sFace[(8 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf2) : 0.0;
+      sFace[(9 * 4 + f) * E + e] = ok ? __ldg(a.tau + gf2) : 0.0;
+    }
+    for (int g = tid; g < E * NFF; g += T) {
+      const int e = g / NFF, fj = g - e * NFF;
+      const bool ok = g < ne * NFF;
+      sVm[e * VMLD + fj] = ok ? __ldg(a.vmapP + e0 * NFF + g) : 0;
+      sMp[e * VMLD + fj] = ok ? __ldg(a.mapP + e0 * NFF + g) : 0;
+    }
+  }
+  __syncthreads();
+
+  if (upd) {
+    // ---- face terms -> sFc (as the SIMT variant) ----------------------------
+    for (int it = tid; it < E * NFF; it += T) {
+      const int e = it / NFF, fj = it - e * NFF, f = fj / Nfp;
+      if (e >= ne) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) sFc[(v * NFF + fj) * EP + e] = 0.0;
+        continue;
+      }
+      const long p = (e0 + e) * NFF + fj;
+      const long iP = sVm[e * VMLD + fj], p2 = sMp[e * VMLD + fj];
+      const int nodeM = sFm[fj];
+      const double *F4 = sFace + f * E + e;
+      const double nx = F4[0], ny = F4[4 * E], nz = F4[8 * E], fs = F4[12 * E],
+                   ta = F4[16 * E], nx2 = F4[20 * E], ny2 = F4[24 * E], nz2 = F4[28 * E],
+                   fs2 = F4[32 * E], ta2 = F4[36 * E];
+      if (PHYS == A_EUL) {
+        double qb[5], g1[5], g2[5], w[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          qb[v] = 0.5 * (sU[(v * Np + nodeM) * EP + e] + __ldg(a.u + v * vs + iP));
+          g1[v] = a.phi_in[v * vsF + p];
+          g2[v] = a.phi_in[v * vsF + p2];
+          w[v] = 0.5 * (fs * ta * g1[v] - fs2 * ta2 * g2[v]);
+        }
+        const JacPre P = jac_pre(a.gamma, qb);
+        jac_t_add(P, a.gamma, nx, ny, nz, g1, 0.5 * fs, w);
+        jac_t_add(P, a.gamma, nx2, ny2, nz2, g2, 0.5 * fs2, w);
+#pragma unroll
+        for (int v = 0; v < 5; v++) sFc[(v * NFF + fj) * EP + e] = w[v];
+      } else {
+        const long nM = (e0 + e) * Np + nodeM;
+        const double an = nx * __ldg(a.vel + nM) + ny * __ldg(a.vel + vs + nM) +
+                          nz * __ldg(a.vel + 2 * vs + nM);
+        const double an2 = nx2 * __ldg(a.vel + iP) + ny2 * __ldg(a.vel + vs + iP) +
+                           nz2 * __ldg(a.vel + 2 * vs + iP);
+        const double g1 = a.phi_in[p], g2 = a.phi_in[p2];
+        sFc[fj * EP + e] = fs * (0.5 * an + 0.5 * ta) * g1 + fs2 * (0.5 * an2 - 0.5 * ta2) * g2;
+      }
+    }
+
+    // ---- nu = [WD^T] mu on the tensor cores --------------------------------
+    double acc[C::WMV][2];
+#pragma unroll
+    for (int i = 0; i < C::WMV; i++) acc[i][0] = acc[i][1] = 0.0;
+    const int m0 = mg * C::WMV;
+    const double *Ab = a.AV + (long)m0 * 32 + lane;
+    const double *Bb = sB + (lane & 3) * BLD + ng * 8 + (lane >> 2);
+#pragma unroll 3
+    for (int ks = 0; ks < C::KS; ks++) {
+      const double bv = Bb[ks * 4 * BLD];
+#pragma unroll
+      for (int i = 0; i < C::WMV; i++)
+        if (m0 + i < C::MTV) adj_dmma(acc[i], __ldg(Ab + ((long)ks * C::MTV + i) * 32), bv);
+    }
+    // results -> sOut[row][v][e] (row = d*Np + j)
+#pragma unroll
+    for (int i = 0; i < C::WMV; i++) {
+      const int row = (m0 + i) * 8 + (lane >> 2);
+      if (m0 + i < C::MTV && row < 3 * Np) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int col = ng * 8 + (lane & 3) * 2 + h, v = col / E, e = col - v * E;
+          sOut[(row * NV + v) * EP + e] = acc[i][h];
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  if (upd) {
+    // ---- combine: lam' = lam + dt (volume + face terms), lk' = a mu ---------
+    for (int it = tid; it < E * Np; it += T) {
+      const int j = it / E, e = it - j * E;
+      const double *gg = sGeo + e;
+      double w[NV];
+#pragma unroll
+      for (int v = 0; v < NV; v++) w[v] = 0.0;
+      double nu[3][NV];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) nu[d][v] = sOut[((d * Np + j) * NV + v) * EP + e];
+      JacPre P;
+      if (PHYS == A_EUL) {
+        double q[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q[v] = sU[(v * Np + j) * EP + e];
+        P = jac_pre(a.gamma, q);
+      }
+#pragma unroll
+      for (int x = 0; x < 3; x++) {
+        double Gx[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+          Gx[v] = gg[x * E] * nu[0][v] + gg[(3 + x) * E] * nu[1][v] + gg[(6 + x) * E] * nu[2][v];
+        if (PHYS == A_EUL) {
+          jac_t_add(P, a.gamma, x == 0, x == 1, x == 2, Gx, 1.0, w);
+        } else {
+          const long n = (e < ne) ? (e0 + e) * Np + j : 0;
+          w[0] += __ldg(a.vel + x * vs + n) * Gx[0];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const int fj = sNF[j * 4 + c];
+        if (fj < 0) break;
+#pragma unroll
+        for (int v = 0; v < NV; v++) w[v] += sFc[(v * NFF + fj) * EP + e];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        const int s = (v * Np + j) * EP + e;
+        const double mu = sB[j * BLD + v * E + e];
+        const double lamn = sLam[s] + a.dt * w[v];
+        const double lkn = a.rka * mu;
+        sLam[s] = lamn;
+        sU[s] = lkn;
+        sB[j * BLD + v * E + e] = lkn + a.rkb_next * lamn;
+      }
+    }
+    __syncthreads();
+  }
+
+  if (a.phi_next) {
+    // ---- phi' = -LIFT^T mu' on the tensor cores -> sOut[fj][v][e] -----------
+    double acc[C::WML][2];
+#pragma unroll
+    for (int i = 0; i < C::WML; i++) acc[i][0] = acc[i][1] = 0.0;
+    const int m0 = mg * C::WML;
+    const double *Ab = a.AL + (long)m0 * 32 + lane;
+    const double *Bb = sB + (lane & 3) * BLD + ng * 8 + (lane >> 2);
+#pragma unroll 3
+    for (int ks = 0; ks < C::KS; ks++) {
+      const double bv = Bb[ks * 4 * BLD];
+#pragma unroll
+      for (int i = 0; i < C::WML; i++)
+        if (m0 + i < C::MTL) adj_dmma(acc[i], __ldg(Ab + ((long)ks * C::MTL + i) * 32), bv);
+    }
+#pragma unroll
+    for (int i = 0; i < C::WML; i++) {
+      const int row = (m0 + i) * 8 + (lane >> 2);
+      if (m0 + i < C::MTL && row < NFF) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int col = ng * 8 + (lane & 3) * 2 + h, v = col / E, e = col - v * E;
+          sOut[(row * NV + v) * EP + e] = acc[i][h];
+        }
+      }
+    }
+    __syncthreads();
+    for (int v = 0; v < NV; v++) {
+      const long base = v * vsF + e0 * NFF;
+      for (int g = tid; g < ne * NFF; g += T) {
+        const int e = g / NFF, fj = g - e * NFF;
+        a.phi_out[base + g] = sOut[(fj * NV + v) * EP + e];
+      }
+    }
+  }
+
+  if (upd) {
+    for (int v = 0; v < NV; v++) {
+      const long base = v * vs + e0 * Np;
+      for (int g = tid; g < ne * Np; g += T) {
+        const int e = g / Np, i = g - e * Np;
+        const int s = (v * Np + i) * EP + e;
+        a.lam[base + g] = sLam[s];
+        a.lk[base + g] = sU[s];
+      }
+    }
+  }
+}
+
 // Partner face point of every face point (see the file comment); flags a
 // face point without exactly one partner or a pairing that is not an
 // involution.
@@ -399,15 +695,18 @@ __global__ void adjoint_mapP_check_kernel(long n, const int *__restrict__ mapP, 
 // ---------------------------------------------------------------------------
 
 struct AdjVariant {
-  int E, T, IPV, IPL;
+  int kind;                  // 0: SIMT (k-major operators), 1: DMMA (A fragments)
+  int E, T, minb;
   size_t smem;
+  int IPV, IPL;              // SIMT: padded rows of the k-major operators
+  int MTV, MTL, KS;          // DMMA: m-tiles and k-steps of the fragments
   cudaError_t (*launch)(const AdjArgs &, cudaStream_t);
 };
 
-template <int PHYS, int N, int E>
+template <int PHYS, int N, int E, int MINB>
 cudaError_t launch_adj(const AdjArgs &a, cudaStream_t s) {
   using C = ACfg<PHYS, N, E>;
-  auto k = adjoint_stage_kernel<PHYS, N, E>;
+  auto k = adjoint_stage_kernel<PHYS, N, E, MINB>;
   cudaError_t e =
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -416,22 +715,53 @@ cudaError_t launch_adj(const AdjArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E>
-constexpr AdjVariant adj_variant() {
+template <int PHYS, int N, int E, int MINB = 1>
+AdjVariant adj_variant() {
   using C = ACfg<PHYS, N, E>;
-  return AdjVariant{E, C::T, C::IPV, C::IPL, C::SMEM, launch_adj<PHYS, N, E>};
+  return AdjVariant{0, E, C::T, MINB, C::SMEM, C::IPV, C::IPL, 0, 0, 0,
+                    launch_adj<PHYS, N, E, MINB>};
 }
 
-bool adjoint_variant(int physics, int N, AdjVariant *out) {
-  static const AdjVariant eul[] = {adj_variant<A_EUL, 1, 16>(), adj_variant<A_EUL, 2, 16>(),
-                                   adj_variant<A_EUL, 3, 8>(),  adj_variant<A_EUL, 4, 8>(),
-                                   adj_variant<A_EUL, 5, 8>(),  adj_variant<A_EUL, 6, 4>()};
-  static const AdjVariant adv[] = {adj_variant<A_ADV, 1, 64>(), adj_variant<A_ADV, 2, 32>(),
-                                   adj_variant<A_ADV, 3, 32>(), adj_variant<A_ADV, 4, 32>(),
-                                   adj_variant<A_ADV, 5, 16>(), adj_variant<A_ADV, 6, 16>()};
-  if (N < 1 || N > 6) return false;
-  *out = physics == DGLM_EULER ? eul[N - 1] : adv[N - 1];
-  return true;
+template <int PHYS, int N, int E, int MG, int MINB>
+cudaError_t launch_adj_dmma(const AdjArgs &a, cudaStream_t s) {
+  using C = DCfg<PHYS, N, E, MG>;
+  auto k = adjoint_dmma_kernel<PHYS, N, E, MG, MINB>;
+  cudaError_t e =
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int blocks = (a.K + E - 1) / E;
+  k<<<blocks, C::T, C::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E, int MG, int MINB = 1>
+AdjVariant adj_dmma_variant() {
+  using C = DCfg<PHYS, N, E, MG>;
+  return AdjVariant{1, E, C::T, MINB, C::SMEM, 0, 0, C::MTV, C::MTL, C::KS,
+                    launch_adj_dmma<PHYS, N, E, MG, MINB>};
+}
+
+// Tile shapes per (physics, N); the first is the default.
+const std::vector<AdjVariant> &adjoint_variants(int physics, int N) {
+  static const std::vector<AdjVariant> none;
+  static const std::vector<AdjVariant> eul[6] = {
+      {adj_variant<A_EUL, 1, 16>()},
+      {adj_variant<A_EUL, 2, 16>(), adj_dmma_variant<A_EUL, 2, 8, 1>()},
+      {adj_variant<A_EUL, 3, 8>(), adj_dmma_variant<A_EUL, 3, 8, 2>()},
+      {adj_dmma_variant<A_EUL, 4, 8, 2, 2>(), adj_variant<A_EUL, 4, 4, 4>(),
+       adj_dmma_variant<A_EUL, 4, 8, 2>(), adj_dmma_variant<A_EUL, 4, 8, 3>(),
+       adj_variant<A_EUL, 4, 8, 3>()},
+      {adj_variant<A_EUL, 5, 8>(), adj_dmma_variant<A_EUL, 5, 8, 2>()},
+      {adj_variant<A_EUL, 6, 4>()}};
+  static const std::vector<AdjVariant> adv[6] = {
+      {adj_variant<A_ADV, 1, 64>()},
+      {adj_variant<A_ADV, 2, 32>(), adj_dmma_variant<A_ADV, 2, 32, 1>()},
+      {adj_variant<A_ADV, 3, 32>(), adj_dmma_variant<A_ADV, 3, 32, 2>()},
+      {adj_variant<A_ADV, 4, 32>(), adj_dmma_variant<A_ADV, 4, 32, 2>()},
+      {adj_variant<A_ADV, 5, 16>(), adj_dmma_variant<A_ADV, 5, 16, 2>()},
+      {adj_variant<A_ADV, 6, 16>()}};
+  if (N < 1 || N > 6 || (physics != DGLM_EULER && physics != DGLM_ADVECTION)) return none;
+  return physics == DGLM_EULER ? eul[N - 1] : adv[N - 1];
 }
 
 }  // namespace dglm
@@ -444,6 +774,7 @@ using namespace dglm;
 
 struct AdjointTape {
   AdjVariant var{};
+  int var_index = 0;
   long state = 0;            // doubles per stored state (nvar * vs)
   long vsF = 0;              // doubles between variables of a face-point field
   int nsteps = 0, every = 0, nseg = 0, cap_ckpt = 0, cap_steps = 0, cap_store = 0;
@@ -503,8 +834,13 @@ dglm_status tape_setup(dglm_handle *h) {
   free_tape(h);
   AdjointTape *t = new AdjointTape();
   h->tape = t;
-  if (!adjoint_variant(h->d.physics, h->d.N, &t->var))
+  const std::vector<AdjVariant> &vl = adjoint_variants(h->d.physics, h->d.N);
+  if (vl.empty()) {
+    free_tape(h);
     return set_error(DGLM_ERR_UNSUPPORTED, "adjoint: order not built (1..6)");
+  }
+  t->var_index = h->adj_variant < (int)vl.size() ? h->adj_variant : 0;
+  t->var = vl[t->var_index];
   const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF;
   const long K = h->d.K;
   t->state = (long)h->nvar * h->vs;
@@ -513,8 +849,11 @@ dglm_status tape_setup(dglm_handle *h) {
   auto chk = [&](dglm_status s) {
     if (st == DGLM_OK) st = s;
   };
-  chk(talloc(t, t->fixed, &t->AV, (size_t)Np * t->var.IPV));
-  chk(talloc(t, t->fixed, &t->AL, (size_t)Np * t->var.IPL));
+  const AdjVariant &v = t->var;
+  const size_t nav = v.kind == 0 ? (size_t)Np * v.IPV : (size_t)v.KS * v.MTV * 32;
+  const size_t nal = v.kind == 0 ? (size_t)Np * v.IPL : (size_t)v.KS * v.MTL * 32;
+  chk(talloc(t, t->fixed, &t->AV, nav));
+  chk(talloc(t, t->fixed, &t->AL, nal));
   chk(talloc(t, t->fixed, &t->mapP, (size_t)K * NFF));
   chk(talloc(t, t->fixed, &t->bad, 1));
   chk(talloc(t, t->fixed, &t->lam, (size_t)t->state));
@@ -526,13 +865,30 @@ dglm_status tape_setup(dglm_handle *h) {
     free_tape(h);
     return st;
   }
-  std::vector<double> av((size_t)Np * t->var.IPV, 0.0), al((size_t)Np * t->var.IPL, 0.0);
-  for (int i = 0; i < Np; i++) {
-    for (int j = 0; j < Np; j++)
-      for (int d = 0; d < 3; d++)
-        av[(size_t)i * t->var.IPV + 3 * j + d] = h->Ahost[(size_t)i * KA + d * Np + j];
-    for (int fj = 0; fj < NFF; fj++)
-      al[(size_t)i * t->var.IPL + fj] = h->Ahost[(size_t)i * KA + 3 * Np + fj];
+  std::vector<double> av(nav, 0.0), al(nal, 0.0);
+  auto WD = [&](int d, int i, int j) { return h->Ahost[(size_t)i * KA + d * Np + j]; };
+  auto NL = [&](int i, int fj) { return h->Ahost[(size_t)i * KA + 3 * Np + fj]; };   // -LIFT
+  if (v.kind == 0) {
+    for (int i = 0; i < Np; i++) {
+      for (int j = 0; j < Np; j++)
+        for (int d = 0; d < 3; d++) av[(size_t)i * v.IPV + 3 * j + d] = WD(d, i, j);
+      for (int fj = 0; fj < NFF; fj++) al[(size_t)i * v.IPL + fj] = NL(i, fj);
+    }
+  } else {
+    // A fragments [kstep][mtile][lane]: row 8*mtile + lane/4, k 4*kstep + lane%4
+    for (int ks = 0; ks < v.KS; ks++)
+      for (int lane = 0; lane < 32; lane++) {
+        const int k = 4 * ks + lane % 4;
+        if (k >= Np) continue;
+        for (int mt = 0; mt < v.MTV; mt++) {
+          const int row = 8 * mt + lane / 4;
+          if (row < 3 * Np) av[((size_t)ks * v.MTV + mt) * 32 + lane] = WD(row / Np, k, row % Np);
+        }
+        for (int mt = 0; mt < v.MTL; mt++) {
+          const int row = 8 * mt + lane / 4;
+          if (row < NFF) al[((size_t)ks * v.MTL + mt) * 32 + lane] = NL(k, row);
+        }
+      }
   }
   cudaStream_t s = h->stream;
   cudaError_t e = cudaStreamSynchronize(s);
@@ -856,6 +1212,33 @@ dglm_status dglm_adjoint_rhs(dglm_handle *h, const double *const *u, const doubl
   if (e == cudaSuccess) e = t->var.launch(a, s);
   if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_rhs");
   return fetch_fields(h, out, t->lam, 1, "dglm_adjoint_rhs");
+}
+
+int dglm_adjoint_variant_count(int physics, int N) {
+  return (int)adjoint_variants(physics, N).size();
+}
+
+dglm_status dglm_adjoint_variant_describe(int physics, int N, int variant, char *buf,
+                                          size_t len) {
+  const std::vector<AdjVariant> &vl = adjoint_variants(physics, N);
+  if (!buf || len == 0 || variant < 0 || variant >= (int)vl.size())
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_variant_describe: no such variant");
+  const AdjVariant &v = vl[variant];
+  snprintf(buf, len, "adjoint-%s E=%d threads=%d minblocks=%d smem=%zu",
+           v.kind == 0 ? "simt" : "dmma", v.E, v.T, v.minb, v.smem);
+  return DGLM_OK;
+}
+
+dglm_status dglm_adjoint_set_variant(dglm_handle *h, int variant) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_adjoint_set_variant: NULL handle");
+  if (variant < 0 || variant >= dglm_adjoint_variant_count(h->d.physics, h->d.N))
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_set_variant: no such variant");
+  if (variant == h->adj_variant) return DGLM_OK;
+  DeviceGuard g(h->dev);
+  cudaStreamSynchronize(h->stream);
+  free_tape(h);   // operator layout depends on the tile shape; record again
+  h->adj_variant = variant;
+  return DGLM_OK;
 }
 
 dglm_status dglm_adjoint_tape_bytes(dglm_handle *h, size_t *bytes) {

@@ -41,6 +41,7 @@ struct dglm_handle {
   size_t bytes = 0;
   std::vector<void *> allocs;
   AdjointTape *tape = nullptr;   // discrete adjoint (dglm_adjoint.cu)
+  int adj_variant = 0;           // adjoint tile shape
 };
 
 

@@ -239,6 +239,12 @@ dglm_status dglm_adjoint_replay(dglm_handle *h);
 dglm_status dglm_adjoint_rhs(dglm_handle *h, const double *const *u, const double *const *mu,
                              double *const *out);
 dglm_status dglm_adjoint_tape_bytes(dglm_handle *h, size_t *bytes);
+/* Tile shapes of the adjoint stage kernel for (physics, N); selecting one
+ * drops the tape (record again). */
+int dglm_adjoint_variant_count(int physics, int N);
+dglm_status dglm_adjoint_variant_describe(int physics, int N, int variant, char *buf,
+                                          size_t len);
+dglm_status dglm_adjoint_set_variant(dglm_handle *h, int variant);
 
 #ifdef __cplusplus
 }

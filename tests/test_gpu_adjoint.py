@@ -74,6 +74,27 @@ def test_reverse_sweep_matches_oracle(phys, N):
     s.close()
 
 
+@pytest.mark.parametrize("phys", ["euler", "advection"])
+@pytest.mark.parametrize("N", [2, 3, 4, 5])
+def test_every_adjoint_variant_matches_oracle(phys, N):
+    from exadglm_b200.capi import adjoint_variants
+    prob = make(phys, N)
+    O = oracle.Oracle(prob)
+    u0 = prob.u0.reshape(prob.nvar, -1)
+    _, dt, tau = O.run_record(3, u0)
+    lamT = np.random.default_rng(N).standard_normal(u0.shape)
+    ref = O.adjoint(u0, dt, tau, lamT)
+    s = Solver(prob, variant=-1)
+    for v, desc in enumerate(adjoint_variants(phys, N)):
+        s.adjoint_set_variant(v)
+        s.set_state(u0)
+        s.adjoint_record(3, 2)
+        err = rel(s.adjoint_backward(lamT), ref)
+        print(f"{phys} N={N} {desc}: rel L2 {err:.2e}")
+        assert err < SWEEP_TOL, (desc, err)
+    s.close()
+
+
 def test_checkpoint_spacing_and_replay_are_exact():
     prob = make("euler", 3)
     rng = np.random.default_rng(5)
