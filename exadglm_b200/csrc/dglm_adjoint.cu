@@ -779,6 +779,7 @@ struct AdjointTape {
   long vsF = 0;              // doubles between variables of a face-point field
   int nsteps = 0, every = 0, nseg = 0, cap_ckpt = 0, cap_steps = 0, cap_store = 0;
   bool recorded = false;
+  bool last_seg_stored = false;   // the store already holds the last segment's stage inputs
   std::vector<double> dt;    // dt of every recorded step
   double *AV = nullptr, *AL = nullptr;
   int *mapP = nullptr, *bad = nullptr;
@@ -1060,6 +1061,7 @@ dglm_status dglm_adjoint_record(dglm_handle *h, int nsteps, int checkpoint_every
   if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record");
   h->launches = 0;
   const bool euler = h->d.physics == DGLM_EULER;
+  const int last_s0 = (nsteps - 1) / checkpoint_every * checkpoint_every;
   for (int i = 0; i < nsteps; i++) {
     const size_t bytes = sizeof(double) * t->state;
     if (i % checkpoint_every == 0) {
@@ -1067,7 +1069,27 @@ dglm_status dglm_adjoint_record(dglm_handle *h, int nsteps, int checkpoint_every
                           bytes, cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record");
     }
-    st = run_steps(h, 1);
+    if (i < last_s0) {
+      st = run_steps(h, 1);
+    } else {
+      // last segment: the stages write their outputs straight into the
+      // segment store (slot j + 1 = output of stage j), so the reverse sweep
+      // starts without recomputing it; the final stage writes the state back
+      const double *ck = t->ckpt + (size_t)(i / checkpoint_every) * t->state;
+      auto slot = [&](int j) -> double * {
+        return j == 0 ? const_cast<double *>(ck) : t->store + (size_t)(j - 1) * t->state;
+      };
+      const double *in[5];
+      double *out[5];
+      for (int k = 0; k < 5; k++) {
+        const int j = 5 * (i - last_s0) + k;
+        in[k] = (i == last_s0 && k == 0) ? h->u[h->cur] : slot(j);
+        out[k] = (i == nsteps - 1 && k == 4) ? h->u[h->cur ^ 1] : slot(j + 1);
+      }
+      st = issue_step_ptrs(h, in, out, s);
+      h->launches += euler ? 8 : 7;
+      h->cur ^= 1;
+    }
     if (st != DGLM_OK) return st;
     if (euler || i == 0)
       e = cudaMemcpyAsync(const_cast<double *>(tau_of(h, i)), h->tau,
@@ -1089,6 +1111,7 @@ dglm_status dglm_adjoint_record(dglm_handle *h, int nsteps, int checkpoint_every
   t->every = checkpoint_every;
   t->nseg = (nsteps + checkpoint_every - 1) / checkpoint_every;
   t->recorded = true;
+  t->last_seg_stored = true;
   return DGLM_OK;
 }
 
@@ -1140,8 +1163,10 @@ dglm_status dglm_adjoint_backward(dglm_handle *h, const double *const *lam_T,
     auto slot = [&](int j) -> double * {
       return j == 0 ? ck : t->store + (size_t)(j - 1) * t->state;
     };
-    // recompute the segment's stage inputs from its checkpoint
-    for (int i = s0; i < s1 && e == cudaSuccess; i++)
+    // recompute the segment's stage inputs from its checkpoint (the last
+    // segment's are still in the store from the recording, on the first sweep)
+    const bool stored = seg == t->nseg - 1 && t->last_seg_stored;
+    for (int i = s0; i < s1 && e == cudaSuccess && !stored; i++)
       for (int k = 0; k < 5 && e == cudaSuccess; k++) {
         const int j = 5 * (i - s0) + k;
         if (i == s1 - 1 && k == 4) break;   // the last stage's output is not needed
@@ -1167,6 +1192,8 @@ dglm_status dglm_adjoint_backward(dglm_handle *h, const double *const *lam_T,
         p ^= 1;
       }
   }
+  // the store now holds the first segment: a second sweep recomputes all
+  if (t->nseg > 1) t->last_seg_stored = false;
   if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_backward");
   return fetch_fields(h, lam_0, t->lam, on_device, "dglm_adjoint_backward");
 }

@@ -119,6 +119,7 @@ struct StageVariantInfo {
   int npad;      // MIXED: MMA N (output nodes, padded)
   int kva, kfa;  // MIXED: volume / lift K extents of the operand images
   int bimg;      // MIXED: bytes of the operator image (hi then lo)
+  int groups;    // PIPE: consumer groups taking alternate tiles (1 or 2)
 };
 
 // fused FP64 stage launcher (dglm_stage_fp64.cu)

@@ -85,6 +85,8 @@ inline dglm_status dalloc(dglm_handle *h, T **p, size_t count) {
 StageArgs stage_args(dglm_handle *h, const double *u_in, double *u_out, int s);
 void free_tape(dglm_handle *h);
 dglm_status run_steps(dglm_handle *h, int nsteps);
+dglm_status issue_step_ptrs(dglm_handle *h, const double *const *in, double *const *out,
+                            cudaStream_t s);
 dglm_status ensure_rhs_scratch(dglm_handle *h);
 
 }  // namespace dglm

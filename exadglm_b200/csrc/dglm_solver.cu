@@ -200,6 +200,27 @@ dglm_status upload_operator_layout(dglm_handle *h) {
                     "operator upload");
 }
 
+}  // namespace
+
+// One LSERK step whose stage k reads in[k] and writes out[k] (for the
+// adjoint's recording of stage inputs); dt, tau and the wave-speed max as in
+// a normal step.
+dglm_status dglm::issue_step_ptrs(dglm_handle *h, const double *const *in, double *const *out,
+                                  cudaStream_t s) {
+  const int frozen = h->d.physics == DGLM_ADVECTION;
+  cudaError_t e = launch_step_begin(h->d.N, h->d.cfl, h->d.tmax, frozen, h->sc, h->dt_hist, s);
+  if (e == cudaSuccess && !frozen)
+    e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv, h->tau, s);
+  for (int st = 0; st < 5 && e == cudaSuccess; st++) {
+    StageArgs a = stage_args(h, in[st], out[st], st);
+    e = launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, s);
+  }
+  if (e == cudaSuccess) e = launch_step_end(h->sc, s);
+  return cuda_check(e, "step launch");
+}
+
+namespace {
+
 // Issues one LSERK step starting from u[cur] (ends in u[cur^1]).
 dglm_status issue_step(dglm_handle *h, int cur, cudaStream_t s) {
   const int frozen = h->d.physics == DGLM_ADVECTION;
@@ -647,7 +668,8 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
              v.threads, v.smem);
   else
     snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu",
-             v.mode == MODE_PIPE ? "pipe-dmma" : "dmma", v.E, v.CPT, v.WM, v.threads, v.smem);
+             v.mode == MODE_PIPE ? (v.groups == 2 ? "pipe2-dmma" : "pipe-dmma") : "dmma", v.E,
+             v.CPT, v.WM, v.threads, v.smem);
   return DGLM_OK;
 }
 

@@ -539,10 +539,10 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
-template <int PHYS, int N, int E, int WN, int WM, bool AS>
+template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG>
 static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
-  using C = PCfg<PHYS, N, E, WN, WM, AS>;
-  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG>;
+  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -552,9 +552,9 @@ static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int WN, int WM, bool AS>
+template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1>
 static Variant make_pipe() {
-  using C = PCfg<PHYS, N, E, WN, WM, AS>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG>;
   StageVariantInfo i{};
   i.mode = MODE_PIPE;
   i.E = E;
@@ -567,7 +567,8 @@ static Variant make_pipe() {
   i.KFP = C::KFP;
   i.threads = C::THREADS;
   i.smem = C::SMEM;
-  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS>};
+  i.groups = NG;
+  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG>};
 }
 
 template <int PHYS, int N, int E, int PREC>
@@ -626,6 +627,7 @@ static const std::vector<Variant> &variants();
 #define V_SIMT(P, NN, E, R, C) make_v<P, NN, MODE_SIMT, E, R, C, 1>()
 #define V_DMMA(P, NN, E, WN, WM) make_v<P, NN, MODE_DMMA, E, 1, WN, WM>()
 #define V_PIPE(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS>()
+#define V_PIPE2(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS, 2>()
 #define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
@@ -643,6 +645,7 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_SIMT(EUL, 4, 16, 5, 5), V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
               V_PIPE(EUL, 4, 8, 1, 5, false), V_PIPE(EUL, 4, 8, 1, 3, true),
+              V_PIPE2(EUL, 4, 8, 1, 5, true), V_PIPE2(EUL, 4, 8, 1, 3, true),
               V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5))

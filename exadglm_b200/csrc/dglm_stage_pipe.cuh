@@ -76,6 +76,23 @@ __device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long *b) {
 __device__ __forceinline__ void consumer_sync(int nthreads) {
   asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
+// named barrier `id` over `nthreads` threads (consumer groups of the
+// ping-pong variants use ids 1 + 2g and 2 + 2g)
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ bool group_all(bool v, int id, int nthreads) {
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)v), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
 // AND of a predicate over the consumer threads (named barrier 2)
 __device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
   unsigned r;
@@ -90,7 +107,7 @@ __device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
   return r != 0;
 }
 
-template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM>
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1>
 struct PCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -98,9 +115,10 @@ struct PCfg {
   static constexpr int MT = (Np + 7) / 8, NT = NCOL / 8;
   static constexpr int WN = WN_, WM = WM_ > MT ? MT : WM_;
   static constexpr int MGROUPS = (MT + WM - 1) / WM;
-  static constexpr int NWC = MGROUPS * (NT / WN);      // consumer warps
-  static constexpr int TC = 32 * NWC;                   // consumer threads
-  static constexpr int THREADS = TC + 32;               // + producer warp
+  static constexpr int NG = NG_;                        // consumer groups (ping-pong)
+  static constexpr int NWC = MGROUPS * (NT / WN);      // consumer warps per group
+  static constexpr int TC = 32 * NWC;                   // consumer threads per group
+  static constexpr int THREADS = NG * TC + 32;          // + producer warp
   static constexpr int KV = 3 * Np, KVP = (KV + 3) / 4 * 4;
   static constexpr int KF = NFF, KFP = (KF + 3) / 4 * 4;
   static constexpr int KS = KVP / 4 + KFP / 4;
@@ -112,13 +130,15 @@ struct PCfg {
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
   static constexpr int S_B = BROWS * BLD > NV * Np * EP ? BROWS * BLD : NV * Np * EP;
-  static constexpr int S_MISC = 8 + NFF / 2 + 1 + 40;   // barriers, Fmask, reduction
-  static constexpr size_t SMEM = sizeof(double) * ((size_t)S_AF + 2 * S_BUF + S_B + S_MISC);
+  static constexpr int S_MISC = 8 + NFF / 2 + 1 + 32 * NG + 8;  // barriers, Fmask, reduction
+  static constexpr size_t SMEM =
+      sizeof(double) * ((size_t)S_AF + 2 * S_BUF + NG * S_B + S_MISC);
   // bytes the producer's bulk copies deliver per tile
   static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE + S_VEL);
   static_assert(NCOL % 8 == 0 && NT % WN == 0, "n-tiles must split over the warps");
   static_assert((E * Np * 8) % 16 == 0 && (E * 8) % 16 == 0, "bulk copies need 16-byte sizes");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
+  static_assert(NG == 1 || NG == 2, "one or two consumer groups");
 };
 
 // Producer warp of the pipelined kernels: optional one-off bulk load of an
@@ -193,25 +213,25 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM>
-__global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1)
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_>
+__global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREADS, 1)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
-  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM>;
+  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 BLD = C::BLD, TC = C::TC;
   extern __shared__ __align__(16) double smem[];
   double *sAF = smem;
   double *sBuf0 = sAF + C::S_AF;
-  double *sB = sBuf0 + 2 * C::S_BUF;
-  unsigned long long *bars = reinterpret_cast<unsigned long long *>(sB + C::S_B);
+  double *sB0 = sBuf0 + 2 * C::S_BUF;   // one working buffer per consumer group
+  unsigned long long *bars = reinterpret_cast<unsigned long long *>(sB0 + C::NG * C::S_B);
   unsigned long long *full = bars, *empty = bars + 2, *abar = bars + 4;
   int *sFm = reinterpret_cast<int *>(bars + 8);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ttid = threadIdx.x, twarp = ttid >> 5, lane = ttid & 31;
   const long vs = a.vs;
 
-  if (tid == 0) {
+  if (ttid == 0) {
     mbar_init(&full[0], 33);
     mbar_init(&full[1], 33);
     mbar_init(&empty[0], C::NWC);
@@ -219,27 +239,36 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1
     mbar_init(abar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
+  for (int i = ttid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
 
   auto buf = [&](int b) { return sBuf0 + b * C::S_BUF; };
 
   // ------------------------------------------------------------- producer
-  if (warp == C::NWC) {
+  if (twarp == C::NG * C::NWC) {
     pipe_producer<C, PHYS>(a, ntiles, sAF, sBuf0, full, empty, abar, 8u * C::S_AF, lane);
     return;
   }
 
   // ------------------------------------------------------------ consumers
+  // Group g takes the CTA's tiles it = g, g + NG, ...; with two groups tile
+  // it always lands in buffer it & 1 = g, and one group's tensor-core phase
+  // overlaps the other's flux and epilogue phases.
+  const int grp = twarp / C::NWC;
+  const int warp = twarp - grp * C::NWC, tid = ttid - grp * TC;
+  const int bar_sync = 1 + 2 * grp, bar_and = 2 + 2 * grp;
+  double *sB = sB0 + grp * C::S_B;
+  auto consumer_sync = [&](int n) { group_sync(bar_sync, n); };
+  auto consumer_all = [&](bool v, int n) { return group_all(v, bar_and, n); };
   double acc[C::WM][C::WN][2];
   const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
   unsigned long long vmax = 0ull;
   bool ok = true;
   if (ASMEM) ok = consumer_all(mbar_wait(abar, 0), TC);
   const double *Afrag = ASMEM ? sAF : a.AT;
-  int it = 0;
-  for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, it++) {
+  int it = grp;
+  for (int t = blockIdx.x + grp * gridDim.x; ok && t < ntiles; t += C::NG * gridDim.x, it += C::NG) {
     const int b = it & 1;
     if (!consumer_all(mbar_wait(&full[b], (it >> 1) & 1), TC)) {
       ok = false;
@@ -433,10 +462,10 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM>::THREADS, 1
   if (!ok && tid == 0) atomicOr(&a.sc->flags, 4);
   if (PHYS == EUL && a.last_stage && !a.rhs_only) {
     vmax = warp_max_bits(vmax);
-    if (lane == 0) sMax[warp] = vmax;
+    if (lane == 0) sMax[grp * 32 + warp] = vmax;
     consumer_sync(TC);
     if (tid < 32) {
-      unsigned long long v = tid < C::NWC ? sMax[tid] : 0ull;
+      unsigned long long v = tid < C::NWC ? sMax[grp * 32 + tid] : 0ull;
       v = warp_max_bits(v);
       if (tid == 0) atomicMax(&a.sc->acc[a.sc->parity ^ 1], v);
     }

@@ -107,6 +107,8 @@ def test_checkpoint_spacing_and_replay_are_exact():
         s.adjoint_record(10, every)
         finals.append(s.get_state())
         grads.append(s.adjoint_backward(lamT))
+        # a second sweep over the same tape recomputes every segment
+        assert np.array_equal(s.adjoint_backward(lamT), grads[-1]), every
     for g in grads[1:]:
         assert np.array_equal(g, grads[0])
     for f in finals[1:]:
