@@ -28,7 +28,10 @@ EXPORTS = (
     "dglm_set_variant", "dglm_get_variant", "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
     "dglm_calc_maxv_dt_static", "dglm_adjoint_variant_count", "dglm_adjoint_variant_describe",
-    "dglm_adjoint_set_variant",
+    "dglm_adjoint_set_variant", "dglm_batch_create", "dglm_batch_add", "dglm_batch_finalize",
+    "dglm_batch_step", "dglm_batch_sync", "dglm_batch_count", "dglm_batch_get_state",
+    "dglm_batch_get_time", "dglm_batch_set_stream", "dglm_batch_kernel_launches",
+    "dglm_batch_device_bytes", "dglm_batch_destroy",
 )
 
 
@@ -52,6 +55,11 @@ _MESH_FIELDS = ["WDr", "WDs", "WDt", "LIFT", "matrix_order", "rx", "ry", "rz", "
 
 class MeshArrays(C.Structure):
     _fields_ = [(n, C.c_char if n == "matrix_order" else _P) for n in _MESH_FIELDS]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("physics", C.c_int), ("cfl", C.c_double), ("tau_scale", C.c_double),
+                ("tmax", C.c_double), ("device", C.c_int)]
 
 
 _lib = None
@@ -105,6 +113,20 @@ def lib():
         L.dglm_adjoint_rhs.argtypes = [_P, _P, _P, _P]
         L.dglm_adjoint_tape_bytes.argtypes = [_P, C.POINTER(C.c_size_t)]
         L.dglm_adjoint_variant_describe.argtypes = [I, I, I, C.c_char_p, C.c_size_t]
+        L.dglm_batch_create.argtypes = [C.POINTER(BatchDesc), C.POINTER(_P)]
+        L.dglm_batch_add.argtypes = [_P, I, I, C.POINTER(MeshArrays), _P, _P, C.POINTER(I)]
+        L.dglm_batch_finalize.argtypes = [_P]
+        L.dglm_batch_step.argtypes = [_P, I]
+        L.dglm_batch_sync.argtypes = [_P]
+        L.dglm_batch_count.argtypes = [_P]
+        L.dglm_batch_get_state.argtypes = [_P, I, _P, I]
+        L.dglm_batch_get_time.argtypes = [_P, I, C.POINTER(D), C.POINTER(D), C.POINTER(I)]
+        L.dglm_batch_set_stream.argtypes = [_P, _P]
+        L.dglm_batch_kernel_launches.argtypes = [_P]
+        L.dglm_batch_kernel_launches.restype = C.c_long
+        L.dglm_batch_device_bytes.argtypes = [_P]
+        L.dglm_batch_device_bytes.restype = C.c_size_t
+        L.dglm_batch_destroy.argtypes = [_P]
         L.dglm_adjoint_set_variant.argtypes = [_P, I]
         _lib = L
     return _lib
@@ -163,6 +185,33 @@ def _np_ptr(a):
     return C.c_void_p(a.ctypes.data)
 
 
+def mesh_arrays(problem, arr, matrix_order="c", with_velocity=True):
+    """A MeshArrays struct over contiguous copies of the problem's datain
+    arrays; returns (struct, the arrays it points into)."""
+    keep = {}
+
+    def f64(name, a, order="C"):
+        keep[name] = np.ascontiguousarray(np.asarray(a, np.float64).ravel(order))
+        return keep[name].ctypes.data
+
+    def i32(name, a):
+        keep[name] = np.ascontiguousarray(np.asarray(a, np.int32).ravel())
+        return keep[name].ctypes.data
+
+    m = MeshArrays()
+    m.matrix_order = matrix_order.encode()
+    order = "F" if matrix_order == "f" else "C"
+    for n in ("WDr", "WDs", "WDt", "LIFT"):
+        setattr(m, n, f64(n, arr[n], order))
+    for n in ("rx", "ry", "rz", "sx", "sy", "sz", "tx", "ty", "tz", "Fscale", "nx", "ny", "nz"):
+        setattr(m, n, f64(n, arr[n]))
+    for n in ("EtoB", "vmapF", "vmapP", "Fmask"):
+        setattr(m, n, i32(n, arr[n]))
+    if with_velocity and problem.vel is not None:
+        m.vx, m.vy, m.vz = (f64(n, problem.vel[i]) for i, n in enumerate(("vx", "vy", "vz")))
+    return m, keep
+
+
 class Solver:
     """A solver handle for one problem (see :mod:`exadglm_b200.problem`).
 
@@ -188,28 +237,7 @@ class Solver:
         check(L.dglm_create(C.byref(d), C.byref(h)))
         self.h, self.L = h, L
         arr = arrays if arrays is not None else problem.datain_arrays()
-        keep = {}
-
-        def f64(name, a, order="C"):
-            keep[name] = np.ascontiguousarray(np.asarray(a, np.float64).ravel(order))
-            return keep[name].ctypes.data
-
-        def i32(name, a):
-            keep[name] = np.ascontiguousarray(np.asarray(a, np.int32).ravel())
-            return keep[name].ctypes.data
-
-        m = MeshArrays()
-        m.matrix_order = matrix_order.encode()
-        order = "F" if matrix_order == "f" else "C"
-        for n in ("WDr", "WDs", "WDt", "LIFT"):
-            setattr(m, n, f64(n, arr[n], order))
-        for n in ("rx", "ry", "rz", "sx", "sy", "sz", "tx", "ty", "tz", "Fscale", "nx", "ny",
-                  "nz"):
-            setattr(m, n, f64(n, arr[n]))
-        for n in ("EtoB", "vmapF", "vmapP", "Fmask"):
-            setattr(m, n, i32(n, arr[n]))
-        if problem.vel is not None:
-            m.vx, m.vy, m.vz = (f64(n, problem.vel[i]) for i, n in enumerate(("vx", "vy", "vz")))
+        m, self._keep = mesh_arrays(problem, arr, matrix_order)
         check(L.dglm_upload_mesh(h, C.byref(m)))
         if variant is None:
             from .tune import cached_variant
@@ -321,6 +349,80 @@ class Solver:
     def close(self):
         if getattr(self, "h", None):
             self.L.dglm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchSolver:
+    """Many independent advection problems (orders 2..6, constant velocity
+    each) advanced together by one persistent launch per LSERK stage.
+
+    ``problems`` share cfl, tau_scale and tmax (taken from the first)."""
+
+    def __init__(self, problems, device=0, cfl=None, tau_scale=None, tmax=None):
+        L = lib()
+        p0 = problems[0]
+        d = BatchDesc()
+        d.physics = ADVECTION
+        d.cfl = p0.cfl if cfl is None else cfl
+        d.tau_scale = p0.tau_scale if tau_scale is None else tau_scale
+        d.tmax = p0.tmax if tmax is None else tmax
+        d.device = device
+        h = _P()
+        check(L.dglm_batch_create(C.byref(d), C.byref(h)))
+        self.h, self.L, self.problems = h, L, list(problems)
+        try:
+            for p in problems:
+                if p.physics != "advection" or p.vel is None:
+                    raise ValueError("BatchSolver: advection problems with a velocity only")
+                v = np.asarray(p.vel, np.float64)
+                vel = np.ascontiguousarray(v[:, 0])
+                if not (v.min(axis=1) == v.max(axis=1)).all():
+                    raise ValueError("BatchSolver: each problem's velocity must be constant")
+                m, keep = mesh_arrays(p, p.datain_arrays(), with_velocity=False)
+                u0 = np.ascontiguousarray(np.asarray(p.u0, np.float64).ravel())
+                idx = C.c_int()
+                check(L.dglm_batch_add(h, p.N, p.K, C.byref(m), u0.ctypes.data, vel.ctypes.data,
+                                       C.byref(idx)))
+            check(L.dglm_batch_finalize(h))
+        except Exception:
+            self.close()
+            raise
+
+    def step(self, nsteps=1):
+        check(self.L.dglm_batch_step(self.h, int(nsteps)))
+
+    def sync(self):
+        check(self.L.dglm_batch_sync(self.h))
+
+    def get_state(self, i):
+        p = self.problems[i]
+        out = np.empty(p.K * p.Np)
+        check(self.L.dglm_batch_get_state(self.h, int(i), out.ctypes.data, 0))
+        return out
+
+    def time(self, i):
+        t, dt, ts = C.c_double(), C.c_double(), C.c_int()
+        check(self.L.dglm_batch_get_time(self.h, int(i), C.byref(t), C.byref(dt), C.byref(ts)))
+        return t.value, dt.value, ts.value
+
+    def set_stream(self, stream_ptr):
+        check(self.L.dglm_batch_set_stream(self.h, C.c_void_p(int(stream_ptr))))
+
+    def kernel_launches(self):
+        return int(self.L.dglm_batch_kernel_launches(self.h))
+
+    def device_bytes(self):
+        return int(self.L.dglm_batch_device_bytes(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dglm_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -83,6 +83,35 @@ def advection_gaussian(n=8, N=3, v=(1.0, 0.5, 0.25), center=(0.5, 0.5, 0.5), wid
                    name=f"advection_gaussian_N{N}_n{n}")
 
 
+def batch_instances(count=256, seed=0, n_range=(4, 24), orders=(2, 6), cfl=0.5,
+                    tau_scale=1.2, tmax=1000.0):
+    """Independent advection problems for batching, drawn from
+    numpy.random.default_rng(seed): per instance n ~ U{n_range}, N ~ U{orders},
+    v ~ U[-1, 1]^3, Gaussian centre ~ U[0, 1]^3, width w ~ U[0.05, 0.2],
+    u0 = exp(-|x - c|^2 / w^2) on the periodic unit cube of n^3 x 6 tets.
+    Meshes are shared between instances of the same (n, N); the velocity is
+    a broadcast view (constant per instance)."""
+    rng = np.random.default_rng(seed)
+    meshes = {}
+    out = []
+    for i in range(count):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        N = int(rng.integers(orders[0], orders[1] + 1))
+        v = rng.uniform(-1.0, 1.0, 3)
+        c = rng.uniform(0.0, 1.0, 3)
+        w = float(rng.uniform(0.05, 0.2))
+        if (n, N) not in meshes:
+            meshes[(n, N)] = Mesh3D(N, UniformBox(n + 1, n + 1, n + 1))
+        mesh = meshes[(n, N)]
+        x, y, z = _nodes(mesh)
+        r2 = (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2
+        u0 = np.exp(-r2 / (w * w))[None, :]
+        vel = np.broadcast_to(v[:, None], (3, x.size))
+        out.append(Problem("advection", N, mesh, u0, vel, cfl=cfl, tau_scale=tau_scale,
+                           tmax=tmax, name=f"batch{i}_N{N}_n{n}"))
+    return out
+
+
 def euler_sine(n=32, N=4, v=(1.0, 0.5, 0.25), p=1.0, gamma=1.4, cfl=0.4, tau_scale=1.2,
                tmax=1000.0, noise=0.0, seed=0, mesh=None):
     mesh = mesh or Mesh3D(N, UniformBox(n + 1, n + 1, n + 1))

@@ -246,6 +246,36 @@ dglm_status dglm_adjoint_variant_describe(int physics, int N, int variant, char 
                                           size_t len);
 dglm_status dglm_adjoint_set_variant(dglm_handle *h, int variant);
 
+/* ---- batches of independent meshes -------------------------------------
+ * No counterpart in the reference (one mesh per process there).  Linear
+ * advection on many meshes of different size and order (2..6) advanced
+ * together: one persistent kernel launch per LSERK stage covers every
+ * instance, steps run as CUDA graphs, each instance has its own CFL dt
+ * (clipped to tmax) and time.  The velocity of an instance is constant.
+ * Use: dglm_batch_create, dglm_batch_add per instance (host arrays in the
+ * layouts of dglm_upload_mesh; u0 has K*Np values), dglm_batch_finalize
+ * (uploads, builds the tile list, computes the per-instance dt), then
+ * dglm_batch_step / dglm_batch_get_state / dglm_batch_get_time. */
+typedef struct dglm_batch dglm_batch;
+typedef struct {
+    int physics;        /* DGLM_ADVECTION */
+    double cfl, tau_scale, tmax;
+    int device;         /* CUDA device; -1 = current */
+} dglm_batch_desc;
+dglm_status dglm_batch_create(const dglm_batch_desc *desc, dglm_batch **out);
+dglm_status dglm_batch_add(dglm_batch *b, int N, int K, const dglm_mesh_arrays *m,
+                           const double *u0, const double *velocity, int *index);
+dglm_status dglm_batch_finalize(dglm_batch *b);
+dglm_status dglm_batch_step(dglm_batch *b, int nsteps);
+dglm_status dglm_batch_sync(dglm_batch *b);
+int dglm_batch_count(dglm_batch *b);
+dglm_status dglm_batch_get_state(dglm_batch *b, int index, double *u, int on_device);
+dglm_status dglm_batch_get_time(dglm_batch *b, int index, double *t, double *dt, int *tstep);
+dglm_status dglm_batch_set_stream(dglm_batch *b, void *stream);
+long dglm_batch_kernel_launches(dglm_batch *b);
+size_t dglm_batch_device_bytes(dglm_batch *b);
+dglm_status dglm_batch_destroy(dglm_batch *b);
+
 #ifdef __cplusplus
 }
 #endif
