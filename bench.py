@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint"], default=None,
+    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint", "batch"], default=None,
                     help="run one section alone (profiling); prints that section's object")
     ap.add_argument("--accuracy-steps", type=int, default=200,
                     help="steps of the mixed-vs-FP64 relative L2 comparison")
@@ -59,6 +59,10 @@ def parse():
                     help="hexahedra per axis of the adjoint workload (K = 6 n^3)")
     ap.add_argument("--adjoint-steps", type=int, default=500)
     ap.add_argument("--adjoint-every", type=int, default=50, help="checkpoint spacing")
+    ap.add_argument("--batch-count", type=int, default=256, help="instances of the batch workload")
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-sequential", type=int, default=256,
+                    help="instances also run one by one through single-mesh handles")
     return ap.parse_args()
 
 
@@ -354,6 +358,63 @@ def adjoint_section(a, stream):
     return out
 
 
+def batch_section(a, stream):
+    """Many independent advection meshes (n in 4..24, N in 2..6, seeded):
+    one launch per stage for the whole batch, against the same instances run
+    one after another through single-mesh handles.  Both timed with CUDA
+    events around the stepping only."""
+    import torch
+    from exadglm_b200 import problem as P
+    from exadglm_b200.capi import BatchSolver, Solver
+    t0 = time.perf_counter()
+    probs = P.batch_instances(count=a.batch_count, seed=0)
+    setup_s = time.perf_counter() - t0
+    S = a.batch_steps
+    dofs = sum(p.K * p.Np for p in probs) * 5          # DOF-stages per step
+
+    def timed(fn):
+        e0, e1 = _events(stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    b = BatchSolver(probs)
+    b.set_stream(stream.cuda_stream)
+    b.step(3)
+    b.sync()
+    ms = timed(lambda: b.step(S))
+    launches = b.kernel_launches()
+    b.close()
+    out = {
+        "workload": f"{len(probs)} advection instances, n~U{{4..24}}, N~U{{2..6}}, seed 0, "
+                    f"{S} steps, CFL 0.5",
+        "K_total": int(sum(p.K for p in probs)),
+        "dof_stages_per_step": dofs, "steps": S, "ms": ms,
+        "value": dofs * S / (ms * 1e-3), "unit": UNIT, "gpu_launches": launches,
+        "instances_by_order": {str(N): sum(1 for p in probs if p.N == N) for N in range(2, 7)},
+        "host_setup_s": setup_s,
+    }
+    nseq = min(a.batch_sequential, len(probs))
+    if nseq:
+        seq_ms, seq_dofs = 0.0, 0
+        for p in probs[:nseq]:
+            s = Solver(p)
+            s.set_stream(stream.cuda_stream)
+            s.step(2)
+            s.sync()
+            seq_ms += timed(lambda: s.step(S))
+            seq_dofs += p.K * p.Np * 5 * S
+            s.close()
+        out["sequential"] = {"instances": nseq, "ms": seq_ms,
+                             "value": seq_dofs / (seq_ms * 1e-3),
+                             "what": "the same instances one after another, one handle each"}
+        out["speedup_vs_sequential"] = out["value"] / out["sequential"]["value"]
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -387,9 +448,9 @@ def main():
 
     p = build_problem(a)
     stream = torch.cuda.Stream()
-    if a.only in ("mixed", "adjoint"):
+    if a.only in ("mixed", "adjoint", "batch"):
         res = (mixed_section(a, p, stream, float("nan")) if a.only == "mixed"
-               else adjoint_section(a, stream))
+               else adjoint_section(a, stream) if a.only == "adjoint" else batch_section(a, stream))
         if rank == 0:
             print(json.dumps({a.only: res}), flush=True)
         if dist is not None:

@@ -571,10 +571,10 @@ static Variant make_pipe() {
   return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG>};
 }
 
-template <int PHYS, int N, int E, int PREC>
+template <int PHYS, int N, int E, int PREC, int NWC>
 static cudaError_t launch_mixed(const StageArgs &a, cudaStream_t s) {
-  using C = MCfg<PHYS, N, E, PREC>;
-  auto k = stage_mixed_kernel<PHYS, N, E, PREC>;
+  using C = MCfg<PHYS, N, E, PREC, NWC>;
+  auto k = stage_mixed_kernel<PHYS, N, E, PREC, NWC>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -584,9 +584,9 @@ static cudaError_t launch_mixed(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int PREC>
+template <int PHYS, int N, int E, int PREC, int NWC = 8>
 static Variant make_mixed() {
-  using C = MCfg<PHYS, N, E, PREC>;
+  using C = MCfg<PHYS, N, E, PREC, NWC>;
   StageVariantInfo i{};
   i.mode = MODE_MIXED;
   i.E = E;
@@ -597,7 +597,7 @@ static Variant make_mixed() {
   i.kva = C::KVA;
   i.kfa = C::KFA;
   i.bimg = C::BIMG;
-  return Variant{i, &launch_mixed<PHYS, N, E, PREC>};
+  return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC>};
 }
 
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM>
@@ -630,6 +630,8 @@ static const std::vector<Variant> &variants();
 #define V_PIPE2(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS, 2>()
 #define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
+#define V_TF32W(P, NN, E, W) make_mixed<P, NN, E, PREC_TF32, W>()
+#define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -646,7 +648,8 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
               V_PIPE(EUL, 4, 8, 1, 5, false), V_PIPE(EUL, 4, 8, 1, 3, true),
               V_PIPE2(EUL, 4, 8, 1, 5, true), V_PIPE2(EUL, 4, 8, 1, 3, true),
-              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8))
+              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_TF32W(EUL, 4, 8, 16),
+              V_BF16W(EUL, 4, 8, 16))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5))

@@ -16,10 +16,10 @@
 // Per tile: flux phase writes the volume operand -> one thread issues the
 // volume MMAs and commits to an mbarrier -> once they have read the operand
 // the face phase overwrites it with the lift operand -> lift MMAs -> the
-// accumulator is read back with tcgen05.ld into the FP64 epilogue.  The K
-// range is spread over NACC tensor-memory accumulators (a slice of k-steps
-// each) that are summed in FP64 on read-back, so each FP32 running sum covers
-// only a slice of the terms.
+// accumulator is read back with tcgen05.ld into the FP64 epilogue.  The MMAs
+// of a tile go round-robin to NACC tensor-memory accumulators, so
+// consecutive MMAs do not wait on each other and each FP32 running sum
+// covers only 1/NACC of the terms; the partials are added on read-back.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -90,21 +90,25 @@ __device__ __forceinline__ unsigned long long smem_desc(unsigned saddr, unsigned
          ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// x = hi + lo with hi, lo in the operand format (stored as raw bits)
+// x = hi + lo with hi, lo in the operand format (stored as raw bits).  The
+// split runs on the FP32 value of x (one conversion from FP64): hi carries
+// 11 (TF32) or 8 (BF16) significant bits and lo the next ones, so the FP32
+// rounding of x (2^-24) is below what the pair keeps.
 __device__ __forceinline__ void split_tf32(double x, unsigned &hi, unsigned &lo) {
   const float f = (float)x;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(f));
-  const float r = (float)(x - (double)__uint_as_float(hi));
+  const float r = f - __uint_as_float(hi);
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
 }
 __device__ __forceinline__ void split_bf16(double x, unsigned short &hi, unsigned short &lo) {
-  const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
-  const __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+  const float f = (float)x;
+  const __nv_bfloat16 h = __float2bfloat16_rn(f);
+  const __nv_bfloat16 l = __float2bfloat16_rn(f - __bfloat162float(h));
   hi = __bfloat16_as_ushort(h);
   lo = __bfloat16_as_ushort(l);
 }
 
-template <int PHYS, int N, int E_, int PREC>
+template <int PHYS, int N, int E_, int PREC, int NWC_ = 8>
 struct MCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -123,6 +127,9 @@ struct MCfg {
   // every accumulator receives at least one k-step, and they fit in 512 columns
   static constexpr int NACC0 = NPAD * 8 <= 512 ? 8 : NPAD * 4 <= 512 ? 4 : 2;
   static constexpr int NACC = NACC0 < KST ? NACC0 : KST;
+  // MMA issuers: lane 0 of warps 0..NISS-1, issuer w owns accumulators j with
+  // j % NISS == w (one thread's tcgen05.mma issue rate bounds tiny MMAs)
+  static constexpr int NISS = NACC % 4 == 0 ? 4 : NACC % 2 == 0 ? 2 : 1;
   static constexpr int TCOLS = NACC * NPAD <= 32 ? 32 : NACC * NPAD <= 64 ? 64
                                : NACC * NPAD <= 128 ? 128 : NACC * NPAD <= 256 ? 256 : 512;
   static constexpr int SBO_A = KAM / T * 128, SBO_BV = KVA / T * 128, SBO_BF = KFA / T * 128;
@@ -130,7 +137,7 @@ struct MCfg {
   static constexpr int A_BYTES = M * KAM * S;                   // one part (hi or lo)
   static constexpr int BV_BYTES = NPAD * KVA * S, BF_BYTES = NPAD * KFA * S;
   static constexpr int BIMG = 2 * (BV_BYTES + BF_BYTES);        // hi then lo
-  static constexpr int NWC = 8, TC = 32 * NWC, THREADS = TC + 32;
+  static constexpr int NWC = NWC_, TC = 32 * NWC, THREADS = TC + 32;
   // FP64 pipeline buffers (as in PCfg)
   static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
   static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
@@ -149,6 +156,8 @@ struct MCfg {
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
   static_assert(NPAD <= 256, "MMA N limit");
   static_assert(NACC * NPAD <= 512, "tensor memory has 512 columns");
+  static_assert(NWC >= NISS && NACC % NISS == 0, "issuers split the accumulators evenly");
+  static_assert(SMEM < (1u << 18), "descriptor start addresses must fit 14 bits (>> 4)");
 };
 
 // byte offset of element (r, k) in a K-major core-matrix image with 8-row
@@ -175,10 +184,10 @@ __device__ __forceinline__ void put_split(unsigned char *Ahi, unsigned char *Alo
   }
 }
 
-template <int PHYS, int N, int E_, int PREC>
-__global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC>::THREADS, 1)
+template <int PHYS, int N, int E_, int PREC, int NWC_>
+__global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
     stage_mixed_kernel(const StageArgs a, int ntiles) {
-  using C = MCfg<PHYS, N, E_, PREC>;
+  using C = MCfg<PHYS, N, E_, PREC, NWC_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 TC = C::TC;
   extern __shared__ __align__(16) double smem[];
@@ -201,7 +210,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC>::THREADS, 1)
     mbar_init(&empty[0], C::NWC);
     mbar_init(&empty[1], C::NWC);
     mbar_init(abar, 1);
-    mbar_init(mbar, 1);
+    mbar_init(mbar, C::NISS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
@@ -269,21 +278,27 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC>::THREADS, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     consumer_sync(TC);
-    if (tid == 0) {
+    if (lane == 0 && warp < C::NISS) {
       tc_fence_after();
-#pragma unroll 1
+      // descriptors of k-step 0; a k-step advances the start address by 256
+      // bytes (16 in the descriptor's address field)
+      const unsigned long long ah0 = smem_desc(aHi, 128, C::SBO_A);
+      const unsigned long long al0 = smem_desc(aLo, 128, C::SBO_A);
+      const unsigned long long bh0 = smem_desc(bHiV, 128, C::SBO_BV);
+      const unsigned long long bl0 = smem_desc(bLoV, 128, C::SBO_BV);
+#pragma unroll
       for (int ks = 0; ks < C::KSV; ks++) {
-        const unsigned ao = ks * 256;
-        const unsigned long long ah = smem_desc(aHi + ao, 128, C::SBO_A);
-        const unsigned long long al = smem_desc(aLo + ao, 128, C::SBO_A);
-        const unsigned long long bh = smem_desc(bHiV + ao, 128, C::SBO_BV);
-        const unsigned long long bl = smem_desc(bLoV + ao, 128, C::SBO_BV);
-        const int j = ks * C::NACC / C::KST;          // accumulator of this k-step
-        const int first = ks == (j * C::KST + C::NACC - 1) / C::NACC;
-        const unsigned d = tmem + j * C::NPAD;
-        tc_mma<PREC>(d, al, bh, C::IDESC, !first);
-        tc_mma<PREC>(d, ah, bl, C::IDESC, 1);
-        tc_mma<PREC>(d, ah, bh, C::IDESC, 1);
+        // MMA g of the tile (pass p of k-step ks) goes to accumulator
+        // g % NACC, issued by that accumulator's issuer; the first NACC MMAs
+        // initialise the accumulators
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+          const int g = 3 * ks + p, j = g % C::NACC;
+          if (j % C::NISS != warp) continue;
+          const unsigned long long ad = (p == 0 ? al0 : ah0) + 16ull * ks;
+          const unsigned long long bd = (p == 1 ? bl0 : bh0) + 16ull * ks;
+          tc_mma<PREC>(tmem + j * C::NPAD, ad, bd, C::IDESC, g >= C::NACC);
+        }
       }
       tc_commit(mbar);
     }
@@ -327,22 +342,22 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC>::THREADS, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     consumer_sync(TC);
-    if (tid == 0) {
+    if (lane == 0 && warp < C::NISS) {
       tc_fence_after();
-#pragma unroll 1
+      const unsigned long long ah0 = smem_desc(aHi, 128, C::SBO_A);
+      const unsigned long long al0 = smem_desc(aLo, 128, C::SBO_A);
+      const unsigned long long bh0 = smem_desc(bHiF, 128, C::SBO_BF);
+      const unsigned long long bl0 = smem_desc(bLoF, 128, C::SBO_BF);
+#pragma unroll
       for (int ks = 0; ks < C::KSF; ks++) {
-        const unsigned ao = ks * 256;
-        const unsigned long long ah = smem_desc(aHi + ao, 128, C::SBO_A);
-        const unsigned long long al = smem_desc(aLo + ao, 128, C::SBO_A);
-        const unsigned long long bh = smem_desc(bHiF + ao, 128, C::SBO_BF);
-        const unsigned long long bl = smem_desc(bLoF + ao, 128, C::SBO_BF);
-        const int kg = C::KSV + ks;                   // global k-step
-        const int j = kg * C::NACC / C::KST;
-        const int first = kg == (j * C::KST + C::NACC - 1) / C::NACC;
-        const unsigned d = tmem + j * C::NPAD;
-        tc_mma<PREC>(d, al, bh, C::IDESC, !first);
-        tc_mma<PREC>(d, ah, bl, C::IDESC, 1);
-        tc_mma<PREC>(d, ah, bh, C::IDESC, 1);
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+          const int g = 3 * (C::KSV + ks) + p, j = g % C::NACC;   // MMA index within the tile
+          if (j % C::NISS != warp) continue;
+          const unsigned long long ad = (p == 0 ? al0 : ah0) + 16ull * ks;
+          const unsigned long long bd = (p == 1 ? bl0 : bh0) + 16ull * ks;
+          tc_mma<PREC>(tmem + j * C::NPAD, ad, bd, C::IDESC, g >= C::NACC);
+        }
       }
       tc_commit(mbar);
     }
@@ -355,26 +370,30 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC>::THREADS, 1)
 
     // 5. accumulator -> sR as [v][i][EP] (row m lives in TMEM lane
     //    (m % 16) + 32 (m / 16) for M = 64, lane m for M = 128)
-    if (warp < 4) {
-      const int m = C::M == 64 ? 16 * warp + lane : 32 * warp + lane;
+    {
+      // warp w reads lane quarter w % 4 (the quarter a warp may access) and
+      // every (NWC / 4)-th group of 8 columns
+      const int q = warp & 3, cstart = 8 * (warp >> 2), cstep = 8 * (C::NWC / 4);
+      const int m = C::M == 64 ? 16 * q + lane : 32 * q + lane;
       const bool valid = (C::M == 64 ? lane < 16 : true) && m < C::NCOL;
       const int v = m / E, e = m - (m / E) * E;
 #pragma unroll 1
-      for (int c0 = 0; c0 < C::NPAD; c0 += 8) {
-        double sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int c0 = cstart; c0 < C::NPAD; c0 += cstep) {
+        // the partial sums are added in FP32 (the error of each partial, a
+        // slice of the K terms, dominates) and converted once
         float r[C::NACC][8];
 #pragma unroll
         for (int j = 0; j < C::NACC; j++)
-          tmem_ld8(tmem + ((unsigned)(32 * warp) << 16) + j * C::NPAD + c0, r[j]);
+          tmem_ld8(tmem + ((unsigned)(32 * q) << 16) + j * C::NPAD + c0, r[j]);
         tmem_ld_wait();
-#pragma unroll
-        for (int j = 0; j < C::NACC; j++)
-#pragma unroll
-          for (int q = 0; q < 8; q++) sum[q] += (double)r[j][q];
         if (valid) {
 #pragma unroll
-          for (int q = 0; q < 8; q++)
-            if (c0 + q < Np) sR[(v * Np + c0 + q) * EP + e] = sum[q];
+          for (int c = 0; c < 8; c++) {
+            float sum = r[0][c];
+#pragma unroll
+            for (int j = 1; j < C::NACC; j++) sum += r[j][c];
+            if (c0 + c < Np) sR[(v * Np + c0 + c) * EP + e] = (double)sum;
+          }
         }
       }
     }
