@@ -14,8 +14,9 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdglm.so"
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NONFINITE, ERR_UNSUPPORTED, ERR_STATE, ERR_NOMEM, ERR_IO = range(8)
 ADVECTION, EULER = 0, 1
-PREC_FP64, PREC_TF32X3, PREC_BF16X3 = 0, 1, 2
-PRECISIONS = {"fp64": PREC_FP64, "tf32x3": PREC_TF32X3, "bf16x3": PREC_BF16X3}
+PREC_FP64, PREC_TF32X3, PREC_BF16X3, PREC_BF16X6 = 0, 1, 2, 3
+PRECISIONS = {"fp64": PREC_FP64, "tf32x3": PREC_TF32X3, "bf16x3": PREC_BF16X3,
+              "bf16x6": PREC_BF16X6}
 
 # every symbol include/dglm.h declares
 EXPORTS = (
@@ -150,6 +151,8 @@ def variant_precision(desc):
         return "tf32x3"
     if desc.startswith("tcgen05-bf16x3"):
         return "bf16x3"
+    if desc.startswith("tcgen05-bf16x6"):
+        return "bf16x6"
     return "fp64"
 
 

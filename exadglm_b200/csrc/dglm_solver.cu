@@ -125,28 +125,32 @@ uint16_t bf16_rne(float f) {
 // Operator image of a mixed-precision variant: B = A^T blocks (volume: the
 // 3Np columns of [WDr WDs WDt], lift: the NFF columns of -LIFT), each
 // npad rows x (kva | kfa) K, K-major in 8-row x 16-byte core matrices,
-// split into hi and lo parts: [hi vol][hi lift][lo vol][lo lift].
+// split into parts (TF32 / BF16: hi, lo; BF16x6: three BF16 parts):
+// [part 0 vol][part 0 lift][part 1 vol][part 1 lift]...  The split uses the
+// exact FP64 residual at every level.
 std::vector<unsigned char> mixed_image(const dglm_handle *h, const StageVariantInfo &v) {
   const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
   const bool tf = v.prec == DGLM_PREC_TF32X3;
+  const int parts = v.prec == DGLM_PREC_BF16X6 ? 3 : 2;
   const int S = tf ? 4 : 2, T = 16 / S;
   const int bv = v.npad * v.kva * S, bf = v.npad * v.kfa * S;
   std::vector<unsigned char> img((size_t)v.bimg, 0);
   auto put = [&](size_t base, int sbo, int r, int k, double x) {
     const size_t off = base + (size_t)(r / 8) * sbo + (size_t)(k / T) * 128 + (r % 8) * 16 +
                        (k % T) * S;
-    const size_t lo_base = (size_t)bv + bf;   // lo part follows the hi part
-    if (tf) {
-      const uint32_t hi = tf32_rna((float)x);
-      const uint32_t lo = tf32_rna((float)(x - (double)f32_of(hi)));
-      std::memcpy(&img[off], &hi, 4);
-      std::memcpy(&img[off + lo_base], &lo, 4);
-    } else {
-      const uint16_t hi = bf16_rne((float)x);
-      const uint32_t hb = (uint32_t)hi << 16;
-      const uint16_t lo = bf16_rne((float)(x - (double)f32_of(hb)));
-      std::memcpy(&img[off], &hi, 2);
-      std::memcpy(&img[off + lo_base], &lo, 2);
+    double rest = x;
+    for (int p = 0; p < parts; p++) {
+      const size_t o = off + (size_t)p * (bv + bf);
+      if (tf) {
+        const uint32_t q = tf32_rna((float)rest);
+        std::memcpy(&img[o], &q, 4);
+        rest -= (double)f32_of(q);
+      } else {
+        const uint16_t q = bf16_rne((float)rest);
+        const uint32_t qb = (uint32_t)q << 16;
+        std::memcpy(&img[o], &q, 2);
+        rest -= (double)f32_of(qb);
+      }
     }
   };
   for (int n = 0; n < Np; n++) {
@@ -273,7 +277,7 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
                      "dglm_create: order N=" + std::to_string(d.N) + " is not built (1..8)");
   if (d.K <= 0) return set_error(DGLM_ERR_INVALID, "dglm_create: K must be positive");
   if (d.precision != DGLM_PREC_FP64 && d.precision != DGLM_PREC_TF32X3 &&
-      d.precision != DGLM_PREC_BF16X3)
+      d.precision != DGLM_PREC_BF16X3 && d.precision != DGLM_PREC_BF16X6)
     return set_error(DGLM_ERR_INVALID, "dglm_create: unknown precision");
   int first = -1;
   {
@@ -594,6 +598,9 @@ dglm_status dglm_sync(dglm_handle *h) {
   int flags = 0;
   e = cudaMemcpy(&flags, &h->sc->flags, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_check(e, "dglm_sync");
+  if (flags & 4)
+    return set_error(DGLM_ERR_CUDA,
+                     "a bounded wait in a pipelined stage kernel expired; results are invalid");
   if (flags & 3)
     return set_error(DGLM_ERR_NONFINITE, "non-finite wave speed, dt or state met");
   return DGLM_OK;
@@ -649,8 +656,14 @@ dglm_status dglm_rhs(dglm_handle *h, const double *const *u, double *const *rhs)
   for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
     e = cudaMemcpyAsync(rhs[v], h->rhs_out + (size_t)v * h->vs, sizeof(double) * n,
                         cudaMemcpyDeviceToDevice, s);
+  int flags = 0;
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  return cuda_check(e, "dglm_rhs");
+  if (e == cudaSuccess) e = cudaMemcpy(&flags, &h->sc_s->flags, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_rhs");
+  if (flags & 4)
+    return set_error(DGLM_ERR_CUDA,
+                     "dglm_rhs: a bounded wait in a pipelined stage kernel expired");
+  return DGLM_OK;
 }
 
 int dglm_variant_count(int physics, int N) { return stage_variant_count(physics, N); }
@@ -664,8 +677,10 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
              v.smem);
   else if (v.mode == MODE_MIXED)
     snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
-             v.prec == DGLM_PREC_TF32X3 ? "tcgen05-tf32x3" : "tcgen05-bf16x3", v.E, v.npad,
-             v.threads, v.smem);
+             v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"
+             : v.prec == DGLM_PREC_BF16X6 ? "tcgen05-bf16x6"
+                                          : "tcgen05-bf16x3",
+             v.E, v.npad, v.threads, v.smem);
   else
     snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu",
              v.mode == MODE_PIPE ? (v.groups == 2 ? "pipe2-dmma" : "pipe-dmma") : "dmma", v.E,

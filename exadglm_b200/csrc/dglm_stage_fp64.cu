@@ -592,7 +592,9 @@ static Variant make_mixed() {
   i.E = E;
   i.threads = C::THREADS;
   i.smem = C::SMEM;
-  i.prec = PREC == PREC_TF32 ? DGLM_PREC_TF32X3 : DGLM_PREC_BF16X3;
+  i.prec = PREC == PREC_TF32 ? DGLM_PREC_TF32X3
+           : PREC == PREC_BF16X6 ? DGLM_PREC_BF16X6
+                                 : DGLM_PREC_BF16X3;
   i.npad = C::NPAD;
   i.kva = C::KVA;
   i.kfa = C::KFA;
@@ -631,6 +633,7 @@ static const std::vector<Variant> &variants();
 #define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define V_TF32W(P, NN, E, W) make_mixed<P, NN, E, PREC_TF32, W>()
+#define V_BF16X6(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16X6, W>()
 #define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
@@ -648,8 +651,8 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
               V_PIPE(EUL, 4, 8, 1, 5, false), V_PIPE(EUL, 4, 8, 1, 3, true),
               V_PIPE2(EUL, 4, 8, 1, 5, true), V_PIPE2(EUL, 4, 8, 1, 3, true),
-              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_TF32W(EUL, 4, 8, 16),
-              V_BF16W(EUL, 4, 8, 16))
+              V_TF32W(EUL, 4, 8, 16), V_BF16W(EUL, 4, 8, 16), V_BF16X6(EUL, 4, 8, 16),
+              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_BF16X6(EUL, 4, 8, 8))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5))
@@ -658,7 +661,8 @@ DGLM_VARIANTS(EUL, 8, V_DMMA(EUL, 8, 8, 1, 7), V_SIMT(EUL, 8, 4, 8, 5))
 DGLM_VARIANTS(ADV, 1, V_SIMT(ADV, 1, 256, 4, 4), V_DMMA(ADV, 1, 64, 2, 1))
 DGLM_VARIANTS(ADV, 2, V_SIMT(ADV, 2, 128, 5, 4), V_DMMA(ADV, 2, 64, 2, 2))
 DGLM_VARIANTS(ADV, 3, V_DMMA(ADV, 3, 64, 2, 3), V_SIMT(ADV, 3, 64, 5, 4),
-              V_PIPE(ADV, 3, 32, 1, 3, true), V_TF32(ADV, 3, 32), V_BF16(ADV, 3, 32))
+              V_PIPE(ADV, 3, 32, 1, 3, true), V_TF32(ADV, 3, 32), V_BF16(ADV, 3, 32),
+              V_BF16X6(ADV, 3, 32, 8))
 DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5))
 DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7))
 DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6))

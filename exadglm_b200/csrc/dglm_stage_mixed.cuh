@@ -24,7 +24,7 @@
 
 #include <cuda_bf16.h>
 
-enum { PREC_BF16 = 1, PREC_TF32 = 2 };
+enum { PREC_BF16 = 1, PREC_TF32 = 2, PREC_BF16X6 = 3 };
 
 // ---- tcgen05 / TMEM helpers ------------------------------------------------
 __device__ __forceinline__ void tmem_alloc(unsigned *dst_smem, unsigned ncols) {
@@ -108,6 +108,18 @@ __device__ __forceinline__ void split_bf16(double x, unsigned short &hi, unsigne
   lo = __bfloat16_as_ushort(l);
 }
 
+// x = b0 + b1 + b2 in BF16 (24 significant bits of the FP32 value of x)
+__device__ __forceinline__ void split_bf16x3(double x, unsigned short (&p)[3]) {
+  const float f = (float)x;
+  const __nv_bfloat16 b0 = __float2bfloat16_rn(f);
+  const float r1 = f - __bfloat162float(b0);
+  const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 b2 = __float2bfloat16_rn(r1 - __bfloat162float(b1));
+  p[0] = __bfloat16_as_ushort(b0);
+  p[1] = __bfloat16_as_ushort(b1);
+  p[2] = __bfloat16_as_ushort(b2);
+}
+
 template <int PHYS, int N, int E_, int PREC, int NWC_ = 8>
 struct MCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
@@ -118,6 +130,11 @@ struct MCfg {
   // NACC accumulators, each summing the terms of a slice of K in FP32; the
   // slices are added in FP64 when the tile is read back
   static constexpr int S = PREC == PREC_TF32 ? 4 : 2;         // operand bytes
+  // operands split into NPARTS parts; NPROD part products per k-step:
+  // two parts -> a1 b0 + a0 b1 + a0 b0; three parts -> the six products
+  // with part indices summing to at most 2
+  static constexpr int NPARTS = PREC == PREC_BF16X6 ? 3 : 2;
+  static constexpr int NPROD = PREC == PREC_BF16X6 ? 6 : 3;
   static constexpr int T = 16 / S;                              // elements per core row
   static constexpr int KSTEP = 32 / S;                          // K per MMA
   static constexpr int KV = 3 * Np, KVA = (KV + KSTEP - 1) / KSTEP * KSTEP;
@@ -134,9 +151,8 @@ struct MCfg {
                                : NACC * NPAD <= 128 ? 128 : NACC * NPAD <= 256 ? 256 : 512;
   static constexpr int SBO_A = KAM / T * 128, SBO_BV = KVA / T * 128, SBO_BF = KFA / T * 128;
   // byte sizes
-  static constexpr int A_BYTES = M * KAM * S;                   // one part (hi or lo)
   static constexpr int BV_BYTES = NPAD * KVA * S, BF_BYTES = NPAD * KFA * S;
-  static constexpr int BIMG = 2 * (BV_BYTES + BF_BYTES);        // hi then lo
+  static constexpr int BIMG = NPARTS * (BV_BYTES + BF_BYTES);   // part 0, part 1, ...
   static constexpr int NWC = NWC_, TC = 32 * NWC, THREADS = TC + 32;
   // FP64 pipeline buffers (as in PCfg)
   static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
@@ -144,15 +160,24 @@ struct MCfg {
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
   static constexpr int S_R = NV * Np * EP;
-  static constexpr size_t SMEM = (size_t)BIMG + 2 * A_BYTES +
-                                 sizeof(double) * (2 * (size_t)S_BUF + S_R) + 1024;
+  static constexpr size_t FP64_BYTES = sizeof(double) * (2 * (size_t)S_BUF + S_R) + 1024;
+  // separate volume and lift operands let the face phase overlap the volume
+  // MMAs; used where they fit next to the rest
+  static constexpr bool SEPL =
+      (size_t)BIMG + (size_t)NPARTS * M * (KVA + KFA) * S + FP64_BYTES <= 232448;
+  static constexpr int AV_BYTES = M * (SEPL ? KVA : KAM) * S;   // one part, volume (or shared)
+  static constexpr int AF_BYTES = SEPL ? M * KFA * S : 0;       // one part, lift
+  static constexpr int SBO_AV = (SEPL ? KVA : KAM) / T * 128, SBO_AF = (SEPL ? KFA : KAM) / T * 128;
+  static constexpr int A_BYTES = AV_BYTES + AF_BYTES;           // one part
+  static constexpr size_t SMEM = (size_t)BIMG + (size_t)NPARTS * A_BYTES + FP64_BYTES;
   static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE + S_VEL);
   // instruction descriptor: F32 accumulate, A/B format, K-major A and B, N, M
   static constexpr unsigned IDESC = (1u << 4) | ((PREC == PREC_TF32 ? 2u : 1u) << 7) |
                                     ((PREC == PREC_TF32 ? 2u : 1u) << 10) |
                                     ((unsigned)(NPAD >> 3) << 17) | ((unsigned)(M >> 4) << 24);
   static_assert(NCOL <= 128, "one MMA tile covers at most 128 columns");
-  static_assert(BIMG % 16 == 0 && A_BYTES % 16 == 0, "16-byte operand images");
+  static_assert(BIMG % 16 == 0 && AV_BYTES % 16 == 0 && AF_BYTES % 16 == 0,
+                "16-byte operand images");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
   static_assert(NPAD <= 256, "MMA N limit");
   static_assert(NACC * NPAD <= 512, "tensor memory has 512 columns");
@@ -167,20 +192,40 @@ __device__ __forceinline__ int core_off(int r, int k, int sbo) {
   return (r >> 3) * sbo + (k / C::T) * 128 + (r & 7) * 16 + (k % C::T) * C::S;
 }
 
+// operand element (r, k) split into its parts; part p of the image starts
+// at A + p * C::A_BYTES, the row-group stride is sbo
 template <class C, int PREC>
-__device__ __forceinline__ void put_split(unsigned char *Ahi, unsigned char *Alo, int r, int k,
-                                          double x) {
-  const int off = core_off<C>(r, k, C::SBO_A);
+__device__ __forceinline__ void put_split(unsigned char *A, int r, int k, int sbo, double x) {
+  const int off = core_off<C>(r, k, sbo);
   if (PREC == PREC_TF32) {
     unsigned h, l;
     split_tf32(x, h, l);
-    *reinterpret_cast<unsigned *>(Ahi + off) = h;
-    *reinterpret_cast<unsigned *>(Alo + off) = l;
-  } else {
+    *reinterpret_cast<unsigned *>(A + off) = h;
+    *reinterpret_cast<unsigned *>(A + C::A_BYTES + off) = l;
+  } else if (PREC == PREC_BF16) {
     unsigned short h, l;
     split_bf16(x, h, l);
-    *reinterpret_cast<unsigned short *>(Ahi + off) = h;
-    *reinterpret_cast<unsigned short *>(Alo + off) = l;
+    *reinterpret_cast<unsigned short *>(A + off) = h;
+    *reinterpret_cast<unsigned short *>(A + C::A_BYTES + off) = l;
+  } else {
+    unsigned short p[3];
+    split_bf16x3(x, p);
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      *reinterpret_cast<unsigned short *>(A + q * C::A_BYTES + off) = p[q];
+  }
+}
+
+// part indices (a, b) of product q of a k-step
+template <class C>
+__device__ __forceinline__ void prod_parts(int q, int &pa, int &pb) {
+  if (C::NPARTS == 2) {
+    pa = q == 0 ? 1 : 0;
+    pb = q == 1 ? 1 : 0;
+  } else {
+    constexpr int A6[6] = {2, 1, 0, 1, 0, 0}, B6[6] = {0, 1, 2, 0, 1, 0};
+    pa = A6[q];
+    pb = B6[q];
   }
 }
 
@@ -191,9 +236,10 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 TC = C::TC;
   extern __shared__ __align__(16) double smem[];
+  // [operator parts][operand parts: volume (or shared) + lift][FP64 buffers]
   unsigned char *sBimg = reinterpret_cast<unsigned char *>(smem);
-  unsigned char *sAhi = sBimg + C::BIMG, *sAlo = sAhi + C::A_BYTES;
-  double *sBuf0 = reinterpret_cast<double *>(sAlo + C::A_BYTES);
+  unsigned char *sA = sBimg + C::BIMG;                       // part p at p * A_BYTES
+  double *sBuf0 = reinterpret_cast<double *>(sA + C::NPARTS * C::A_BYTES);
   double *sR = sBuf0 + 2 * C::S_BUF;
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(sR + C::S_R);
   unsigned long long *full = bars, *empty = bars + 2, *abar = bars + 4, *mbar = bars + 5;
@@ -214,9 +260,9 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
-  // zero both operand parts once: padding rows and K columns stay zero
-  for (int i = tid; i < 2 * C::A_BYTES / 16; i += C::THREADS)
-    reinterpret_cast<uint4 *>(sAhi)[i] = make_uint4(0, 0, 0, 0);
+  // zero every operand part once: padding rows and K columns stay zero
+  for (int i = tid; i < C::NPARTS * C::A_BYTES / 16; i += C::THREADS)
+    reinterpret_cast<uint4 *>(sA)[i] = make_uint4(0, 0, 0, 0);
   if (warp == 0) tmem_alloc(sTmem, C::TCOLS);
   tc_fence_before();
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -230,12 +276,43 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
   }
 
   const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
-  const unsigned aHi = smem_u32(sAhi), aLo = smem_u32(sAlo);
-  const unsigned bHiV = smem_u32(sBimg), bHiF = bHiV + C::BV_BYTES;
-  const unsigned bLoV = bHiF + C::BF_BYTES, bLoF = bLoV + C::BV_BYTES;
+  unsigned char *sAV = sA, *sAF = sA + C::AV_BYTES * (C::SEPL ? 1 : 0);
+  const unsigned aV = smem_u32(sAV), aF = smem_u32(sAF);
+  const unsigned opV = smem_u32(sBimg), opF = opV + C::BV_BYTES;
+  constexpr unsigned BPART = C::BV_BYTES + C::BF_BYTES;       // operator part stride
   unsigned long long vmax = 0ull;
   bool ok = consumer_all(mbar_wait(abar, 0), TC);
   int it = 0, mma_phase = 0;
+
+  // MMAs of one operand block (volume: k-steps [0, KSV), lift: [KSV, KST)),
+  // issued by lane 0 of warps 0..NISS-1; MMA g of the tile (product q of
+  // k-step ks) goes to accumulator g % NACC, the first NACC initialise them
+  auto issue = [&](unsigned abase, int sbo_a, unsigned bbase, int sbo_b, int ks0, int nks) {
+    if (lane == 0 && warp < C::NISS) {
+      tc_fence_after();
+      unsigned long long ad[C::NPARTS], bd[C::NPARTS];
+#pragma unroll
+      for (int q = 0; q < C::NPARTS; q++) {
+        ad[q] = smem_desc(abase + q * C::A_BYTES, 128, sbo_a);
+        bd[q] = smem_desc(bbase + q * BPART, 128, sbo_b);
+      }
+#pragma unroll 1
+      for (int ks = 0; ks < nks; ks++) {
+#pragma unroll
+        for (int q = 0; q < C::NPROD; q++) {
+          const int g = C::NPROD * (ks0 + ks) + q, j = g % C::NACC;
+          if (j % C::NISS != warp) continue;
+          int pa, pb;
+          prod_parts<C>(q, pa, pb);
+          // a k-step advances the start address by 256 bytes (16 in the field)
+          tc_mma<PREC>(tmem + j * C::NPAD, ad[pa] + 16ull * ks, bd[pb] + 16ull * ks, C::IDESC,
+                       g >= C::NACC);
+        }
+      }
+      tc_commit(mbar);
+    }
+  };
+
   for (int t = blockIdx.x; ok && t < ntiles; t += gridDim.x, it++) {
     const int b = it & 1;
     if (!consumer_all(mbar_wait(&full[b], (it >> 1) & 1), TC)) {
@@ -262,55 +339,35 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const int m = v * E + e;
-          put_split<C, PREC>(sAhi, sAlo, m, i, rx * F[v] + ry * Gf[v] + rz * W[v]);
-          put_split<C, PREC>(sAhi, sAlo, m, Np + i, sx * F[v] + sy * Gf[v] + sz * W[v]);
-          put_split<C, PREC>(sAhi, sAlo, m, 2 * Np + i, tx * F[v] + ty * Gf[v] + tz * W[v]);
+          put_split<C, PREC>(sAV, m, i, C::SBO_AV, rx * F[v] + ry * Gf[v] + rz * W[v]);
+          put_split<C, PREC>(sAV, m, Np + i, C::SBO_AV, sx * F[v] + sy * Gf[v] + sz * W[v]);
+          put_split<C, PREC>(sAV, m, 2 * Np + i, C::SBO_AV, tx * F[v] + ty * Gf[v] + tz * W[v]);
         }
       } else {
         const double uu = bU[e * Np + i];
         const double F = bV[e * Np + i] * uu, Gf = bV[E * Np + e * Np + i] * uu,
                      W = bV[2 * E * Np + e * Np + i] * uu;
-        put_split<C, PREC>(sAhi, sAlo, e, i, rx * F + ry * Gf + rz * W);
-        put_split<C, PREC>(sAhi, sAlo, e, Np + i, sx * F + sy * Gf + sz * W);
-        put_split<C, PREC>(sAhi, sAlo, e, 2 * Np + i, tx * F + ty * Gf + tz * W);
+        put_split<C, PREC>(sAV, e, i, C::SBO_AV, rx * F + ry * Gf + rz * W);
+        put_split<C, PREC>(sAV, e, Np + i, C::SBO_AV, sx * F + sy * Gf + sz * W);
+        put_split<C, PREC>(sAV, e, 2 * Np + i, C::SBO_AV, tx * F + ty * Gf + tz * W);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     consumer_sync(TC);
-    if (lane == 0 && warp < C::NISS) {
-      tc_fence_after();
-      // descriptors of k-step 0; a k-step advances the start address by 256
-      // bytes (16 in the descriptor's address field)
-      const unsigned long long ah0 = smem_desc(aHi, 128, C::SBO_A);
-      const unsigned long long al0 = smem_desc(aLo, 128, C::SBO_A);
-      const unsigned long long bh0 = smem_desc(bHiV, 128, C::SBO_BV);
-      const unsigned long long bl0 = smem_desc(bLoV, 128, C::SBO_BV);
-#pragma unroll
-      for (int ks = 0; ks < C::KSV; ks++) {
-        // MMA g of the tile (pass p of k-step ks) goes to accumulator
-        // g % NACC, issued by that accumulator's issuer; the first NACC MMAs
-        // initialise the accumulators
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-          const int g = 3 * ks + p, j = g % C::NACC;
-          if (j % C::NISS != warp) continue;
-          const unsigned long long ad = (p == 0 ? al0 : ah0) + 16ull * ks;
-          const unsigned long long bd = (p == 1 ? bl0 : bh0) + 16ull * ks;
-          tc_mma<PREC>(tmem + j * C::NPAD, ad, bd, C::IDESC, g >= C::NACC);
-        }
+    issue(aV, C::SBO_AV, opV, C::SBO_BV, 0, C::KSV);
+    if (!C::SEPL) {
+      // the volume MMAs must have read the shared operand before it is reused
+      if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
+        ok = false;
+        break;
       }
-      tc_commit(mbar);
+      mma_phase ^= 1;
+      tc_fence_after();
     }
-    // the volume MMAs must have read the operand before it is overwritten
-    if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
-      ok = false;
-      break;
-    }
-    mma_phase ^= 1;
-    tc_fence_after();
 
-    // 3. face fluxes -> operand rows m, k = fj
+    // 3. face fluxes -> lift operand rows m, k = fj (overlaps the volume MMAs
+    //    when the lift operand has its own buffer)
     for (int itm = tid; itm < E * NFF; itm += TC) {
       const int fj = itm / E, e = itm - fj * E, f = fj / Nfp;
       const int nodeM = sFm[fj];
@@ -328,7 +385,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];
-          put_split<C, PREC>(sAhi, sAlo, v * E + e, fj, (nd - tau * (qb[v] - qm[v])) * fs);
+          put_split<C, PREC>(sAF, v * E + e, fj, C::SBO_AF, (nd - tau * (qb[v] - qm[v])) * fs);
         }
       } else {
         const double um = bU[e * Np + nodeM];
@@ -336,31 +393,25 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
         const double F = bV[e * Np + nodeM] * ub, Gf = bV[E * Np + e * Np + nodeM] * ub,
                      W = bV[2 * E * Np + e * Np + nodeM] * ub;
         const double nd = nx * F + ny * Gf + nz * W;
-        put_split<C, PREC>(sAhi, sAlo, e, fj, (nd - tau * (ub - um)) * fs);
+        put_split<C, PREC>(sAF, e, fj, C::SBO_AF, (nd - tau * (ub - um)) * fs);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     consumer_sync(TC);
-    if (lane == 0 && warp < C::NISS) {
-      tc_fence_after();
-      const unsigned long long ah0 = smem_desc(aHi, 128, C::SBO_A);
-      const unsigned long long al0 = smem_desc(aLo, 128, C::SBO_A);
-      const unsigned long long bh0 = smem_desc(bHiF, 128, C::SBO_BF);
-      const unsigned long long bl0 = smem_desc(bLoF, 128, C::SBO_BF);
-#pragma unroll
-      for (int ks = 0; ks < C::KSF; ks++) {
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-          const int g = 3 * (C::KSV + ks) + p, j = g % C::NACC;   // MMA index within the tile
-          if (j % C::NISS != warp) continue;
-          const unsigned long long ad = (p == 0 ? al0 : ah0) + 16ull * ks;
-          const unsigned long long bd = (p == 1 ? bl0 : bh0) + 16ull * ks;
-          tc_mma<PREC>(tmem + j * C::NPAD, ad, bd, C::IDESC, g >= C::NACC);
-        }
+    if (C::SEPL) {
+      // the volume commits' phase is waited for before the next commit: a
+      // parity wait cannot tell a phase from the one two phases later, so
+      // two phases of this barrier must never complete unobserved
+      if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
+        ok = false;
+        break;
       }
-      tc_commit(mbar);
+      mma_phase ^= 1;
+      tc_fence_after();
     }
+    issue(aF, C::SBO_AF, opF, C::SBO_BF, C::KSV, C::KSF);
+    // a commit arrives once all earlier MMAs of its thread are done
     if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
       ok = false;
       break;
@@ -399,6 +450,9 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
     }
     tc_fence_before();
     consumer_sync(TC);
+    // 6. LSERK update with coalesced stores; the new state goes back to
+    //    shared memory only when the fused wave-speed pass reads it
+    const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
     for (int v = 0; v < NV; v++) {
       const long base = v * vs + e0 * Np;
       for (int g = tid; g < ne * Np; g += TC) {
@@ -411,7 +465,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
           const double un = bU[v * E * Np + g] + a.rkb * kn;
           a.kreg[base + g] = kn;
           a.u_out[base + g] = un;
-          bU[v * E * Np + g] = un;
+          if (keep_u) bU[v * E * Np + g] = un;
         }
       }
     }

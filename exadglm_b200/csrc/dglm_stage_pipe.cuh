@@ -410,6 +410,8 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREA
       }
     }
     consumer_sync(TC);
+    // the new state goes back to shared memory only for the fused wave speed
+    const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
     for (int v = 0; v < NV; v++) {
       const long base = v * vs + e0 * Np;
       for (int g = tid; g < ne * Np; g += TC) {
@@ -422,7 +424,7 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREA
           const double un = bU[v * E * Np + g] + a.rkb * kn;
           a.kreg[base + g] = kn;
           a.u_out[base + g] = un;
-          bU[v * E * Np + g] = un;
+          if (keep_u) bU[v * E * Np + g] = un;
         }
       }
     }

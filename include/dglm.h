@@ -62,7 +62,8 @@ typedef enum { DGLM_ADVECTION = 0, DGLM_EULER = 1 } dglm_physics;
 typedef enum {
     DGLM_PREC_FP64 = 0,        /* plain method: FP64 throughout */
     DGLM_PREC_TF32X3 = 1,      /* 3-pass TF32 on tcgen05, FP32 accumulate */
-    DGLM_PREC_BF16X3 = 2       /* split-BF16 (3 products) on tcgen05, FP32 accumulate */
+    DGLM_PREC_BF16X3 = 2,      /* split-BF16, 2 parts, 3 products, FP32 accumulate */
+    DGLM_PREC_BF16X6 = 3       /* split-BF16, 3 parts (24 bits), 6 products, FP32 accumulate */
 } dglm_precision;
 
 /* Solver description: the reference's compile-time common.h parameters
@@ -122,7 +123,10 @@ dglm_status dglm_step_fixed_dt(dglm_handle *h, int nsteps, double dt);
  * handle's current tau, without the per-step dt/tau work (for timing the
  * stage kernel on its own).  Asynchronous. */
 dglm_status dglm_stage(dglm_handle *h, int stage, double dt);
-/* Synchronises the stream and reports a device-side non-finite flag. */
+/* Synchronises the stream and reports device-side flags: DGLM_ERR_NONFINITE
+ * for a non-finite wave speed, dt or state, DGLM_ERR_CUDA when a bounded
+ * wait inside a pipelined stage kernel expired (the step's results are then
+ * invalid).  The flags are cleared by dglm_set_state. */
 dglm_status dglm_sync(dglm_handle *h);
 /* Time, last dt and step counter (synchronises). */
 dglm_status dglm_get_time(dglm_handle *h, double *t, double *dt, int *tstep);
