@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint", "batch"], default=None,
+    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint", "batch", "precision"],
+                    default=None,
                     help="run one section alone (profiling); prints that section's object")
     ap.add_argument("--accuracy-steps", type=int, default=200,
                     help="steps of the mixed-vs-FP64 relative L2 comparison")
@@ -60,6 +61,8 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=500)
     ap.add_argument("--adjoint-every", type=int, default=50, help="checkpoint spacing")
     ap.add_argument("--batch-count", type=int, default=256, help="instances of the batch workload")
+    ap.add_argument("--precision-n", type=int, default=48,
+                    help="hexahedra per axis of the N=6 precision study (K = 6 n^3)")
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--batch-sequential", type=int, default=256,
                     help="instances also run one by one through single-mesh handles")
@@ -415,6 +418,46 @@ def batch_section(a, stream):
     return out
 
 
+def precision_section(a, stream):
+    """Precision study: Euler N=6 on n^3 x 6 tets (default 48 -> K = 663,552),
+    the headline initial state, --accuracy-steps steps of the FP64 path and
+    of each mixed mode from the same state; relative L2 against FP64 per field,
+    and ms per step of each."""
+    import numpy as np
+    from exadglm_b200 import problem as P
+    from exadglm_b200.capi import Solver, variants
+    p6 = P.euler_sine(n=a.precision_n, N=6, cfl=0.4)
+    S = a.accuracy_steps
+    out = {"workload": f"euler_sine N=6 K={p6.K} (n={a.precision_n}) CFL 0.4, {S} steps"}
+    ref = None
+    for prec in ("fp64", "tf32x3", "bf16x6", "bf16x3"):
+        s = Solver(p6, precision=prec)
+        s.set_stream(stream.cuda_stream)
+        s.step(2)
+        s.sync()
+        s.set_state(p6.u0)
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        s.step(S)
+        e1.record(stream)
+        e1.synchronize()
+        s.sync()
+        u = s.get_state()
+        ms = e0.elapsed_time(e1) / S
+        row = {"ms_per_step": ms, "kernel": variants("euler", 6)[s.variant()],
+               "value": dof_stages_per_step(p6) / (ms * 1e-3), "unit": UNIT}
+        if ref is None:
+            ref = u
+        else:
+            row["rel_l2_vs_fp64"] = float(np.linalg.norm(u - ref) / np.linalg.norm(ref))
+            row["rel_l2_per_field"] = [float(np.linalg.norm(u[v] - ref[v]) / np.linalg.norm(ref[v]))
+                                       for v in range(p6.nvar)]
+            row["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / ms
+        out[prec] = row
+        s.close()
+    return out
+
+
 def main():
     a = parse()
     if a.impl == "reference":
@@ -448,9 +491,11 @@ def main():
 
     p = build_problem(a)
     stream = torch.cuda.Stream()
-    if a.only in ("mixed", "adjoint", "batch"):
+    if a.only in ("mixed", "adjoint", "batch", "precision"):
         res = (mixed_section(a, p, stream, float("nan")) if a.only == "mixed"
-               else adjoint_section(a, stream) if a.only == "adjoint" else batch_section(a, stream))
+               else adjoint_section(a, stream) if a.only == "adjoint"
+               else precision_section(a, stream) if a.only == "precision"
+               else batch_section(a, stream))
         if rank == 0:
             print(json.dumps({a.only: res}), flush=True)
         if dist is not None:

@@ -147,12 +147,9 @@ def ptr_table(ptrs):
 
 def variant_precision(desc):
     """Precision mode of a variant from its description."""
-    if desc.startswith("tcgen05-tf32x3"):
-        return "tf32x3"
-    if desc.startswith("tcgen05-bf16x3"):
-        return "bf16x3"
-    if desc.startswith("tcgen05-bf16x6"):
-        return "bf16x6"
+    for prec in ("tf32x3", "bf16x3", "bf16x6"):
+        if desc.startswith(("tcgen05-" + prec, "mma16-" + prec, "pipe-mma16-" + prec)):
+            return prec
     return "fp64"
 
 

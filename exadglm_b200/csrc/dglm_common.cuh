@@ -101,7 +101,7 @@ dglm_status set_error(dglm_status s, const std::string &msg);
 dglm_status cuda_check(cudaError_t e, const char *what);
 
 // contraction engines of the fused stage kernel
-enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3 };
+enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3, MODE_MMA16 = 4 };
 
 // One compiled tile shape of the fused stage kernel.
 struct StageVariantInfo {
@@ -120,6 +120,8 @@ struct StageVariantInfo {
   int kva, kfa;  // MIXED: volume / lift K extents of the operand images
   int bimg;      // MIXED: bytes of the operator image (hi then lo)
   int groups;    // PIPE: consumer groups taking alternate tiles (1 or 2)
+  int kstep;     // MMA16: K per mma.sync (8 TF32, 16 BF16)
+  int persistent;  // 1: one CTA per SM walking the tiles (TMA-fed pipeline)
 };
 
 // fused FP64 stage launcher (dglm_stage_fp64.cu)

@@ -89,6 +89,10 @@ namespace {
 size_t op_doubles(const StageVariantInfo &v, int Np, int NFF) {
   if (v.mode == MODE_SIMT) return (size_t)(3 * Np + NFF) * v.IP;
   if (v.mode == MODE_MIXED) return ((size_t)v.bimg + 7) / 8;
+  if (v.mode == MODE_MMA16) {
+    const int parts = v.prec == DGLM_PREC_BF16X6 ? 3 : 2;
+    return (size_t)(v.KVP / v.kstep + v.KFP / v.kstep) * v.MT * parts * 64;   // 512 B each
+  }
   return (size_t)(v.KVP / 4 + v.KFP / 4) * v.MT * 32;
 }
 
@@ -167,9 +171,70 @@ std::vector<unsigned char> mixed_image(const dglm_handle *h, const StageVariantI
 //   DMMA: m8n8k4 A fragments, [kstep][mtile][lane] with row = 8*mtile +
 //         lane/4 and column 4*kstep + lane%4 inside the volume block
 //         (ksteps [0, KVP/4)) or the lift block (ksteps [KVP/4, ...)).
+// Fragments of the split-precision mma.sync engine: per (k-step, m-tile,
+// part) 32 lanes x 4 32-bit registers in the m16n8k8 TF32 / m16n8k16 BF16 A
+// layout (see contract_m16), parts split with the exact FP64 residual.
+std::vector<uint32_t> m16_fragments(const dglm_handle *h, const StageVariantInfo &v) {
+  const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
+  const bool tf = v.prec == DGLM_PREC_TF32X3;
+  const int parts = v.prec == DGLM_PREC_BF16X6 ? 3 : 2;
+  const int ksv = v.KVP / v.kstep, ksf = v.KFP / v.kstep;
+  std::vector<uint32_t> out((size_t)(ksv + ksf) * v.MT * parts * 128, 0u);
+  // operator entry for row r and k-column kk of k-step ks (0 outside)
+  auto A = [&](int r, int ks, int kk) -> double {
+    if (r >= Np) return 0.0;
+    if (ks < ksv) {
+      const int k = ks * v.kstep + kk;
+      return k < KV ? h->Ahost[(size_t)r * KA + k] : 0.0;
+    }
+    const int k = (ks - ksv) * v.kstep + kk;
+    return k < NFF ? h->Ahost[(size_t)r * KA + KV + k] : 0.0;
+  };
+  auto parts_of = [&](double x, uint32_t *p) {
+    double rest = x;
+    for (int q = 0; q < parts; q++) {
+      if (tf) {
+        p[q] = tf32_rna((float)rest);
+        rest -= (double)f32_of(p[q]);
+      } else {
+        const uint16_t b = bf16_rne((float)rest);
+        p[q] = b;
+        rest -= (double)f32_of((uint32_t)b << 16);
+      }
+    }
+  };
+  for (int ks = 0; ks < ksv + ksf; ks++)
+    for (int mt = 0; mt < v.MT; mt++)
+      for (int lane = 0; lane < 32; lane++) {
+        const int g = lane >> 2, t = lane & 3, r0 = mt * 16 + g;
+        uint32_t reg[4][3] = {};
+        if (tf) {
+          const int rr[4] = {r0, r0 + 8, r0, r0 + 8}, kk[4] = {t, t, t + 4, t + 4};
+          for (int c = 0; c < 4; c++) parts_of(A(rr[c], ks, kk[c]), reg[c]);
+        } else {
+          const int rr[4] = {r0, r0 + 8, r0, r0 + 8}, kk[4] = {2 * t, 2 * t, 2 * t + 8, 2 * t + 8};
+          for (int c = 0; c < 4; c++) {
+            uint32_t lo[3], hi[3];
+            parts_of(A(rr[c], ks, kk[c]), lo);
+            parts_of(A(rr[c], ks, kk[c] + 1), hi);
+            for (int q = 0; q < parts; q++) reg[c][q] = lo[q] | (hi[q] << 16);
+          }
+        }
+        for (int q = 0; q < parts; q++)
+          for (int c = 0; c < 4; c++)
+            out[((((size_t)ks * v.MT + mt) * parts + q) * 32 + lane) * 4 + c] = reg[c][q];
+      }
+  return out;
+}
+
 dglm_status upload_operator_layout(dglm_handle *h) {
   const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
   const StageVariantInfo &v = h->vinfo;
+  if (v.mode == MODE_MMA16) {
+    std::vector<uint32_t> fr = m16_fragments(h, v);
+    return cuda_check(cudaMemcpy(h->AT, fr.data(), fr.size() * 4, cudaMemcpyHostToDevice),
+                      "operator upload");
+  }
   if (v.mode == MODE_MIXED) {
     std::vector<unsigned char> img = mixed_image(h, v);
     return cuda_check(cudaMemcpy(h->AT, img.data(), img.size(), cudaMemcpyHostToDevice),
@@ -675,6 +740,12 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
   if (v.mode == MODE_SIMT)
     snprintf(buf, len, "simt E=%d R=%d CPT=%d threads=%d smem=%zu", v.E, v.R, v.CPT, v.threads,
              v.smem);
+  else if (v.mode == MODE_MMA16)
+    snprintf(buf, len, "%smma16-%s E=%d WN=%d WM=%d threads=%d smem=%zu",
+             v.persistent ? "pipe-" : "",
+             v.prec == DGLM_PREC_TF32X3 ? "tf32x3" : v.prec == DGLM_PREC_BF16X6 ? "bf16x6"
+                                                                                : "bf16x3",
+             v.E, v.CPT, v.WM, v.threads, v.smem);
   else if (v.mode == MODE_MIXED)
     snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
              v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"

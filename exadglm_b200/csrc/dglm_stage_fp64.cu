@@ -33,6 +33,7 @@
 //
 // Shared layouts put the element index fastest ([..][e], row stride E+1)
 // so that every phase's per-lane accesses are consecutive or odd-strided.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -61,7 +62,7 @@ __device__ __forceinline__ void euler_flux_fast(double g, const double q[5], dou
 // configuration
 // ---------------------------------------------------------------------------
 
-template <int PHYS, int N, int MODE, int E_, int R_, int CPT_, int WM_>
+template <int PHYS, int N, int MODE, int E_, int R_, int CPT_, int WM_, int PR_ = 0>
 struct Cfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -78,9 +79,22 @@ struct Cfg {
   static constexpr int WN = CPT_;
   static constexpr int MGROUPS = (MT + WM - 1) / WM;
   static constexpr int WARPS_D = MODE == MODE_DMMA ? MGROUPS * (NT / WN) : 0;
-  static constexpr int THREADS = MODE == MODE_SIMT ? CG * G : 32 * WARPS_D;
-  static constexpr int KV = 3 * Np, KVP = (KV + 3) / 4 * 4;    // volume k (padded to 4)
-  static constexpr int KF = NFF, KFP = (KF + 3) / 4 * 4;
+  // MMA16: split-precision mma.sync, m16n8k8 (TF32, PR_ = 2) or m16n8k16
+  // (BF16: two parts, PR_ = 1; three parts, PR_ = 3)
+  static constexpr bool M16 = MODE == MODE_MMA16;
+  static constexpr int KSTEP16 = PR_ == 2 ? 8 : 16;
+  static constexpr int NPARTS16 = PR_ == 3 ? 3 : 2, NPROD16 = PR_ == 3 ? 6 : 3;
+  static constexpr int MT16 = (Np + 15) / 16;
+  static constexpr int WM16 = WM_ > MT16 ? MT16 : WM_;
+  static constexpr int MG16 = (MT16 + WM16 - 1) / WM16;
+  static constexpr int WARPS_16 = M16 ? MG16 * (NT / WN) : 0;
+  static constexpr int THREADS =
+      MODE == MODE_SIMT ? CG * G : 32 * (M16 ? WARPS_16 : WARPS_D);
+  static constexpr int KPAD = M16 ? KSTEP16 : 4;
+  static constexpr int KV = 3 * Np, KVP = (KV + KPAD - 1) / KPAD * KPAD;   // volume k (padded)
+  static constexpr int KF = NFF, KFP = (KF + KPAD - 1) / KPAD * KPAD;
+  static constexpr int KSV16 = KVP / KSTEP16, KSF16 = KFP / KSTEP16, KST16 = KSV16 + KSF16;
+  static constexpr int SL16 = (KST16 + 7) / 8;   // k-steps per FP32 slice (8 slices)
   static constexpr int IP = MODE == MODE_SIMT ? G * R : 8 * MT;     // padded rows
   static constexpr int BLD = MODE == MODE_SIMT ? NCOL : NCOL + 4;   // B row stride
   static constexpr int BROWS = KVP > KFP ? KVP : KFP;
@@ -157,19 +171,161 @@ __device__ __forceinline__ void contract_dmma(const double *__restrict__ Afrag, 
   }
 }
 
+// Split-precision mma.sync (legacy tensor-core path, for orders whose tcgen05
+// operand images do not fit in shared memory).  A = the operator, its parts
+// pre-split on the host into fragments [kstep][mtile][part][lane] (4 x 32
+// bits per lane, one coalesced 512-byte load); B = the FP64 fluxes in
+// shared memory, split in registers; NPROD16 part products per k-step into
+// FP32 accumulators that are folded into FP64 every SL16 k-steps.
+//   m16n8k8 TF32:  a0=A[g][t] a1=A[g+8][t] a2=A[g][t+4] a3=A[g+8][t+4],
+//                  b0=B[t][g] b1=B[t+4][g]
+//   m16n8k16 BF16: a0=A[g][2t..2t+1] a1=A[g+8][2t..] a2=A[g][2t+8..] a3=A[g+8][2t+8..],
+//                  b0=B[2t..2t+1][g] b1=B[2t+8..2t+9][g]  (low half = lower k)
+//   C: c0=C[g][2t] c1=C[g][2t+1] c2=C[g+8][2t] c3=C[g+8][2t+1]
+// with g = lane/4, t = lane%4.
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const unsigned (&a)[4],
+                                                const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ void mma_bf16_16x8x16(float (&d)[4], const unsigned (&a)[4],
+                                                 const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// parts of an FP64 value: TF32 (hi, lo) or BF16 (2 or 3 parts) as raw bits
+template <int PR>
+__device__ __forceinline__ void split_parts(double x, unsigned (&p)[3]) {
+  const float f = (float)x;
+  if (PR == 2) {
+    unsigned h, l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
+    const float r = f - __uint_as_float(h);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
+    p[0] = h;
+    p[1] = l;
+    p[2] = 0;
+  } else {
+    float r = f;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const unsigned short b = __bfloat16_as_ushort(__float2bfloat16_rn(r));
+      p[q] = b;
+      r -= __uint_as_float((unsigned)b << 16);
+    }
+  }
+}
+
+template <class C>
+__device__ __forceinline__ void prod16(int q, int &pa, int &pb) {
+  if (C::NPARTS16 == 2) {
+    pa = q == 0 ? 1 : 0;
+    pb = q == 1 ? 1 : 0;
+  } else {
+    constexpr int A6[6] = {2, 1, 0, 1, 0, 0}, B6[6] = {0, 1, 2, 0, 1, 0};
+    pa = A6[q];
+    pb = B6[q];
+  }
+}
+
+template <class C, int PR>
+__device__ __forceinline__ void contract_m16(const uint4 *__restrict__ A16, int ks0, int nks,
+                                             const double *sB,
+                                             float (&acc)[C::WM16][C::WN][4],
+                                             double (&tot)[C::WM16][C::WN][4], int warp,
+                                             int lane) {
+  constexpr int NP = C::NPARTS16, BLD = C::BLD;
+  const int mg = warp % C::MG16, ng = warp / C::MG16;
+  const int m0 = mg * C::WM16, n0 = ng * C::WN;
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll 1
+  for (int ks = 0; ks < nks; ks++) {
+    const int kg = ks0 + ks;
+    unsigned bp[C::WN][3][2];
+#pragma unroll
+    for (int j = 0; j < C::WN; j++) {
+      const double *Bc = sB + (n0 + j) * 8 + g + ks * C::KSTEP16 * BLD;
+      if (PR == 2) {
+        unsigned p0[3], p1[3];
+        split_parts<PR>(Bc[t * BLD], p0);
+        split_parts<PR>(Bc[(t + 4) * BLD], p1);
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+          bp[j][q][0] = p0[q];
+          bp[j][q][1] = p1[q];
+        }
+      } else {
+        unsigned x0[3], x1[3], x2[3], x3[3];
+        split_parts<PR>(Bc[(2 * t) * BLD], x0);
+        split_parts<PR>(Bc[(2 * t + 1) * BLD], x1);
+        split_parts<PR>(Bc[(2 * t + 8) * BLD], x2);
+        split_parts<PR>(Bc[(2 * t + 9) * BLD], x3);
+#pragma unroll
+        for (int q = 0; q < NP; q++) {
+          bp[j][q][0] = x0[q] | (x1[q] << 16);
+          bp[j][q][1] = x2[q] | (x3[q] << 16);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < C::WM16; i++) {
+      if (m0 + i >= C::MT16) continue;
+      unsigned ap[3][4];
+#pragma unroll
+      for (int q = 0; q < NP; q++) {
+        const uint4 v = __ldg(A16 + (((long)kg * C::MT16 + m0 + i) * NP + q) * 32 + lane);
+        ap[q][0] = v.x;
+        ap[q][1] = v.y;
+        ap[q][2] = v.z;
+        ap[q][3] = v.w;
+      }
+#pragma unroll
+      for (int j = 0; j < C::WN; j++)
+#pragma unroll
+        for (int q = 0; q < C::NPROD16; q++) {
+          int pa, pb;
+          prod16<C>(q, pa, pb);
+          if (PR == 2)
+            mma_tf32_16x8x8(acc[i][j], ap[pa], bp[j][pb]);
+          else
+            mma_bf16_16x8x16(acc[i][j], ap[pa], bp[j][pb]);
+        }
+    }
+    if ((kg + 1) % C::SL16 == 0 || kg + 1 == C::KST16) {
+#pragma unroll
+      for (int i = 0; i < C::WM16; i++)
+#pragma unroll
+        for (int j = 0; j < C::WN; j++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            tot[i][j][c] += (double)acc[i][j][c];
+            acc[i][j][c] = 0.f;
+          }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // the stage kernel
 // ---------------------------------------------------------------------------
 
-template <int PHYS, int N, int MODE, int E_, int R_, int CPT_, int WM_>
-__global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>::THREADS)
+template <int PHYS, int N, int MODE, int E_, int R_, int CPT_, int WM_, int PR_>
+__global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::THREADS)
     stage_fp64_kernel(const StageArgs a) {
-  using C = Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>;
+  using C = Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 BLD = C::BLD, T = C::THREADS;
-  constexpr bool SIMT = MODE == MODE_SIMT;
+  constexpr bool SIMT = MODE == MODE_SIMT, M16 = MODE == MODE_MMA16;
   constexpr int AR = SIMT ? C::R : 1, AC = SIMT ? C::CPT : 1;     // SIMT accumulators
-  constexpr int DM = SIMT ? 1 : C::WM, DN = SIMT ? 1 : C::WN;     // DMMA accumulators
+  constexpr int DM = (SIMT || M16) ? 1 : C::WM, DN = (SIMT || M16) ? 1 : C::WN;   // DMMA
+  constexpr int QM = M16 ? C::WM16 : 1, QN = M16 ? C::WN : 1;     // MMA16 accumulators
   extern __shared__ __align__(16) double smem[];
   double *sU = smem;                    // [v][i][EP]
   double *sB = sU + C::S_U;             // [k][BLD], col = v*E + e
@@ -257,8 +413,22 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>::THREADS
   for (int i = 0; i < DM; i++)
 #pragma unroll
     for (int j = 0; j < DN; j++) accD[i][j][0] = accD[i][j][1] = 0.0;
+  float acc16[QM][QN][4];
+  double tot16[QM][QN][4];
+#pragma unroll
+  for (int i = 0; i < QM; i++)
+#pragma unroll
+    for (int j = 0; j < QN; j++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        acc16[i][j][c] = 0.f;
+        tot16[i][j][c] = 0.0;
+      }
   if constexpr (SIMT) {
     contract_simt<C, C::KV>(a.AT, 0, sB, accS, tid);
+  } else if constexpr (M16) {
+    contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), 0, C::KSV16, sB, acc16, tot16,
+                         warp, lane);
   } else {
     if (warp < C::WARPS_D) contract_dmma<C, C::KVP / 4>(a.AT, 0, sB, accD, warp, lane);
   }
@@ -308,6 +478,9 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>::THREADS
   // 4. lift contraction (A columns [3Np, 3Np+NFF) hold -LIFT)
   if constexpr (SIMT) {
     contract_simt<C, C::KF>(a.AT, C::KV, sB, accS, tid);
+  } else if constexpr (M16) {
+    contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), C::KSV16, C::KSF16, sB, acc16,
+                         tot16, warp, lane);
   } else {
     if (warp < C::WARPS_D) contract_dmma<C, C::KFP / 4>(a.AT, C::KVP / 4, sB, accD, warp, lane);
   }
@@ -327,6 +500,22 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_>::THREADS
           sR[(v * Np + i) * EP + e] = accS[r][j];
         }
       }
+    }
+  } else if constexpr (M16) {
+    const int mg = warp % C::MG16, ng = warp / C::MG16;
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int ii = 0; ii < QM; ii++) {
+      if (mg * C::WM16 + ii >= C::MT16) continue;
+#pragma unroll
+      for (int jj = 0; jj < QN; jj++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const int i = (mg * C::WM16 + ii) * 16 + g + (c >= 2 ? 8 : 0);
+          const int col = (ng * C::WN + jj) * 8 + 2 * t + (c & 1);
+          const int v = col / E, e = col - v * E;
+          if (i < Np) sR[(v * Np + i) * EP + e] = tot16[ii][jj][c];
+        }
     }
   } else {
     if (warp < C::WARPS_D) {
@@ -520,10 +709,10 @@ struct Variant {
   cudaError_t (*launch)(const StageArgs &, cudaStream_t);
 };
 
-template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM>
+template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
 static cudaError_t launch_v(const StageArgs &a, cudaStream_t s) {
-  using C = Cfg<PHYS, N, MODE, E, R, CPT, WM>;
-  auto k = stage_fp64_kernel<PHYS, N, MODE, E, R, CPT, WM>;
+  using C = Cfg<PHYS, N, MODE, E, R, CPT, WM, PR>;
+  auto k = stage_fp64_kernel<PHYS, N, MODE, E, R, CPT, WM, PR>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -539,10 +728,10 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
-template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG>
+template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG, int PR>
 static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG>;
-  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR>;
+  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -552,23 +741,28 @@ static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1>
+template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1, int PR = 0>
 static Variant make_pipe() {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR>;
   StageVariantInfo i{};
-  i.mode = MODE_PIPE;
+  i.mode = PR ? MODE_MMA16 : MODE_PIPE;
   i.E = E;
   i.R = 8;
   i.CPT = WN;
-  i.WM = C::WM;
+  i.WM = PR ? C::WM16 : C::WM;
   i.IP = 8 * C::MT;
-  i.MT = C::MT;
+  i.MT = PR ? C::MT16 : C::MT;
   i.KVP = C::KVP;
   i.KFP = C::KFP;
   i.threads = C::THREADS;
   i.smem = C::SMEM;
   i.groups = NG;
-  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG>};
+  i.persistent = 1;
+  if (PR) {
+    i.prec = PR == 2 ? DGLM_PREC_TF32X3 : PR == 3 ? DGLM_PREC_BF16X6 : DGLM_PREC_BF16X3;
+    i.kstep = C::KSTEP16;
+  }
+  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR>};
 }
 
 template <int PHYS, int N, int E, int PREC, int NWC>
@@ -602,22 +796,26 @@ static Variant make_mixed() {
   return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC>};
 }
 
-template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM>
+template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
 static Variant make_v() {
-  using C = Cfg<PHYS, N, MODE, E, R, CPT, WM>;
+  using C = Cfg<PHYS, N, MODE, E, R, CPT, WM, PR>;
   StageVariantInfo i{};
   i.mode = MODE;
   i.E = E;
   i.R = MODE == MODE_SIMT ? R : 8;
   i.CPT = CPT;
-  i.WM = C::WM;
+  i.WM = MODE == MODE_MMA16 ? C::WM16 : C::WM;
   i.IP = C::IP;
-  i.MT = C::MT;
+  i.MT = MODE == MODE_MMA16 ? C::MT16 : C::MT;
   i.KVP = C::KVP;
   i.KFP = C::KFP;
   i.threads = C::THREADS;
   i.smem = C::SMEM;
-  return Variant{i, &launch_v<PHYS, N, MODE, E, R, CPT, WM>};
+  if (MODE == MODE_MMA16) {
+    i.prec = PR == 2 ? DGLM_PREC_TF32X3 : PR == 3 ? DGLM_PREC_BF16X6 : DGLM_PREC_BF16X3;
+    i.kstep = C::KSTEP16;
+  }
+  return Variant{i, &launch_v<PHYS, N, MODE, E, R, CPT, WM, PR>};
 }
 
 // Candidate tile shapes per (physics, N); entry 0 is the default, the others
@@ -634,6 +832,9 @@ static const std::vector<Variant> &variants();
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define V_TF32W(P, NN, E, W) make_mixed<P, NN, E, PREC_TF32, W>()
 #define V_BF16X6(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16X6, W>()
+// split-precision mma.sync (legacy tensor cores): E, WN n-tiles, WM m-tiles
+#define V_M16(P, NN, E, WN, WM, PR) make_v<P, NN, MODE_MMA16, E, 1, WN, WM, PR>()
+#define V_PM16(P, NN, E, WN, WM, PR) make_pipe<P, NN, E, WN, WM, false, 1, PR>()
 #define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
@@ -652,10 +853,14 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPE(EUL, 4, 8, 1, 5, false), V_PIPE(EUL, 4, 8, 1, 3, true),
               V_PIPE2(EUL, 4, 8, 1, 5, true), V_PIPE2(EUL, 4, 8, 1, 3, true),
               V_TF32W(EUL, 4, 8, 16), V_BF16W(EUL, 4, 8, 16), V_BF16X6(EUL, 4, 8, 16),
-              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_BF16X6(EUL, 4, 8, 8))
+              V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_BF16X6(EUL, 4, 8, 8),
+              V_M16(EUL, 4, 8, 1, 3, 2), V_M16(EUL, 4, 8, 1, 1, 1), V_M16(EUL, 4, 8, 1, 1, 3),
+              V_PM16(EUL, 4, 8, 1, 3, 1))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
-              V_SIMT(EUL, 5, 8, 7, 5))
-DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5))
+              V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
+              V_M16(EUL, 5, 8, 1, 2, 3))
+DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
+              V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 DGLM_VARIANTS(EUL, 8, V_DMMA(EUL, 8, 8, 1, 7), V_SIMT(EUL, 8, 4, 8, 5))
 DGLM_VARIANTS(ADV, 1, V_SIMT(ADV, 1, 256, 4, 4), V_DMMA(ADV, 1, 64, 2, 1))
@@ -665,7 +870,9 @@ DGLM_VARIANTS(ADV, 3, V_DMMA(ADV, 3, 64, 2, 3), V_SIMT(ADV, 3, 64, 5, 4),
               V_BF16X6(ADV, 3, 32, 8))
 DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5))
 DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7))
-DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6))
+DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6),
+              V_M16(ADV, 6, 32, 1, 2, 2), V_M16(ADV, 6, 32, 1, 2, 1),
+              V_M16(ADV, 6, 32, 1, 2, 3))
 DGLM_VARIANTS(ADV, 7, V_SIMT(ADV, 7, 16, 8, 4), V_DMMA(ADV, 7, 16, 1, 5))
 DGLM_VARIANTS(ADV, 8, V_SIMT(ADV, 8, 16, 8, 4), V_DMMA(ADV, 8, 16, 1, 7))
 

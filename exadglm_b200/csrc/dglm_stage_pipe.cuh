@@ -107,7 +107,7 @@ __device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
   return r != 0;
 }
 
-template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1>
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1, int PR_ = 0>
 struct PCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -115,16 +115,26 @@ struct PCfg {
   static constexpr int MT = (Np + 7) / 8, NT = NCOL / 8;
   static constexpr int WN = WN_, WM = WM_ > MT ? MT : WM_;
   static constexpr int MGROUPS = (MT + WM - 1) / WM;
+  // PR_ != 0: split-precision mma.sync contraction (see contract_m16)
+  static constexpr bool M16 = PR_ != 0;
+  static constexpr int KSTEP16 = PR_ == 2 ? 8 : 16;
+  static constexpr int NPARTS16 = PR_ == 3 ? 3 : 2, NPROD16 = PR_ == 3 ? 6 : 3;
+  static constexpr int MT16 = (Np + 15) / 16;
+  static constexpr int WM16 = WM_ > MT16 ? MT16 : WM_;
+  static constexpr int MG16 = (MT16 + WM16 - 1) / WM16;
   static constexpr int NG = NG_;                        // consumer groups (ping-pong)
-  static constexpr int NWC = MGROUPS * (NT / WN);      // consumer warps per group
+  static constexpr int NWC = (M16 ? MG16 : MGROUPS) * (NT / WN);   // consumer warps per group
   static constexpr int TC = 32 * NWC;                   // consumer threads per group
   static constexpr int THREADS = NG * TC + 32;          // + producer warp
-  static constexpr int KV = 3 * Np, KVP = (KV + 3) / 4 * 4;
-  static constexpr int KF = NFF, KFP = (KF + 3) / 4 * 4;
+  static constexpr int KPAD = M16 ? KSTEP16 : 4;
+  static constexpr int KV = 3 * Np, KVP = (KV + KPAD - 1) / KPAD * KPAD;
+  static constexpr int KF = NFF, KFP = (KF + KPAD - 1) / KPAD * KPAD;
   static constexpr int KS = KVP / 4 + KFP / 4;
+  static constexpr int KSV16 = KVP / KSTEP16, KSF16 = KFP / KSTEP16, KST16 = KSV16 + KSF16;
+  static constexpr int SL16 = (KST16 + 7) / 8;
   static constexpr int BLD = NCOL + 4, BROWS = KVP > KFP ? KVP : KFP;
-  // shared memory segments, in doubles
-  static constexpr int S_AF = ASMEM ? KS * MT * 32 : 0;
+  // shared memory segments, in doubles (operator A fragments when ASMEM)
+  static constexpr int S_AF = !ASMEM ? 0 : M16 ? KST16 * MT16 * NPARTS16 * 64 : KS * MT * 32;
   static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
   static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
@@ -139,6 +149,7 @@ struct PCfg {
   static_assert((E * Np * 8) % 16 == 0 && (E * 8) % 16 == 0, "bulk copies need 16-byte sizes");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
   static_assert(NG == 1 || NG == 2, "one or two consumer groups");
+  static_assert(!(M16 && ASMEM), "mma.sync operator fragments are read from global memory");
 };
 
 // Producer warp of the pipelined kernels: optional one-off bulk load of an
@@ -213,10 +224,10 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_>
-__global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREADS, 1)
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_, int PR_>
+__global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::THREADS, 1)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
-  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>;
+  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 BLD = C::BLD, TC = C::TC;
   extern __shared__ __align__(16) double smem[];
@@ -261,7 +272,10 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREA
   double *sB = sB0 + grp * C::S_B;
   auto consumer_sync = [&](int n) { group_sync(bar_sync, n); };
   auto consumer_all = [&](bool v, int n) { return group_all(v, bar_and, n); };
-  double acc[C::WM][C::WN][2];
+  double acc[C::M16 ? 1 : C::WM][C::M16 ? 1 : C::WN][2];
+  constexpr int QM = C::M16 ? C::WM16 : 1, QN = C::M16 ? C::WN : 1;
+  float acc16[QM][QN][4];
+  double tot16[QM][QN][4];
   const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
   unsigned long long vmax = 0ull;
   bool ok = true;
@@ -311,11 +325,23 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREA
     consumer_sync(TC);
 
     // 2. volume contraction
+    if constexpr (C::M16) {
+#pragma unroll
+      for (int i = 0; i < QM; i++)
+#pragma unroll
+        for (int j = 0; j < QN; j++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            acc16[i][j][c] = 0.f;
+            tot16[i][j][c] = 0.0;
+          }
+      contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), 0, C::KSV16, sB, acc16,
+                           tot16, warp, lane);
+    } else {
 #pragma unroll
     for (int i = 0; i < C::WM; i++)
 #pragma unroll
       for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-    {
       const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
       const int m0 = mg * C::WM, n0 = ng * C::WN;
       const double *Ab = Afrag + (long)m0 * 32 + lane;
@@ -370,7 +396,10 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREA
     consumer_sync(TC);
 
     // 4. lift contraction
-    {
+    if constexpr (C::M16) {
+      contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), C::KSV16, C::KSF16, sB,
+                           acc16, tot16, warp, lane);
+    } else {
       const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
       const int m0 = mg * C::WM, n0 = ng * C::WN;
       const double *Ab = Afrag + ((long)(C::KVP / 4) * C::MT + m0) * 32 + lane;
@@ -392,7 +421,23 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_>::THREA
     consumer_sync(TC);
 
     // 5. epilogue: rhs -> sB as [v][i][EP], then the coalesced LSERK update
-    {
+    if constexpr (C::M16) {
+      const int mg = warp % C::MG16, ng = warp / C::MG16;
+      const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+      for (int ii = 0; ii < QM; ii++) {
+        if (mg * C::WM16 + ii >= C::MT16) continue;
+#pragma unroll
+        for (int jj = 0; jj < QN; jj++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            const int i = (mg * C::WM16 + ii) * 16 + g + (c >= 2 ? 8 : 0);
+            const int col = (ng * C::WN + jj) * 8 + 2 * t + (c & 1);
+            const int v = col / E, e = col - v * E;
+            if (i < Np) sB[(v * Np + i) * EP + e] = tot16[ii][jj][c];
+          }
+      }
+    } else {
       const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
 #pragma unroll
       for (int ii = 0; ii < C::WM; ii++) {

@@ -10,7 +10,8 @@ result (the right-hand side is a sum of large terms that nearly cancel):
                                            2^-21 (BF16x6).
 TF32x3 keeps ~22 significant bits per operand (measured ~2^-23), BF16x3 ~16
 bits (measured ~2^-18), BF16x6 24 bits with six part products; every mode
-spreads its MMAs over 8 FP32 tensor-memory accumulators.  The state after 20
+sums its products in FP32 over 8 slices of K (tensor-memory accumulators
+for tcgen05, register accumulators folded into FP64 for mma.sync).  The state after 20
 steps is checked in relative L2 (TF32x3 and BF16x6 <= 1e-6, BF16x3 <= 1e-4).
 """
 import numpy as np
@@ -24,7 +25,9 @@ pytestmark = pytest.mark.gpu
 
 SCALED_TOL = {"tf32x3": 2.0 ** -20, "bf16x3": 2.0 ** -16, "bf16x6": 2.0 ** -21}
 STATE_TOL = {"tf32x3": 1e-6, "bf16x3": 1e-4, "bf16x6": 1e-6}
-CASES = [("euler", 4), ("advection", 3)]
+# tcgen05 variants (Euler N=4, advection N=3) and split-precision mma.sync
+# variants (orders whose tcgen05 operand images exceed shared memory)
+CASES = [("euler", 4), ("advection", 3), ("euler", 5), ("euler", 6), ("advection", 6)]
 
 
 def rel(a, b):
