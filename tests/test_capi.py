@@ -40,8 +40,8 @@ def test_variants_are_described():
         for N in range(1, 9):
             v = capi.variants(phys, N)
             assert len(v) >= 2
-            assert all(d.startswith(("simt", "dmma", "pipe-dmma", "pipe2-dmma", "tcgen05-"))
-                       for d in v)
+            assert all(d.startswith(("simt", "dmma", "pipe-dmma", "pipe2-dmma", "tcgen05-",
+                                      "mma16-", "pipe-mma16-")) for d in v)
             assert capi.variants(phys, N, "fp64")
 
 
