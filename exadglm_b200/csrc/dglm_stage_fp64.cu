@@ -111,6 +111,7 @@ struct Cfg {
   static_assert(MODE == MODE_SIMT || NCOL % 8 == 0, "DMMA needs whole n-tiles");
   static_assert(MODE == MODE_SIMT || NT % WN == 0, "DMMA n-tiles must split over warps");
   static_assert(THREADS <= 1024, "block too large");
+  static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
 };
 
 // ---------------------------------------------------------------------------
@@ -862,7 +863,8 @@ DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
-DGLM_VARIANTS(EUL, 8, V_DMMA(EUL, 8, 8, 1, 7), V_SIMT(EUL, 8, 4, 8, 5))
+// N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB
+DGLM_VARIANTS(EUL, 8, V_SIMT(EUL, 8, 4, 8, 5), V_SIMT(EUL, 8, 4, 6, 5))
 DGLM_VARIANTS(ADV, 1, V_SIMT(ADV, 1, 256, 4, 4), V_DMMA(ADV, 1, 64, 2, 1))
 DGLM_VARIANTS(ADV, 2, V_SIMT(ADV, 2, 128, 5, 4), V_DMMA(ADV, 2, 64, 2, 2))
 DGLM_VARIANTS(ADV, 3, V_DMMA(ADV, 3, 64, 2, 3), V_SIMT(ADV, 3, 64, 5, 4),

@@ -103,6 +103,8 @@ def main(argv=None):
     ap.add_argument("--physics", default="euler", choices=["euler", "advection"])
     ap.add_argument("--orders", default="1-8")
     ap.add_argument("--dofs", type=float, default=2e7, help="target DOF count of the test mesh")
+    ap.add_argument("--precisions", default="fp64,tf32x3,bf16x3,bf16x6",
+                    help="modes to tune (those without variants for an order are skipped)")
     a = ap.parse_args(argv)
     lo, _, hi = a.orders.partition("-")
     for N in range(int(lo), int(hi or lo) + 1):
@@ -111,10 +113,13 @@ def main(argv=None):
         n = max(3, int(round((a.dofs / (6 * Np * nv)) ** (1 / 3))))
         prob = (P.euler_sine(n=n, N=N) if a.physics == "euler"
                 else P.advection_gaussian(n=n, N=N))
-        best, timings = tune(prob)
-        print(f"{a.physics} N={N} K={prob.K}: best variant {best}")
-        for t, v, d in sorted(timings):
-            print(f"   {t:8.4f} ms  v{v}  {d}")
+        for prec in a.precisions.split(","):
+            if not capi.variants(a.physics, N, prec):
+                continue
+            best, timings = tune(prob, precision=prec)
+            print(f"{a.physics} N={N} K={prob.K} {prec}: best variant {best}")
+            for t, v, d in sorted(timings):
+                print(f"   {t:8.4f} ms  v{v}  {d}")
     return 0
 
 
