@@ -182,6 +182,7 @@ struct MCfg {
   static_assert(NPAD <= 256, "MMA N limit");
   static_assert(NACC * NPAD <= 512, "tensor memory has 512 columns");
   static_assert(NWC >= NISS && NACC % NISS == 0, "issuers split the accumulators evenly");
+  static_assert(PHYS != EUL || S_R >= 8 * E * Nfp, "wave-speed terms reuse the rhs buffer");
   static_assert(SMEM < (1u << 18), "descriptor start addresses must fit 14 bits (>> 4)");
 };
 
@@ -453,23 +454,44 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
     // 6. LSERK update with coalesced stores; the new state goes back to
     //    shared memory only when the fused wave-speed pass reads it
     const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
-    for (int v = 0; v < NV; v++) {
-      const long base = v * vs + e0 * Np;
-      for (int g = tid; g < ne * Np; g += TC) {
-        const int e = g / Np, i = g - e * Np;
-        const double rhs = sR[(v * Np + i) * EP + e];
-        if (a.rhs_only) {
-          a.u_out[base + g] = rhs;
-        } else {
-          const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
-          const double un = bU[v * E * Np + g] + a.rkb * kn;
-          a.kreg[base + g] = kn;
-          a.u_out[base + g] = un;
-          if (keep_u) bU[v * E * Np + g] = un;
-        }
+    // one flat loop over (variable, node): every thread has independent
+    // updates in flight
+    for (int vg = tid; vg < NV * ne * Np; vg += TC) {
+      const int v = vg / (ne * Np), g = vg - v * (ne * Np);
+      const int e = g / Np, i = g - e * Np;
+      const long gi = v * vs + e0 * Np + g;
+      const double rhs = sR[(v * Np + i) * EP + e];
+      if (a.rhs_only) {
+        a.u_out[gi] = rhs;
+      } else {
+        const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
+        const double un = bU[v * E * Np + g] + a.rkb * kn;
+        a.kreg[gi] = kn;
+        a.u_out[gi] = un;
+        if (keep_u) bU[v * E * Np + g] = un;
       }
     }
     if (PHYS == EUL && a.last_stage && !a.rhs_only) {
+      consumer_sync(TC);
+      // |v|^2 and c^2 at every face node in parallel (into the rhs staging
+      // buffer, free by now), then the per-face max
+      double *sW = sR;
+      for (int it = tid; it < 4 * E * Nfp; it += TC) {
+        const int fe = it / Nfp, j = it - fe * Nfp, f = fe / E, e = fe - f * E;
+        double v2 = 0.0, c2 = 0.0;
+        if (e < ne) {
+          const int nd = e * Np + sFm[f * Nfp + j];
+          const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
+                       u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
+          const double ir = 1.0 / u1;
+          const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
+          v2 = vx * vx + vy * vy + vz * vz;
+          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
+          c2 = fabs(a.gamma * pres * ir);
+        }
+        sW[2 * it] = v2;
+        sW[2 * it + 1] = c2;
+      }
       consumer_sync(TC);
       for (int itm = tid; itm < 4 * E; itm += TC) {
         const int f = itm / E, e = itm - f * E;
@@ -477,15 +499,8 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
         double mv2 = 0.0, mc2 = 0.0;
         bool bad = false;
         for (int j = 0; j < Nfp; j++) {
-          const int nd = e * Np + sFm[f * Nfp + j];
-          const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
-                       u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
-          const double ir = 1.0 / u1;
-          const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
-          const double v2 = vx * vx + vy * vy + vz * vz;
+          const double v2 = sW[2 * (itm * Nfp + j)], c2 = sW[2 * (itm * Nfp + j) + 1];
           mv2 = v2 > mv2 ? v2 : mv2;
-          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-          const double c2 = fabs(a.gamma * pres * ir);
           mc2 = c2 > mc2 ? c2 : mc2;
           bad |= (v2 != v2) || (c2 != c2);
         }

@@ -150,6 +150,7 @@ struct PCfg {
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
   static_assert(NG == 1 || NG == 2, "one or two consumer groups");
   static_assert(!(M16 && ASMEM), "mma.sync operator fragments are read from global memory");
+  static_assert(PHYS != EUL || S_B >= 8 * E * Nfp, "wave-speed terms reuse the rhs buffer");
 };
 
 // Producer warp of the pipelined kernels: optional one-off bulk load of an
@@ -457,40 +458,54 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
     consumer_sync(TC);
     // the new state goes back to shared memory only for the fused wave speed
     const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
-    for (int v = 0; v < NV; v++) {
-      const long base = v * vs + e0 * Np;
-      for (int g = tid; g < ne * Np; g += TC) {
-        const int e = g / Np, i = g - e * Np;
-        const double rhs = sB[(v * Np + i) * EP + e];
-        if (a.rhs_only) {
-          a.u_out[base + g] = rhs;
-        } else {
-          const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
-          const double un = bU[v * E * Np + g] + a.rkb * kn;
-          a.kreg[base + g] = kn;
-          a.u_out[base + g] = un;
-          if (keep_u) bU[v * E * Np + g] = un;
-        }
+    // one flat loop over (variable, node): every thread has independent
+    // updates in flight
+    for (int vg = tid; vg < NV * ne * Np; vg += TC) {
+      const int v = vg / (ne * Np), g = vg - v * (ne * Np);
+      const int e = g / Np, i = g - e * Np;
+      const long gi = v * vs + e0 * Np + g;
+      const double rhs = sB[(v * Np + i) * EP + e];
+      if (a.rhs_only) {
+        a.u_out[gi] = rhs;
+      } else {
+        const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
+        const double un = bU[v * E * Np + g] + a.rkb * kn;
+        a.kreg[gi] = kn;
+        a.u_out[gi] = un;
+        if (keep_u) bU[v * E * Np + g] = un;
       }
     }
     if (PHYS == EUL && a.last_stage && !a.rhs_only) {
       consumer_sync(TC);
       // fused calc_maxv on the new state
+      // |v|^2 and c^2 at every face node in parallel (into the rhs staging
+      // buffer, free by now), then the per-face max
+      double *sW = sB;
+      for (int it = tid; it < 4 * E * Nfp; it += TC) {
+        const int fe = it / Nfp, j = it - fe * Nfp, f = fe / E, e = fe - f * E;
+        double v2 = 0.0, c2 = 0.0;
+        if (e < ne) {
+          const int nd = e * Np + sFm[f * Nfp + j];
+          const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
+                       u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
+          const double ir = 1.0 / u1;
+          const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
+          v2 = vx * vx + vy * vy + vz * vz;
+          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
+          c2 = fabs(a.gamma * pres * ir);
+        }
+        sW[2 * it] = v2;
+        sW[2 * it + 1] = c2;
+      }
+      consumer_sync(TC);
       for (int itm = tid; itm < 4 * E; itm += TC) {
         const int f = itm / E, e = itm - f * E;
         if (e >= ne) continue;
         double mv2 = 0.0, mc2 = 0.0;
         bool bad = false;
         for (int j = 0; j < Nfp; j++) {
-          const int nd = e * Np + sFm[f * Nfp + j];
-          const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
-                       u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
-          const double ir = 1.0 / u1;
-          const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
-          const double v2 = vx * vx + vy * vy + vz * vz;
+          const double v2 = sW[2 * (itm * Nfp + j)], c2 = sW[2 * (itm * Nfp + j) + 1];
           mv2 = v2 > mv2 ? v2 : mv2;
-          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-          const double c2 = fabs(a.gamma * pres * ir);
           mc2 = c2 > mc2 ? c2 : mc2;
           bad |= (v2 != v2) || (c2 != c2);
         }
