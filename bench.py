@@ -243,6 +243,25 @@ def run_reference_arm(a):
     return 0
 
 
+def reduce_max(x, dist=None):
+    """Max of a per-rank scalar over the process group (identity without
+    one); the tensor lives where the backend wants it (CUDA for NCCL, CPU
+    for gloo)."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, units_per_step, steps, ms_max):
+    """Whole-job rate of `world` replicas: all ranks' units over the slowest
+    rank's time."""
+    return world * units_per_step * steps / (ms_max * 1e-3)
+
+
 def _events(stream):
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -483,11 +502,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist)
 
     p = build_problem(a)
     stream = torch.cuda.Stream()
@@ -523,7 +538,7 @@ def main():
     clk = clocks.stop()
     barrier()
     ms_max = max_over_ranks(ms)
-    value = world * per_step * a.steps / (ms_max * 1e-3)
+    value = replica_rate(world, per_step, a.steps, ms_max)
 
     # ---- stage kernel alone, for the roofline -----------------------------
     t, dt, _ = s.time()
