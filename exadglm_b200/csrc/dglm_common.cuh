@@ -122,6 +122,10 @@ struct StageVariantInfo {
   int groups;    // PIPE: consumer groups taking alternate tiles (1 or 2)
   int kstep;     // MMA16: K per mma.sync (8 TF32, 16 BF16)
   int persistent;  // 1: one CTA per SM walking the tiles (TMA-fed pipeline)
+  int ring;        // PIPE: tile buffers in the producer/consumer ring (2 to 4)
+  int producers;   // PIPE: producer warps sharing the neighbour gathers (1 to 4)
+  int ksplit;      // PIPE: k-chunks of the DMMA contraction summed in the epilogue
+  int fused;       // PIPE: 1 = volume and lift contractions in one DMMA pass
 };
 
 // fused FP64 stage launcher (dglm_stage_fp64.cu)

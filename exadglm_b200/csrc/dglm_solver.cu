@@ -752,10 +752,20 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
              : v.prec == DGLM_PREC_BF16X6 ? "tcgen05-bf16x6"
                                           : "tcgen05-bf16x3",
              v.E, v.npad, v.threads, v.smem);
-  else
-    snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu",
-             v.mode == MODE_PIPE ? (v.groups == 2 ? "pipe2-dmma" : "pipe-dmma") : "dmma", v.E,
-             v.CPT, v.WM, v.threads, v.smem);
+  else {
+    const int n = snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu",
+                           v.mode == MODE_PIPE ? (v.groups == 2 ? "pipe2-dmma" : "pipe-dmma")
+                                               : "dmma",
+                           v.E, v.CPT, v.WM, v.threads, v.smem);
+    // ring depth, producer warps and k-split are named only when they differ
+    // from 2, 1 and 1
+    if (v.mode == MODE_PIPE && (v.ring > 2 || v.producers > 1 || v.ksplit > 1) && n > 0 &&
+        (size_t)n < len) {
+      const int m = snprintf(buf + n, len - n, " ring=%d prod=%d", v.ring, v.producers);
+      if (v.ksplit > 1 && m > 0 && (size_t)(n + m) < len)
+        snprintf(buf + n + m, len - n - m, " ksplit=%d%s", v.ksplit, v.fused ? " fused" : "");
+    }
+  }
   return DGLM_OK;
 }
 

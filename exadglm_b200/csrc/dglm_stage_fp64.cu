@@ -729,10 +729,11 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
-template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG, int PR>
+template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG, int PR, int NB, int PW,
+          int KSP, bool FU>
 static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR>;
-  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>;
+  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -742,9 +743,10 @@ static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1, int PR = 0>
+template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1, int PR = 0, int NB = 2,
+          int PW = 1, int KSP = 1, bool FU = false>
 static Variant make_pipe() {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>;
   StageVariantInfo i{};
   i.mode = PR ? MODE_MMA16 : MODE_PIPE;
   i.E = E;
@@ -759,11 +761,15 @@ static Variant make_pipe() {
   i.smem = C::SMEM;
   i.groups = NG;
   i.persistent = 1;
+  i.ring = NB;
+  i.producers = PW;
+  i.ksplit = KSP;
+  i.fused = FU ? 1 : 0;
   if (PR) {
     i.prec = PR == 2 ? DGLM_PREC_TF32X3 : PR == 3 ? DGLM_PREC_BF16X6 : DGLM_PREC_BF16X3;
     i.kstep = C::KSTEP16;
   }
-  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR>};
+  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>};
 }
 
 template <int PHYS, int N, int E, int PREC, int NWC>
@@ -829,6 +835,15 @@ static const std::vector<Variant> &variants();
 #define V_DMMA(P, NN, E, WN, WM) make_v<P, NN, MODE_DMMA, E, 1, WN, WM>()
 #define V_PIPE(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS>()
 #define V_PIPE2(P, NN, E, WN, WM, AS) make_pipe<P, NN, E, WN, WM, AS, 2>()
+// two consumer groups, a ring of NB buffers and PW producer warps
+#define V_PIPE2R(P, NN, E, WN, WM, NB, PW) make_pipe<P, NN, E, WN, WM, false, 2, 0, NB, PW>()
+// one consumer group, a ring of NB buffers and PW producer warps
+#define V_PIPER(P, NN, E, WN, WM, AS, NB, PW) make_pipe<P, NN, E, WN, WM, AS, 1, 0, NB, PW>()
+// one consumer group, all m-tiles per warp, KSP k-chunks, PW producer warps
+#define V_PIPEK(P, NN, E, WN, AS, KSP, PW) make_pipe<P, NN, E, WN, 99, AS, 1, 0, 2, PW, KSP>()
+// as V_PIPEK with the volume and lift contractions fused into one pass
+#define V_PIPEF(P, NN, E, WN, AS, KSP, PW) \
+  make_pipe<P, NN, E, WN, 99, AS, 1, 0, 2, PW, KSP, true>()
 #define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define V_TF32W(P, NN, E, W) make_mixed<P, NN, E, PREC_TF32, W>()
@@ -847,7 +862,8 @@ static const std::vector<Variant> &variants();
 DGLM_VARIANTS(EUL, 1, V_SIMT(EUL, 1, 128, 4, 5), V_DMMA(EUL, 1, 64, 4, 1))
 DGLM_VARIANTS(EUL, 2, V_SIMT(EUL, 2, 64, 5, 5), V_DMMA(EUL, 2, 32, 4, 2))
 DGLM_VARIANTS(EUL, 3, V_DMMA(EUL, 3, 16, 2, 3), V_SIMT(EUL, 3, 32, 5, 5),
-              V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true))
+              V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true),
+              V_PIPEF(EUL, 3, 8, 1, true, 3, 2), V_PIPEF(EUL, 3, 16, 2, true, 3, 2))
 DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_SIMT(EUL, 4, 16, 5, 5), V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
@@ -856,10 +872,12 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_TF32W(EUL, 4, 8, 16), V_BF16W(EUL, 4, 8, 16), V_BF16X6(EUL, 4, 8, 16),
               V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_BF16X6(EUL, 4, 8, 8),
               V_M16(EUL, 4, 8, 1, 3, 2), V_M16(EUL, 4, 8, 1, 1, 1), V_M16(EUL, 4, 8, 1, 1, 3),
-              V_PM16(EUL, 4, 8, 1, 3, 1))
+              V_PM16(EUL, 4, 8, 1, 3, 1), V_PIPER(EUL, 4, 8, 1, 2, true, 2, 2),
+              V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
+              V_PIPEF(EUL, 4, 8, 1, true, 3, 1))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
-              V_M16(EUL, 5, 8, 1, 2, 3))
+              V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
@@ -869,9 +887,11 @@ DGLM_VARIANTS(ADV, 1, V_SIMT(ADV, 1, 256, 4, 4), V_DMMA(ADV, 1, 64, 2, 1))
 DGLM_VARIANTS(ADV, 2, V_SIMT(ADV, 2, 128, 5, 4), V_DMMA(ADV, 2, 64, 2, 2))
 DGLM_VARIANTS(ADV, 3, V_DMMA(ADV, 3, 64, 2, 3), V_SIMT(ADV, 3, 64, 5, 4),
               V_PIPE(ADV, 3, 32, 1, 3, true), V_TF32(ADV, 3, 32), V_BF16(ADV, 3, 32),
-              V_BF16X6(ADV, 3, 32, 8))
-DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5))
-DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7))
+              V_BF16X6(ADV, 3, 32, 8), V_PIPEF(ADV, 3, 32, 1, true, 3, 2))
+DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5),
+              V_PIPEF(ADV, 4, 32, 1, false, 3, 2))
+DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7),
+              V_PIPEF(ADV, 5, 16, 1, false, 4, 2))
 DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6),
               V_M16(ADV, 6, 32, 1, 2, 2), V_M16(ADV, 6, 32, 1, 2, 1),
               V_M16(ADV, 6, 32, 1, 2, 3))

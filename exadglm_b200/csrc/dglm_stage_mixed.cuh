@@ -123,6 +123,7 @@ __device__ __forceinline__ void split_bf16x3(double x, unsigned short (&p)[3]) {
 template <int PHYS, int N, int E_, int PREC, int NWC_ = 8>
 struct MCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
+  static constexpr int NB = 2, PW = 1;   // tile ring and producer warps (pipe_producer)
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
   static constexpr int E = E_, EP = E_ + 1, NCOL = NV * E;
   static constexpr int M = NCOL <= 64 ? 64 : 128;            // MMA rows
@@ -155,7 +156,10 @@ struct MCfg {
   static constexpr int BIMG = NPARTS * (BV_BYTES + BF_BYTES);   // part 0, part 1, ...
   static constexpr int NWC = NWC_, TC = 32 * NWC, THREADS = TC + 32;
   // FP64 pipeline buffers (as in PCfg)
-  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
+  // neighbour traces [v][e][UPS], written by pipe_producer (conflict-free
+  // gathers and face-flux reads)
+  static constexpr int UPS = E >= 16 ? NFF + 1 : NFF + 2;
+  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * E * UPS;
   static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
@@ -272,7 +276,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
   const unsigned tmem = *sTmem;
 
   if (warp == C::NWC) {
-    pipe_producer<C, PHYS>(a, ntiles, sBimg, sBuf0, full, empty, abar, C::BIMG, lane);
+    pipe_producer<C, PHYS>(a, ntiles, sBimg, sBuf0, full, empty, abar, C::BIMG, 0, lane);
     return;
   }
 
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           qm[v] = bU[v * E * Np + e * Np + nodeM];
-          qb[v] = 0.5 * (qm[v] + bUP[(v * NFF + fj) * E + e]);
+          qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
         }
         euler_flux_fast(a.gamma, qb, F, Gf, W);
 #pragma unroll
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
         }
       } else {
         const double um = bU[e * Np + nodeM];
-        const double ub = 0.5 * (um + bUP[fj * E + e]);
+        const double ub = 0.5 * (um + bUP[e * C::UPS + fj]);
         const double F = bV[e * Np + nodeM] * ub, Gf = bV[E * Np + e * Np + nodeM] * ub,
                      W = bV[2 * E * Np + e * Np + nodeM] * ub;
         const double nd = nx * F + ny * Gf + nz * W;

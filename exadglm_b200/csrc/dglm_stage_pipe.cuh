@@ -3,9 +3,9 @@
 // dmma_8x8x4).
 //
 // One CTA per SM walks the element tiles t = blockIdx.x, +gridDim.x, ...
-// with a two-deep shared-memory pipeline:
+// with a ring of two to four shared-memory tile buffers:
 //
-//   producer warp   TMA bulk copies (cp.async.bulk, mbarrier complete_tx) of
+//   producer warps  TMA bulk copies (cp.async.bulk, mbarrier complete_tx) of
 //                   the next tile's state u, RK register k, metrics, face
 //                   data (and advection velocity) -- all contiguous per tile
 //                   -- plus cp.async gathers of the neighbour traces
@@ -107,7 +107,8 @@ __device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
   return r != 0;
 }
 
-template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1, int PR_ = 0>
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1, int PR_ = 0,
+          int NB_ = 2, int PW_ = 1, int KSP_ = 1, bool FU_ = false>
 struct PCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -123,57 +124,92 @@ struct PCfg {
   static constexpr int WM16 = WM_ > MT16 ? MT16 : WM_;
   static constexpr int MG16 = (MT16 + WM16 - 1) / WM16;
   static constexpr int NG = NG_;                        // consumer groups (ping-pong)
-  static constexpr int NWC = (M16 ? MG16 : MGROUPS) * (NT / WN);   // consumer warps per group
+  static constexpr int NB = NB_;                        // tile buffers in the ring
+  static constexpr int PW = PW_;                        // producer warps
+  // KSP > 1: each DMMA warp takes all m-tiles of its n-block over one of KSP
+  // k-chunks of each contraction and stores a partial rhs; the epilogue sums
+  // the KSP partials (no padded m-tiles, fewer operand loads per DMMA)
+  static constexpr int KSP = KSP_;
+  // FUSE: face-flux rows sit below the volume rows, both flux phases run
+  // back to back and one DMMA pass covers the stacked k range
+  static constexpr bool FUSE = FU_;
+  static constexpr int NWC = (M16 ? MG16 : MGROUPS) * (NT / WN) * KSP;   // consumer warps per group
   static constexpr int TC = 32 * NWC;                   // consumer threads per group
-  static constexpr int THREADS = NG * TC + 32;          // + producer warp
+  static constexpr int THREADS = NG * TC + 32 * PW;     // + producer warps
   static constexpr int KPAD = M16 ? KSTEP16 : 4;
   static constexpr int KV = 3 * Np, KVP = (KV + KPAD - 1) / KPAD * KPAD;
   static constexpr int KF = NFF, KFP = (KF + KPAD - 1) / KPAD * KPAD;
   static constexpr int KS = KVP / 4 + KFP / 4;
   static constexpr int KSV16 = KVP / KSTEP16, KSF16 = KFP / KSTEP16, KST16 = KSV16 + KSF16;
   static constexpr int SL16 = (KST16 + 7) / 8;
-  static constexpr int BLD = NCOL + 4, BROWS = KVP > KFP ? KVP : KFP;
+  // rows of the contraction operand: the DMMA path pads the row stride to
+  // 8 (mod 16) doubles and flips column bit 2 on rows whose bit 1 is set
+  // (bcol), so that stores of two neighbouring rows by a half-warp and the
+  // m8n8k4 B-fragment loads (rows k0..k0+3) both hit 16 distinct bank pairs
+  static constexpr bool SWZ = !M16;
+  static constexpr int BLD = M16 ? NCOL + 4 : NCOL + (24 - NCOL % 16) % 16;
+  static constexpr int BROWS = FUSE ? KVP + KFP : KVP > KFP ? KVP : KFP;
+  static constexpr int FR0 = FUSE ? KVP : 0;             // first face-flux row
+  // neighbour traces [v][e][UPS]: consecutive gathers write consecutive
+  // words, and face-flux reads (8 elements x 2 face nodes, or 16 elements)
+  // land on distinct bank pairs
+  static constexpr int UPS = E >= 16 ? NFF + 1 : NFF + 2;
   // shared memory segments, in doubles (operator A fragments when ASMEM)
   static constexpr int S_AF = !ASMEM ? 0 : M16 ? KST16 * MT16 * NPARTS16 * 64 : KS * MT * 32;
-  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * NFF * E;
+  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * E * UPS;
   static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
-  static constexpr int S_B = BROWS * BLD > NV * Np * EP ? BROWS * BLD : NV * Np * EP;
-  static constexpr int S_MISC = 8 + NFF / 2 + 1 + 32 * NG + 8;  // barriers, Fmask, reduction
+  static constexpr int S_R = NV * Np * EP;              // one rhs (partial) [v][i][EP]
+  static constexpr int S_B = BROWS * BLD > KSP * S_R ? BROWS * BLD : KSP * S_R;
+  // barriers: full[NB], empty[NB], the operator-image barrier, padding
+  static constexpr int NBAR = 2 * NB + 2 > 8 ? 2 * NB + 2 : 8;
+  static constexpr int S_MISC = NBAR + NFF / 2 + 1 + 32 * NG + 8;  // barriers, Fmask, reduction
   static constexpr size_t SMEM =
-      sizeof(double) * ((size_t)S_AF + 2 * S_BUF + NG * S_B + S_MISC);
+      sizeof(double) * ((size_t)S_AF + NB * S_BUF + NG * S_B + S_MISC);
   // bytes the producer's bulk copies deliver per tile
   static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE + S_VEL);
   static_assert(NCOL % 8 == 0 && NT % WN == 0, "n-tiles must split over the warps");
   static_assert((E * Np * 8) % 16 == 0 && (E * 8) % 16 == 0, "bulk copies need 16-byte sizes");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
   static_assert(NG == 1 || NG == 2, "one or two consumer groups");
+  static_assert(NB >= 2 && NB <= 4 && PW >= 1 && PW <= 4, "ring of 2..4, 1..4 producers");
+  static_assert(KSP == 1 || (!M16 && MGROUPS == 1), "k-split takes all m-tiles per warp");
+  static_assert(!(FUSE && M16), "the fused contraction is a DMMA path");
+  static_assert(FR0 % 4 == 0, "face rows start on a k-step");
+  static_assert(NWC <= 32, "per-warp wave-speed maxima fit one warp");
   static_assert(!(M16 && ASMEM), "mma.sync operator fragments are read from global memory");
   static_assert(PHYS != EUL || S_B >= 8 * E * Nfp, "wave-speed terms reuse the rhs buffer");
+  static_assert(S_UP % 2 == 0, "segments after the traces stay 16-byte aligned");
+  __device__ static __forceinline__ int bcol(int row, int col) {
+    return SWZ ? col ^ (((row >> 1) & 1) << 2) : col;
+  }
 };
 
-// Producer warp of the pipelined kernels: optional one-off bulk load of an
-// operator image into shared memory (abar), then per tile (two-deep ring)
-// TMA bulk copies of the tile's u, k, metrics, face data (and advection
-// velocity) and cp.async gathers of the neighbour traces.
+// Producer warps of the pipelined kernels: optional one-off bulk load of an
+// operator image into shared memory (abar), then per tile (ring of C::NB
+// buffers) TMA bulk copies of the tile's u, k, metrics, face data (and
+// advection velocity), issued by producer warp 0, and cp.async gathers of the
+// neighbour traces, split over the C::PW producer warps.  full[b] completes
+// once the bulk bytes have landed and all 32 * PW lanes' gathers are done.
 template <class C, int PHYS>
 __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, void *op_smem,
                                               double *sBuf0, unsigned long long *full,
                                               unsigned long long *empty,
                                               unsigned long long *abar, unsigned op_bytes,
-                                              int lane) {
-  constexpr int NV = C::NV, Np = C::Np, NFF = C::NFF, E = C::E;
+                                              int pw, int lane) {
+  constexpr int NV = C::NV, Np = C::Np, NFF = C::NFF, E = C::E, NB = C::NB;
   const long vs = a.vs, gs = a.gstride;
-  if (op_bytes && lane == 0) {
+  const bool lead = pw == 0 && lane == 0;
+  if (op_bytes && lead) {
     mbar_arrive_expect_tx(abar, op_bytes);
     bulk_g2s(op_smem, a.AT, op_bytes, abar);
   }
   int it = 0;
   bool ok = true;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
-    const int b = it & 1;
-    if (it >= 2 && !mbar_wait(&empty[b], ((it >> 1) - 1) & 1)) {
+    const int b = it % NB;
+    if (it >= NB && !mbar_wait(&empty[b], ((it / NB) - 1) & 1)) {
       ok = false;
       break;
     }
@@ -182,7 +218,7 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
     double *B = sBuf0 + b * C::S_BUF;
     double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
     double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
-    if (lane == 0) {
+    if (lead) {
       mbar_arrive_expect_tx(&full[b], C::TX);
       for (int v = 0; v < NV; v++) {
         bulk_g2s(bU + v * E * Np, a.u_in + v * vs + e0 * Np, 8u * E * Np, &full[b]);
@@ -197,57 +233,60 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
         for (int q = 0; q < 3; q++)
           bulk_g2s(bV + q * E * Np, a.vel + q * vs + e0 * Np, 8u * E * Np, &full[b]);
     }
-    // neighbour traces u+ = u[vmapP] into [v][fj][e]: all of this lane's
+    // neighbour traces u+ = u[vmapP] into [v][e][UPS]: all of this lane's
     // vmapP loads are issued first, so their latency is paid once
-    constexpr int GPL = (E * NFF + 31) / 32;
+    constexpr int PT = 32 * C::PW;
+    constexpr int GPL = (E * NFF + PT - 1) / PT;
     int vmr[GPL];
 #pragma unroll
     for (int j = 0; j < GPL; j++) {
-      const int idx = lane + 32 * j;
+      const int idx = 32 * pw + lane + PT * j;
       vmr[j] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
     }
 #pragma unroll
     for (int j = 0; j < GPL; j++) {
-      const int idx = lane + 32 * j;
+      const int idx = 32 * pw + lane + PT * j;
       if (vmr[j] >= 0) {
         const int e = idx / NFF, fj = idx - e * NFF;
 #pragma unroll
         for (int v = 0; v < NV; v++)
-          cp_async8(bUP + (v * NFF + fj) * E + e, a.u_in + v * vs + vmr[j]);
+          cp_async8(bUP + (v * E + e) * C::UPS + fj, a.u_in + v * vs + vmr[j]);
       }
     }
     cp_async_arrive_noinc(&full[b]);
   }
   if (!ok) atomicOr(&a.sc->flags, 4);
-  // let the copies of the last two tiles settle before this warp leaves
-  for (int j = (it > 2 ? it - 2 : 0); j < it; j++) mbar_wait(&full[j & 1], (j >> 1) & 1);
+  // let the copies of the last NB tiles settle before this warp leaves
+  for (int j = (it > NB ? it - NB : 0); j < it; j++) mbar_wait(&full[j % NB], (j / NB) & 1);
   if (op_bytes) mbar_wait(abar, 0);
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_, int PR_>
-__global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::THREADS, 1)
+template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_, int PR_, int NB_,
+          int PW_, int KSP_, bool FU_>
+__global__ void __launch_bounds__(
+    PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_>::THREADS, 1)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
-  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>;
+  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 BLD = C::BLD, TC = C::TC;
   extern __shared__ __align__(16) double smem[];
   double *sAF = smem;
   double *sBuf0 = sAF + C::S_AF;
-  double *sB0 = sBuf0 + 2 * C::S_BUF;   // one working buffer per consumer group
+  double *sB0 = sBuf0 + C::NB * C::S_BUF;   // one working buffer per consumer group
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(sB0 + C::NG * C::S_B);
-  unsigned long long *full = bars, *empty = bars + 2, *abar = bars + 4;
-  int *sFm = reinterpret_cast<int *>(bars + 8);
+  unsigned long long *full = bars, *empty = bars + C::NB, *abar = bars + 2 * C::NB;
+  int *sFm = reinterpret_cast<int *>(bars + C::NBAR);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
 
   const int ttid = threadIdx.x, twarp = ttid >> 5, lane = ttid & 31;
   const long vs = a.vs;
 
   if (ttid == 0) {
-    mbar_init(&full[0], 33);
-    mbar_init(&full[1], 33);
-    mbar_init(&empty[0], C::NWC);
-    mbar_init(&empty[1], C::NWC);
+    for (int b = 0; b < C::NB; b++) {
+      mbar_init(&full[b], 1 + 32 * C::PW);
+      mbar_init(&empty[b], C::NWC);
+    }
     mbar_init(abar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -258,15 +297,17 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
   auto buf = [&](int b) { return sBuf0 + b * C::S_BUF; };
 
   // ------------------------------------------------------------- producer
-  if (twarp == C::NG * C::NWC) {
-    pipe_producer<C, PHYS>(a, ntiles, sAF, sBuf0, full, empty, abar, 8u * C::S_AF, lane);
+  if (twarp >= C::NG * C::NWC) {
+    pipe_producer<C, PHYS>(a, ntiles, sAF, sBuf0, full, empty, abar, 8u * C::S_AF,
+                           twarp - C::NG * C::NWC, lane);
     return;
   }
 
   // ------------------------------------------------------------ consumers
-  // Group g takes the CTA's tiles it = g, g + NG, ...; with two groups tile
-  // it always lands in buffer it & 1 = g, and one group's tensor-core phase
-  // overlaps the other's flux and epilogue phases.
+  // Group g takes the CTA's tiles it = g, g + NG, ... from buffer it % NB;
+  // with two groups one group's tensor-core phase overlaps the other's flux
+  // and epilogue phases, and a ring deeper than two lets the producers fill
+  // the next tile while both groups hold theirs.
   const int grp = twarp / C::NWC;
   const int warp = twarp - grp * C::NWC, tid = ttid - grp * TC;
   const int bar_sync = 1 + 2 * grp, bar_and = 2 + 2 * grp;
@@ -282,10 +323,39 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
   bool ok = true;
   if (ASMEM) ok = consumer_all(mbar_wait(abar, 0), TC);
   const double *Afrag = ASMEM ? sAF : a.AT;
+  // DMMA warp roles: m-group, n-block and k-chunk (KSP > 1: one m-group)
+  constexpr int NBLK = C::NT / C::WN;
+  const int mg = C::KSP > 1 ? 0 : warp % C::MGROUPS;
+  const int ng = C::KSP > 1 ? warp % NBLK : warp / C::MGROUPS;
+  const int kc = C::KSP > 1 ? warp / NBLK : 0;
+  const int m0 = mg * C::WM, n0 = ng * C::WN;
+  // acc += A[:, k-steps of this warp's chunk of [0, nks)] x sB rows; the A
+  // fragments of k-step ks start at Afrag + a_off + ks * MT * 32
+  auto dmma_phase = [&](long a_off, int nks) {
+    const int kchunk = (nks + C::KSP - 1) / C::KSP;
+    const int kb = kc * kchunk, ke = min(kb + kchunk, nks);
+    const double *Ab = Afrag + a_off + (long)m0 * 32 + lane;
+    // row k0 + (lane & 3) with k0 % 4 == 0: the swizzle bit is lane bit 1
+    const double *Bb = sB + (lane & 3) * BLD + n0 * 8 + C::bcol(lane & 3, lane >> 2);
+#pragma unroll 2
+    for (int ks = kb; ks < ke; ks++) {
+      double av[C::WM], bv[C::WN];
+#pragma unroll
+      for (int i = 0; i < C::WM; i++)
+        av[i] = (m0 + i < C::MT) ? Ab[((long)ks * C::MT + i) * 32] : 0.0;
+#pragma unroll
+      for (int j = 0; j < C::WN; j++) bv[j] = Bb[ks * 4 * BLD + j * 8];
+#pragma unroll
+      for (int i = 0; i < C::WM; i++)
+        if (m0 + i < C::MT)   // warp-uniform: m-tiles past MT are skipped
+#pragma unroll
+          for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
+    }
+  };
   int it = grp;
   for (int t = blockIdx.x + grp * gridDim.x; ok && t < ntiles; t += C::NG * gridDim.x, it += C::NG) {
-    const int b = it & 1;
-    if (!consumer_all(mbar_wait(&full[b], (it >> 1) & 1), TC)) {
+    const int b = it % C::NB;
+    if (!consumer_all(mbar_wait(&full[b], (it / C::NB) & 1), TC)) {
       ok = false;
       break;
     }
@@ -308,25 +378,27 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
         euler_flux_fast(a.gamma, q, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          const int col = v * E + e;
-          sB[(0 * Np + i) * BLD + col] = rx * F[v] + ry * Gf[v] + rz * W[v];
-          sB[(1 * Np + i) * BLD + col] = sx * F[v] + sy * Gf[v] + sz * W[v];
-          sB[(2 * Np + i) * BLD + col] = tx * F[v] + ty * Gf[v] + tz * W[v];
+          const int col = v * E + e, r0 = i, r1 = Np + i, r2 = 2 * Np + i;
+          sB[r0 * BLD + C::bcol(r0, col)] = rx * F[v] + ry * Gf[v] + rz * W[v];
+          sB[r1 * BLD + C::bcol(r1, col)] = sx * F[v] + sy * Gf[v] + sz * W[v];
+          sB[r2 * BLD + C::bcol(r2, col)] = tx * F[v] + ty * Gf[v] + tz * W[v];
         }
       } else {
         const double uu = bU[e * Np + i];
         const double F = bV[e * Np + i] * uu, Gf = bV[E * Np + e * Np + i] * uu,
                      W = bV[2 * E * Np + e * Np + i] * uu;
-        sB[(0 * Np + i) * BLD + e] = rx * F + ry * Gf + rz * W;
-        sB[(1 * Np + i) * BLD + e] = sx * F + sy * Gf + sz * W;
-        sB[(2 * Np + i) * BLD + e] = tx * F + ty * Gf + tz * W;
+        const int r0 = i, r1 = Np + i, r2 = 2 * Np + i;
+        sB[r0 * BLD + C::bcol(r0, e)] = rx * F + ry * Gf + rz * W;
+        sB[r1 * BLD + C::bcol(r1, e)] = sx * F + sy * Gf + sz * W;
+        sB[r2 * BLD + C::bcol(r2, e)] = tx * F + ty * Gf + tz * W;
       }
     }
     for (int g = tid; g < (C::KVP - C::KV) * BLD; g += TC) sB[C::KV * BLD + g] = 0.0;
-    consumer_sync(TC);
 
-    // 2. volume contraction
-    if constexpr (C::M16) {
+    // 2. volume contraction (FUSE: part of the one pass after the face fluxes)
+    if constexpr (!C::FUSE) consumer_sync(TC);
+    if constexpr (C::FUSE) {
+    } else if constexpr (C::M16) {
 #pragma unroll
       for (int i = 0; i < QM; i++)
 #pragma unroll
@@ -340,30 +412,14 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
                            tot16, warp, lane);
     } else {
 #pragma unroll
-    for (int i = 0; i < C::WM; i++)
+      for (int i = 0; i < C::WM; i++)
 #pragma unroll
-      for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
-      const int m0 = mg * C::WM, n0 = ng * C::WN;
-      const double *Ab = Afrag + (long)m0 * 32 + lane;
-      const double *Bb = sB + (lane & 3) * BLD + n0 * 8 + (lane >> 2);
-#pragma unroll 2
-      for (int ks = 0; ks < C::KVP / 4; ks++) {
-        double av[C::WM], bv[C::WN];
-#pragma unroll
-        for (int i = 0; i < C::WM; i++)
-          av[i] = (m0 + i < C::MT) ? Ab[((long)ks * C::MT + i) * 32] : 0.0;
-#pragma unroll
-        for (int j = 0; j < C::WN; j++) bv[j] = Bb[ks * 4 * BLD + j * 8];
-#pragma unroll
-        for (int i = 0; i < C::WM; i++)
-#pragma unroll
-          for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
-      }
+        for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+      dmma_phase(0, C::KVP / 4);
     }
-    consumer_sync(TC);
+    if constexpr (!C::FUSE) consumer_sync(TC);
 
-    // 3. face fluxes -> sB rows [0, NFF)
+    // 3. face fluxes -> sB rows [FR0, FR0 + NFF)
     for (int itm = tid; itm < E * NFF; itm += TC) {
       const int fj = itm / E, e = itm - fj * E, f = fj / Nfp;
       const int nodeM = sFm[fj];
@@ -376,48 +432,41 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           qm[v] = bU[v * E * Np + e * Np + nodeM];
-          qb[v] = 0.5 * (qm[v] + bUP[(v * NFF + fj) * E + e]);
+          qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
         }
         euler_flux_fast(a.gamma, qb, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];
-          sB[fj * BLD + v * E + e] = (nd - tau * (qb[v] - qm[v])) * fs;
+          const int r = C::FR0 + fj;
+          sB[r * BLD + C::bcol(r, v * E + e)] = (nd - tau * (qb[v] - qm[v])) * fs;
         }
       } else {
         const double um = bU[e * Np + nodeM];
-        const double ub = 0.5 * (um + bUP[fj * E + e]);
+        const double ub = 0.5 * (um + bUP[e * C::UPS + fj]);
         const double F = bV[e * Np + nodeM] * ub, Gf = bV[E * Np + e * Np + nodeM] * ub,
                      W = bV[2 * E * Np + e * Np + nodeM] * ub;
         const double nd = nx * F + ny * Gf + nz * W;
-        sB[fj * BLD + e] = (nd - tau * (ub - um)) * fs;
+        const int r = C::FR0 + fj;
+        sB[r * BLD + C::bcol(r, e)] = (nd - tau * (ub - um)) * fs;
       }
     }
-    for (int g = tid; g < (C::KFP - C::KF) * BLD; g += TC) sB[C::KF * BLD + g] = 0.0;
+    for (int g = tid; g < (C::KFP - C::KF) * BLD; g += TC)
+      sB[(C::FR0 + C::KF) * BLD + g] = 0.0;
     consumer_sync(TC);
 
-    // 4. lift contraction
-    if constexpr (C::M16) {
+    // 4. lift contraction (FUSE: the whole stacked contraction)
+    if constexpr (C::FUSE) {
+#pragma unroll
+      for (int i = 0; i < C::WM; i++)
+#pragma unroll
+        for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+      dmma_phase(0, C::KVP / 4 + C::KFP / 4);
+    } else if constexpr (C::M16) {
       contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), C::KSV16, C::KSF16, sB,
                            acc16, tot16, warp, lane);
     } else {
-      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
-      const int m0 = mg * C::WM, n0 = ng * C::WN;
-      const double *Ab = Afrag + ((long)(C::KVP / 4) * C::MT + m0) * 32 + lane;
-      const double *Bb = sB + (lane & 3) * BLD + n0 * 8 + (lane >> 2);
-#pragma unroll 2
-      for (int ks = 0; ks < C::KFP / 4; ks++) {
-        double av[C::WM], bv[C::WN];
-#pragma unroll
-        for (int i = 0; i < C::WM; i++)
-          av[i] = (m0 + i < C::MT) ? Ab[((long)ks * C::MT + i) * 32] : 0.0;
-#pragma unroll
-        for (int j = 0; j < C::WN; j++) bv[j] = Bb[ks * 4 * BLD + j * 8];
-#pragma unroll
-        for (int i = 0; i < C::WM; i++)
-#pragma unroll
-          for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
-      }
+      dmma_phase((long)(C::KVP / 4) * C::MT * 32, C::KFP / 4);
     }
     consumer_sync(TC);
 
@@ -439,18 +488,18 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
           }
       }
     } else {
-      const int mg = warp % C::MGROUPS, ng = warp / C::MGROUPS;
+      double *sR = sB + kc * C::S_R;   // this warp's k-chunk partial
 #pragma unroll
       for (int ii = 0; ii < C::WM; ii++) {
-        const int i = (mg * C::WM + ii) * 8 + (lane >> 2);
+        const int i = (m0 + ii) * 8 + (lane >> 2);
         if (i < Np) {
 #pragma unroll
           for (int jj = 0; jj < C::WN; jj++)
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-              const int col = (ng * C::WN + jj) * 8 + (lane & 3) * 2 + h;
+              const int col = (n0 + jj) * 8 + (lane & 3) * 2 + h;
               const int v = col / E, e = col - v * E;
-              sB[(v * Np + i) * EP + e] = acc[ii][jj][h];
+              sR[(v * Np + i) * EP + e] = acc[ii][jj][h];
             }
         }
       }
@@ -464,7 +513,9 @@ __global__ void __launch_bounds__(PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_>::
       const int v = vg / (ne * Np), g = vg - v * (ne * Np);
       const int e = g / Np, i = g - e * Np;
       const long gi = v * vs + e0 * Np + g;
-      const double rhs = sB[(v * Np + i) * EP + e];
+      double rhs = sB[(v * Np + i) * EP + e];
+#pragma unroll
+      for (int c = 1; c < C::KSP; c++) rhs += sB[c * C::S_R + (v * Np + i) * EP + e];
       if (a.rhs_only) {
         a.u_out[gi] = rhs;
       } else {
