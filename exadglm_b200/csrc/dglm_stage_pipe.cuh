@@ -150,17 +150,23 @@ struct PCfg {
   static constexpr int BLD = M16 ? NCOL + 4 : NCOL + (24 - NCOL % 16) % 16;
   static constexpr int BROWS = FUSE ? KVP + KFP : KVP > KFP ? KVP : KFP;
   static constexpr int FR0 = FUSE ? KVP : 0;             // first face-flux row
-  // neighbour traces [v][e][UPS]: consecutive gathers write consecutive
-  // words, and face-flux reads (8 elements x 2 face nodes, or 16 elements)
-  // land on distinct bank pairs
-  static constexpr int UPS = E >= 16 ? NFF + 1 : NFF + 2;
+  // neighbour traces [v][e][UPS] with UPS = 4 (mod 8): the face-flux
+  // threads take 4 elements x 4 face nodes per half-warp, whose trace reads
+  // (e * UPS + fj), face-data reads (e * 4 + f) and stores to four
+  // consecutive contraction rows all land on distinct bank pairs; the
+  // gathers write consecutive words
+  static constexpr int UPS = NFF % 8 == 4 ? NFF : NFF + 4;
   // shared memory segments, in doubles (operator A fragments when ASMEM)
   static constexpr int S_AF = !ASMEM ? 0 : M16 ? KST16 * MT16 * NPARTS16 * 64 : KS * MT * 32;
   static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * E * UPS;
   static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
-  static constexpr int S_R = NV * Np * EP;              // one rhs (partial) [v][i][EP]
+  // one rhs (partial) [v][e][IP], IP = 2 (mod 4): accumulator stores (4 rows
+  // x 4 column pairs per half-warp) and the epilogue's node-contiguous reads
+  // are free of bank conflicts
+  static constexpr int IP = Np + (6 - Np % 4) % 4;
+  static constexpr int S_R = NV * E * IP;
   static constexpr int S_B = BROWS * BLD > KSP * S_R ? BROWS * BLD : KSP * S_R;
   // barriers: full[NB], empty[NB], the operator-image barrier, padding
   static constexpr int NBAR = 2 * NB + 2 > 8 ? 2 * NB + 2 : 8;
@@ -181,6 +187,7 @@ struct PCfg {
   static_assert(!(M16 && ASMEM), "mma.sync operator fragments are read from global memory");
   static_assert(PHYS != EUL || S_B >= 8 * E * Nfp, "wave-speed terms reuse the rhs buffer");
   static_assert(S_UP % 2 == 0, "segments after the traces stay 16-byte aligned");
+  static_assert(E % 4 == 0 && NFF % 4 == 0, "face-flux threads in 4 x 4 blocks");
   __device__ static __forceinline__ int bcol(int row, int col) {
     return SWZ ? col ^ (((row >> 1) & 1) << 2) : col;
   }
@@ -268,7 +275,7 @@ __global__ void __launch_bounds__(
     PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_>::THREADS, 1)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
   using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_>;
-  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E,
                 BLD = C::BLD, TC = C::TC;
   extern __shared__ __align__(16) double smem[];
   double *sAF = smem;
@@ -421,7 +428,9 @@ __global__ void __launch_bounds__(
 
     // 3. face fluxes -> sB rows [FR0, FR0 + NFF)
     for (int itm = tid; itm < E * NFF; itm += TC) {
-      const int fj = itm / E, e = itm - fj * E, f = fj / Nfp;
+      // 4 x 4 blocks of (element, face node), element blocks fastest
+      const int blk = itm >> 4, eb = blk % (E / 4), fb = blk / (E / 4);
+      const int e = eb * 4 + (itm & 3), fj = fb * 4 + ((itm >> 2) & 3), f = fj / Nfp;
       const int nodeM = sFm[fj];
       // face arrays arrive in their global order: [array][e][f]
       const double nx = bF[0 * 4 * E + e * 4 + f], ny = bF[1 * 4 * E + e * 4 + f],
@@ -470,7 +479,7 @@ __global__ void __launch_bounds__(
     }
     consumer_sync(TC);
 
-    // 5. epilogue: rhs -> sB as [v][i][EP], then the coalesced LSERK update
+    // 5. epilogue: rhs -> sB as [v][e][IP], then the coalesced LSERK update
     if constexpr (C::M16) {
       const int mg = warp % C::MG16, ng = warp / C::MG16;
       const int g = lane >> 2, t = lane & 3;
@@ -484,7 +493,7 @@ __global__ void __launch_bounds__(
             const int i = (mg * C::WM16 + ii) * 16 + g + (c >= 2 ? 8 : 0);
             const int col = (ng * C::WN + jj) * 8 + 2 * t + (c & 1);
             const int v = col / E, e = col - v * E;
-            if (i < Np) sB[(v * Np + i) * EP + e] = tot16[ii][jj][c];
+            if (i < Np) sB[(v * E + e) * C::IP + i] = tot16[ii][jj][c];
           }
       }
     } else {
@@ -499,7 +508,7 @@ __global__ void __launch_bounds__(
             for (int h = 0; h < 2; h++) {
               const int col = (n0 + jj) * 8 + (lane & 3) * 2 + h;
               const int v = col / E, e = col - v * E;
-              sR[(v * Np + i) * EP + e] = acc[ii][jj][h];
+              sR[(v * E + e) * C::IP + i] = acc[ii][jj][h];
             }
         }
       }
@@ -513,9 +522,10 @@ __global__ void __launch_bounds__(
       const int v = vg / (ne * Np), g = vg - v * (ne * Np);
       const int e = g / Np, i = g - e * Np;
       const long gi = v * vs + e0 * Np + g;
-      double rhs = sB[(v * Np + i) * EP + e];
+      const int ri = (v * E + e) * C::IP + i;
+      double rhs = sB[ri];
 #pragma unroll
-      for (int c = 1; c < C::KSP; c++) rhs += sB[c * C::S_R + (v * Np + i) * EP + e];
+      for (int c = 1; c < C::KSP; c++) rhs += sB[c * C::S_R + ri];
       if (a.rhs_only) {
         a.u_out[gi] = rhs;
       } else {
