@@ -64,6 +64,7 @@ struct AdjArgs {
   double *lam, *lk;      // adjoints of u and k (updated in place, own tile only)
   const double *phi_in;  // phi of this stage, nvar x vsF
   double *phi_out;       // phi of the next stage in reverse order
+  double *fw;            // face terms of this stage (split variants), nvar x vsF
   long vs, vsF, gstride;
   int K;
   double gamma, dt, rka, rkb, rkb_next;
@@ -385,7 +386,56 @@ __device__ __forceinline__ void adj_dmma(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
-template <int PHYS, int N, int E_, int MG_>
+// Face terms of the adjoint stage, one thread per face point p = e NFF + fj
+// (the face loop of the fused kernels, split out so that its gathers -- the
+// partner trace u[vmapP], phi at p and at the partner point mapP[p], and the
+// partner face's normal, fscale and tau -- run at full occupancy):
+//   w = 1/2 (fs tau g1 - fs2 tau2 g2) + 1/2 fs A_n(qb)^T g1 + 1/2 fs2 A_n2(qb)^T g2
+// with qb the face average of the stage state and g1, g2 = phi at p, mapP[p]
+// (Euler); the upwind-flux transpose for advection.  Output fw[v vsF + p].
+template <int PHYS, int N>
+__global__ void __launch_bounds__(256) adjoint_face_kernel(const AdjArgs a) {
+  constexpr int NV = PHYS == A_EUL ? 5 : 1;
+  constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (p >= (long)a.K * NFF) return;
+  const long e = p / NFF;
+  const int fj = (int)(p - e * NFF), f = fj / Nfp;
+  const long vs = a.vs, vsF = a.vsF, gs = a.gstride;
+  const long gf = e * 4 + f, gf2 = __ldg(a.vmapF + gf);
+  const long iP = __ldg(a.vmapP + p), p2 = __ldg(a.mapP + p);
+  const long nM = e * Np + __ldg(a.Fmask + fj);
+  const double nx = __ldg(a.nrm + gf), ny = __ldg(a.nrm + 4 * gs + gf),
+               nz = __ldg(a.nrm + 8 * gs + gf), fs = __ldg(a.fscale + gf), ta = __ldg(a.tau + gf);
+  const double nx2 = __ldg(a.nrm + gf2), ny2 = __ldg(a.nrm + 4 * gs + gf2),
+               nz2 = __ldg(a.nrm + 8 * gs + gf2), fs2 = __ldg(a.fscale + gf2),
+               ta2 = __ldg(a.tau + gf2);
+  if (PHYS == A_EUL) {
+    double qb[5], g1[5], g2[5], w[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      qb[v] = 0.5 * (__ldg(a.u + v * vs + nM) + __ldg(a.u + v * vs + iP));
+      g1[v] = a.phi_in[v * vsF + p];
+      g2[v] = a.phi_in[v * vsF + p2];
+      w[v] = 0.5 * (fs * ta * g1[v] - fs2 * ta2 * g2[v]);
+    }
+    const JacPre P = jac_pre(a.gamma, qb);
+    jac_t_add(P, a.gamma, nx, ny, nz, g1, 0.5 * fs, w);
+    jac_t_add(P, a.gamma, nx2, ny2, nz2, g2, 0.5 * fs2, w);
+#pragma unroll
+    for (int v = 0; v < 5; v++) a.fw[v * vsF + p] = w[v];
+  } else {
+    const double an = nx * __ldg(a.vel + nM) + ny * __ldg(a.vel + vs + nM) +
+                      nz * __ldg(a.vel + 2 * vs + nM);
+    const double an2 = nx2 * __ldg(a.vel + iP) + ny2 * __ldg(a.vel + vs + iP) +
+                       nz2 * __ldg(a.vel + 2 * vs + iP);
+    const double g1 = a.phi_in[p], g2 = a.phi_in[p2];
+    a.fw[p] = fs * (0.5 * an + 0.5 * ta) * g1 + fs2 * (0.5 * an2 - 0.5 * ta2) * g2;
+  }
+  (void)NV;
+}
+
+template <int PHYS, int N, int E_, int MG_, bool SPLIT_ = false>
 struct DCfg {
   static constexpr int NV = PHYS == A_EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -395,36 +445,52 @@ struct DCfg {
   static constexpr int MG = MG_;
   static constexpr int WMV = (MTV + MG - 1) / MG, WML = (MTL + MG - 1) / MG;
   static constexpr int WARPS = NT * MG, T = 32 * WARPS;
-  static constexpr int BLD = NCOL + 4;
+  // mu rows [k][BLD]: stride 8 (mod 16) doubles with column bit 2 flipped on
+  // rows whose bit 1 is set (bcol), so that the m8n8k4 B-fragment loads and
+  // stores to two neighbouring rows by a half-warp hit distinct bank pairs
+  static constexpr int BLD = NCOL + (24 - NCOL % 16) % 16;
   static constexpr int VMLD = NFF + 1;
   static constexpr int ROWS = 8 * (MTV > MTL ? MTV : MTL);
-  static constexpr int S_U = NV * Np * EP, S_B = KP * BLD, S_OUT = ROWS * NV * EP,
-                       S_FC = NV * NFF * EP;
+  // per-(variable, element) rows with a stride of 2 (mod 4) doubles: node-
+  // contiguous accesses, accesses by 8 elements x 2 nodes and the DMMA result
+  // stores (4 rows x 4 column pairs) are all free of bank conflicts
+  static constexpr int pad2(int n) { return n + (6 - n % 4) % 4; }
+  static constexpr int IP = pad2(Np), RLD = pad2(ROWS), FRL = pad2(NFF);
+  // SPLIT: the face terms come from adjoint_face_kernel through global
+  // memory; no face buffers, face data or face-point maps in shared memory
+  static constexpr bool SPLIT = SPLIT_;
+  static constexpr int S_U = NV * E * IP, S_B = KP * BLD, S_OUT = NV * E * RLD,
+                       S_FC = SPLIT ? 0 : NV * E * FRL, S_FACE = SPLIT ? 0 : 40 * E,
+                       S_MAPS = SPLIT ? 0 : 2 * E * VMLD;
   static constexpr size_t SMEM =
-      sizeof(double) * (2 * S_U + S_B + S_OUT + S_FC + 9 * E + 40 * E) +
-      sizeof(int) * (2 * E * VMLD + NFF + 4 * Np);
+      sizeof(double) * (2 * S_U + S_B + S_OUT + S_FC + 9 * E + S_FACE) +
+      sizeof(int) * (S_MAPS + NFF + 4 * Np);
   static constexpr int AFV = KS * MTV * 32, AFL = KS * MTL * 32;   // fragment doubles
   static_assert(NCOL % 8 == 0, "columns must fill whole n-tiles");
   static_assert(T <= 1024, "block too large");
+  static_assert(S_OUT >= S_U, "mu staging reuses the result buffer");
+  __device__ static __forceinline__ int bcol(int row, int col) {
+    return col ^ (((row >> 1) & 1) << 2);
+  }
 };
 
-template <int PHYS, int N, int E_, int MG_, int MINB>
-__global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
+template <int PHYS, int N, int E_, int MG_, int MINB, bool SPLIT>
+__global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_, SPLIT>::T, MINB)
     adjoint_dmma_kernel(const AdjArgs a) {
-  using C = DCfg<PHYS, N, E_, MG_>;
-  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
+  using C = DCfg<PHYS, N, E_, MG_, SPLIT>;
+  constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E,
                 BLD = C::BLD, T = C::T, VMLD = C::VMLD, KP = C::KP;
   extern __shared__ __align__(16) double smem[];
-  double *sU = smem;                   // [v][i][EP] stage state, later lk'
-  double *sLam = sU + C::S_U;          // [v][i][EP]
-  double *sB = sLam + C::S_U;          // [k][BLD] mu, col = v*E + e
-  double *sOut = sB + C::S_B;          // [row][v][EP] contraction results
-  double *sFc = sOut + C::S_OUT;       // [v][fj][EP] face terms
+  double *sU = smem;                   // [v][e][IP] stage state, later lk'
+  double *sLam = sU + C::S_U;          // [v][e][IP]
+  double *sB = sLam + C::S_U;          // [k][BLD] mu, col = v*E + e (swizzled)
+  double *sOut = sB + C::S_B;          // [v][e][RLD] contraction results by row
+  double *sFc = sOut + C::S_OUT;       // [v][e][FRL] face terms
   double *sGeo = sFc + C::S_FC;        // [9][E]
   double *sFace = sGeo + 9 * E;        // [10][4][E]
-  int *sVm = reinterpret_cast<int *>(sFace + 40 * E);
-  int *sMp = sVm + E * VMLD;
-  int *sFm = sMp + E * VMLD;
+  int *sVm = reinterpret_cast<int *>(sFace + C::S_FACE);
+  int *sMp = sVm + C::S_MAPS / 2;
+  int *sFm = sVm + C::S_MAPS;
   int *sNF = sFm + NFF;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -448,20 +514,26 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
     for (int g = tid; g < E * Np; g += T) {
       const int e = g / Np, i = g - e * Np;
       const bool ok = g < ne * Np;
-      const double lam = ok ? a.lam[base + g] : 0.0;
-      const double lk = ok ? a.lk[base + g] : 0.0;
-      sLam[(v * Np + i) * EP + e] = lam;
-      sB[i * BLD + v * E + e] = lk + bm * lam;
-      if (upd) sU[(v * Np + i) * EP + e] = ok ? __ldg(a.u + base + g) : (v == 0 ? 1.0 : 0.0);
+      const int s = (v * E + e) * C::IP + i;
+      sLam[s] = ok ? a.lam[base + g] : 0.0;
+      sOut[s] = ok ? a.lk[base + g] : 0.0;   // lk, until mu is formed below
+      if (upd) sU[s] = ok ? __ldg(a.u + base + g) : (v == 0 ? 1.0 : 0.0);
     }
   }
   for (int g = tid; g < (KP - Np) * BLD; g += T) sB[Np * BLD + g] = 0.0;
+  __syncthreads();
+  // mu = lk + b lam -> sB; a half-warp takes 8 elements x 2 nodes
+  for (int g = tid; g < NV * Np * E; g += T) {
+    const int e = g % E, r = g / E, i = r % Np, v = r / Np;
+    const int s = (v * E + e) * C::IP + i;
+    sB[i * BLD + C::bcol(i, v * E + e)] = sOut[s] + bm * sLam[s];
+  }
   if (upd) {
     for (int g = tid; g < 9 * E; g += T) {
       const int m = g / E, e = g - m * E;
       sGeo[g] = e < ne ? __ldg(a.geo + (long)m * a.gstride + e0 + e) : 0.0;
     }
-    for (int g = tid; g < 4 * E; g += T) {
+    for (int g = tid; g < (SPLIT ? 0 : 4 * E); g += T) {
       const int e = g >> 2, f = g & 3;
       const bool ok = e < ne;
       const long gf = (e0 + e) * 4 + f;
@@ -478,7 +550,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
       sFace[(8 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf2) : 0.0;
       sFace[(9 * 4 + f) * E + e] = ok ? __ldg(a.tau + gf2) : 0.0;
     }
-    for (int g = tid; g < E * NFF; g += T) {
+    for (int g = tid; g < (SPLIT ? 0 : E * NFF); g += T) {
       const int e = g / NFF, fj = g - e * NFF;
       const bool ok = g < ne * NFF;
       sVm[e * VMLD + fj] = ok ? __ldg(a.vmapP + e0 * NFF + g) : 0;
@@ -488,12 +560,12 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
   __syncthreads();
 
   if (upd) {
-    // ---- face terms -> sFc (as the SIMT variant) ----------------------------
-    for (int it = tid; it < E * NFF; it += T) {
+    // ---- face terms -> sFc (as the SIMT variant; SPLIT: adjoint_face_kernel)
+    for (int it = tid; it < (SPLIT ? 0 : E * NFF); it += T) {
       const int e = it / NFF, fj = it - e * NFF, f = fj / Nfp;
       if (e >= ne) {
 #pragma unroll
-        for (int v = 0; v < NV; v++) sFc[(v * NFF + fj) * EP + e] = 0.0;
+        for (int v = 0; v < NV; v++) sFc[(v * E + e) * C::FRL + fj] = 0.0;
         continue;
       }
       const long p = (e0 + e) * NFF + fj;
@@ -507,7 +579,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
         double qb[5], g1[5], g2[5], w[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          qb[v] = 0.5 * (sU[(v * Np + nodeM) * EP + e] + __ldg(a.u + v * vs + iP));
+          qb[v] = 0.5 * (sU[(v * E + e) * C::IP + nodeM] + __ldg(a.u + v * vs + iP));
           g1[v] = a.phi_in[v * vsF + p];
           g2[v] = a.phi_in[v * vsF + p2];
           w[v] = 0.5 * (fs * ta * g1[v] - fs2 * ta2 * g2[v]);
@@ -516,7 +588,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
         jac_t_add(P, a.gamma, nx, ny, nz, g1, 0.5 * fs, w);
         jac_t_add(P, a.gamma, nx2, ny2, nz2, g2, 0.5 * fs2, w);
 #pragma unroll
-        for (int v = 0; v < 5; v++) sFc[(v * NFF + fj) * EP + e] = w[v];
+        for (int v = 0; v < 5; v++) sFc[(v * E + e) * C::FRL + fj] = w[v];
       } else {
         const long nM = (e0 + e) * Np + nodeM;
         const double an = nx * __ldg(a.vel + nM) + ny * __ldg(a.vel + vs + nM) +
@@ -524,7 +596,8 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
         const double an2 = nx2 * __ldg(a.vel + iP) + ny2 * __ldg(a.vel + vs + iP) +
                            nz2 * __ldg(a.vel + 2 * vs + iP);
         const double g1 = a.phi_in[p], g2 = a.phi_in[p2];
-        sFc[fj * EP + e] = fs * (0.5 * an + 0.5 * ta) * g1 + fs2 * (0.5 * an2 - 0.5 * ta2) * g2;
+        sFc[e * C::FRL + fj] =
+            fs * (0.5 * an + 0.5 * ta) * g1 + fs2 * (0.5 * an2 - 0.5 * ta2) * g2;
       }
     }
 
@@ -534,7 +607,8 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
     for (int i = 0; i < C::WMV; i++) acc[i][0] = acc[i][1] = 0.0;
     const int m0 = mg * C::WMV;
     const double *Ab = a.AV + (long)m0 * 32 + lane;
-    const double *Bb = sB + (lane & 3) * BLD + ng * 8 + (lane >> 2);
+    // rows k0 + (lane & 3), k0 % 4 == 0: the swizzle bit is lane bit 1
+    const double *Bb = sB + (lane & 3) * BLD + ng * 8 + C::bcol(lane & 3, lane >> 2);
 #pragma unroll 3
     for (int ks = 0; ks < C::KS; ks++) {
       const double bv = Bb[ks * 4 * BLD];
@@ -550,7 +624,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int col = ng * 8 + (lane & 3) * 2 + h, v = col / E, e = col - v * E;
-          sOut[(row * NV + v) * EP + e] = acc[i][h];
+          sOut[(v * E + e) * C::RLD + row] = acc[i][h];
         }
       }
     }
@@ -569,12 +643,12 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
 #pragma unroll
       for (int d = 0; d < 3; d++)
 #pragma unroll
-        for (int v = 0; v < NV; v++) nu[d][v] = sOut[((d * Np + j) * NV + v) * EP + e];
+        for (int v = 0; v < NV; v++) nu[d][v] = sOut[(v * E + e) * C::RLD + d * Np + j];
       JacPre P;
       if (PHYS == A_EUL) {
         double q[5];
 #pragma unroll
-        for (int v = 0; v < 5; v++) q[v] = sU[(v * Np + j) * EP + e];
+        for (int v = 0; v < 5; v++) q[v] = sU[(v * E + e) * C::IP + j];
         P = jac_pre(a.gamma, q);
       }
 #pragma unroll
@@ -594,18 +668,25 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
       for (int c = 0; c < 4; c++) {
         const int fj = sNF[j * 4 + c];
         if (fj < 0) break;
+        if constexpr (SPLIT) {
+          if (e < ne) {
 #pragma unroll
-        for (int v = 0; v < NV; v++) w[v] += sFc[(v * NFF + fj) * EP + e];
+            for (int v = 0; v < NV; v++) w[v] += a.fw[v * vsF + (e0 + e) * NFF + fj];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; v++) w[v] += sFc[(v * E + e) * C::FRL + fj];
+        }
       }
 #pragma unroll
       for (int v = 0; v < NV; v++) {
-        const int s = (v * Np + j) * EP + e;
-        const double mu = sB[j * BLD + v * E + e];
+        const int s = (v * E + e) * C::IP + j, bi = j * BLD + C::bcol(j, v * E + e);
+        const double mu = sB[bi];
         const double lamn = sLam[s] + a.dt * w[v];
         const double lkn = a.rka * mu;
         sLam[s] = lamn;
         sU[s] = lkn;
-        sB[j * BLD + v * E + e] = lkn + a.rkb_next * lamn;
+        sB[bi] = lkn + a.rkb_next * lamn;
       }
     }
     __syncthreads();
@@ -618,7 +699,8 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
     for (int i = 0; i < C::WML; i++) acc[i][0] = acc[i][1] = 0.0;
     const int m0 = mg * C::WML;
     const double *Ab = a.AL + (long)m0 * 32 + lane;
-    const double *Bb = sB + (lane & 3) * BLD + ng * 8 + (lane >> 2);
+    // rows k0 + (lane & 3), k0 % 4 == 0: the swizzle bit is lane bit 1
+    const double *Bb = sB + (lane & 3) * BLD + ng * 8 + C::bcol(lane & 3, lane >> 2);
 #pragma unroll 3
     for (int ks = 0; ks < C::KS; ks++) {
       const double bv = Bb[ks * 4 * BLD];
@@ -633,7 +715,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int col = ng * 8 + (lane & 3) * 2 + h, v = col / E, e = col - v * E;
-          sOut[(row * NV + v) * EP + e] = acc[i][h];
+          sOut[(v * E + e) * C::RLD + row] = acc[i][h];
         }
       }
     }
@@ -642,7 +724,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
       const long base = v * vsF + e0 * NFF;
       for (int g = tid; g < ne * NFF; g += T) {
         const int e = g / NFF, fj = g - e * NFF;
-        a.phi_out[base + g] = sOut[(fj * NV + v) * EP + e];
+        a.phi_out[base + g] = sOut[(v * E + e) * C::RLD + fj];
       }
     }
   }
@@ -652,7 +734,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_>::T, MINB)
       const long base = v * vs + e0 * Np;
       for (int g = tid; g < ne * Np; g += T) {
         const int e = g / Np, i = g - e * Np;
-        const int s = (v * Np + i) * EP + e;
+        const int s = (v * E + e) * C::IP + i;
         a.lam[base + g] = sLam[s];
         a.lk[base + g] = sU[s];
       }
@@ -701,6 +783,7 @@ struct AdjVariant {
   int IPV, IPL;              // SIMT: padded rows of the k-major operators
   int MTV, MTL, KS;          // DMMA: m-tiles and k-steps of the fragments
   cudaError_t (*launch)(const AdjArgs &, cudaStream_t);
+  int split = 0;             // 1: face terms by adjoint_face_kernel into the tape's fw
 };
 
 template <int PHYS, int N, int E, int MINB>
@@ -725,7 +808,7 @@ AdjVariant adj_variant() {
 template <int PHYS, int N, int E, int MG, int MINB>
 cudaError_t launch_adj_dmma(const AdjArgs &a, cudaStream_t s) {
   using C = DCfg<PHYS, N, E, MG>;
-  auto k = adjoint_dmma_kernel<PHYS, N, E, MG, MINB>;
+  auto k = adjoint_dmma_kernel<PHYS, N, E, MG, MINB, false>;
   cudaError_t e =
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -741,6 +824,32 @@ AdjVariant adj_dmma_variant() {
                     launch_adj_dmma<PHYS, N, E, MG, MINB>};
 }
 
+// face-point kernel, then the DMMA kernel without face buffers
+template <int PHYS, int N, int E, int MG, int MINB>
+cudaError_t launch_adj_split(const AdjArgs &a, cudaStream_t s) {
+  using C = DCfg<PHYS, N, E, MG, true>;
+  if (a.update) {
+    const long n = (long)a.K * C::NFF;
+    adjoint_face_kernel<PHYS, N><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  auto k = adjoint_dmma_kernel<PHYS, N, E, MG, MINB, true>;
+  cudaError_t e =
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int blocks = (a.K + E - 1) / E;
+  k<<<blocks, C::T, C::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E, int MG, int MINB = 1>
+AdjVariant adj_split_variant() {
+  using C = DCfg<PHYS, N, E, MG, true>;
+  return AdjVariant{1, E, C::T, MINB, C::SMEM, 0, 0, C::MTV, C::MTL, C::KS,
+                    launch_adj_split<PHYS, N, E, MG, MINB>, 1};
+}
+
 // Tile shapes per (physics, N); the first is the default.
 const std::vector<AdjVariant> &adjoint_variants(int physics, int N) {
   static const std::vector<AdjVariant> none;
@@ -748,9 +857,9 @@ const std::vector<AdjVariant> &adjoint_variants(int physics, int N) {
       {adj_variant<A_EUL, 1, 16>()},
       {adj_variant<A_EUL, 2, 16>(), adj_dmma_variant<A_EUL, 2, 8, 1>()},
       {adj_variant<A_EUL, 3, 8>(), adj_dmma_variant<A_EUL, 3, 8, 2>()},
-      {adj_dmma_variant<A_EUL, 4, 8, 2, 2>(), adj_variant<A_EUL, 4, 4, 4>(),
-       adj_dmma_variant<A_EUL, 4, 8, 2>(), adj_dmma_variant<A_EUL, 4, 8, 3>(),
-       adj_variant<A_EUL, 4, 8, 3>()},
+      {adj_split_variant<A_EUL, 4, 8, 2, 3>(), adj_dmma_variant<A_EUL, 4, 8, 2, 2>(),
+       adj_variant<A_EUL, 4, 4, 4>(), adj_dmma_variant<A_EUL, 4, 8, 3>(),
+       adj_split_variant<A_EUL, 4, 8, 2, 2>()},
       {adj_variant<A_EUL, 5, 8>(), adj_dmma_variant<A_EUL, 5, 8, 2>()},
       {adj_variant<A_EUL, 6, 4>()}};
   static const std::vector<AdjVariant> adv[6] = {
@@ -784,6 +893,7 @@ struct AdjointTape {
   double *AV = nullptr, *AL = nullptr;
   int *mapP = nullptr, *bad = nullptr;
   double *lam = nullptr, *lk = nullptr, *phi[2] = {nullptr, nullptr}, *kbuf = nullptr;
+  double *fw = nullptr;      // face terms of one stage (split variants)
   double *dt_dev = nullptr;  // cap_steps
   double *tau = nullptr;     // cap_steps x 4Kp (Euler) or 4Kp (advection)
   double *ckpt = nullptr;    // cap_ckpt states
@@ -862,6 +972,7 @@ dglm_status tape_setup(dglm_handle *h) {
   chk(talloc(t, t->fixed, &t->kbuf, (size_t)t->state));
   chk(talloc(t, t->fixed, &t->phi[0], (size_t)h->nvar * t->vsF));
   chk(talloc(t, t->fixed, &t->phi[1], (size_t)h->nvar * t->vsF));
+  if (v.split) chk(talloc(t, t->fixed, &t->fw, (size_t)h->nvar * t->vsF));
   if (st != DGLM_OK) {
     free_tape(h);
     return st;
@@ -991,6 +1102,7 @@ AdjArgs adj_args(dglm_handle *h) {
   a.vel = h->vel;
   a.lam = t->lam;
   a.lk = t->lk;
+  a.fw = t->fw;
   a.vs = h->vs;
   a.vsF = t->vsF;
   a.gstride = h->Kp;
@@ -1252,7 +1364,7 @@ dglm_status dglm_adjoint_variant_describe(int physics, int N, int variant, char 
     return set_error(DGLM_ERR_INVALID, "dglm_adjoint_variant_describe: no such variant");
   const AdjVariant &v = vl[variant];
   snprintf(buf, len, "adjoint-%s E=%d threads=%d minblocks=%d smem=%zu",
-           v.kind == 0 ? "simt" : "dmma", v.E, v.T, v.minb, v.smem);
+           v.kind == 0 ? "simt" : v.split ? "dmma-split" : "dmma", v.E, v.T, v.minb, v.smem);
   return DGLM_OK;
 }
 

@@ -126,6 +126,7 @@ struct StageVariantInfo {
   int producers;   // PIPE: producer warps sharing the neighbour gathers (1 to 4)
   int ksplit;      // PIPE: k-chunks of the DMMA contraction summed in the epilogue
   int fused;       // PIPE: 1 = volume and lift contractions in one DMMA pass
+  int op_global;   // PIPE: 1 = operator fragments read through L1, not staged in shared memory
 };
 
 // fused FP64 stage launcher (dglm_stage_fp64.cu)

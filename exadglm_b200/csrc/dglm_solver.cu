@@ -753,10 +753,11 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
                                           : "tcgen05-bf16x3",
              v.E, v.npad, v.threads, v.smem);
   else {
-    const int n = snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu",
+    const int n = snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu%s",
                            v.mode == MODE_PIPE ? (v.groups == 2 ? "pipe2-dmma" : "pipe-dmma")
                                                : "dmma",
-                           v.E, v.CPT, v.WM, v.threads, v.smem);
+                           v.E, v.CPT, v.WM, v.threads, v.smem,
+                           v.mode == MODE_PIPE && v.op_global ? " A=global" : "");
     // ring depth, producer warps and k-split are named only when they differ
     // from 2, 1 and 1
     if (v.mode == MODE_PIPE && (v.ring > 2 || v.producers > 1 || v.ksplit > 1) && n > 0 &&

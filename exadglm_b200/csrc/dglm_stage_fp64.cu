@@ -765,6 +765,7 @@ static Variant make_pipe() {
   i.producers = PW;
   i.ksplit = KSP;
   i.fused = FU ? 1 : 0;
+  i.op_global = AS ? 0 : 1;
   if (PR) {
     i.prec = PR == 2 ? DGLM_PREC_TF32X3 : PR == 3 ? DGLM_PREC_BF16X6 : DGLM_PREC_BF16X3;
     i.kstep = C::KSTEP16;

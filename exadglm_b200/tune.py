@@ -11,6 +11,7 @@ reads to pick its default variant.
 from __future__ import annotations
 
 import json
+import re
 import os
 
 from . import capi
@@ -47,9 +48,17 @@ def cached_variant(physics, N, precision="fp64", device=0):
     ent = load_cache().get(_key(physics, N, precision, name))
     if ent is None:
         return None
-    # match by description: indices move when variants are added
-    descs = capi.variants(physics, N)
-    return descs.index(ent["desc"]) if ent["desc"] in descs else None
+    # match by description: indices move when variants are added; the
+    # shared-memory size is left out of the match, since layout changes move
+    # it without changing the tile shape
+    descs = [_shape(d) for d in capi.variants(physics, N)]
+    want = _shape(ent["desc"])
+    return descs.index(want) if want in descs else None
+
+
+def _shape(desc):
+    """A variant description without its smem=<bytes> field."""
+    return re.sub(r" smem=\d+", "", desc)
 
 
 def time_variants(solver, reps=25):

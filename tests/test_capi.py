@@ -45,6 +45,15 @@ def test_variants_are_described():
             assert capi.variants(phys, N, "fp64")
 
 
+def test_variant_shapes_are_unique_without_smem():
+    # the tuned table matches variants by description with smem=<bytes> left out
+    from exadglm_b200.tune import _shape
+    for phys in ("euler", "advection"):
+        for N in range(1, 9):
+            shapes = [_shape(d) for d in capi.variants(phys, N)]
+            assert len(set(shapes)) == len(shapes), (phys, N, shapes)
+
+
 def _desc(**kw):
     d = capi.Desc()
     d.N, d.physics, d.K, d.precision = 4, capi.EULER, 48, capi.PREC_FP64
