@@ -86,6 +86,23 @@ def test_mixed_steps_error(phys, N, prec):
     s.close()
 
 
+@pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "bf16x6"])
+@pytest.mark.parametrize("phys,N", CASES[:2])
+def test_every_mixed_variant_steps(phys, N, prec):
+    """Every tile shape of the mode through full steps (the LSERK epilogue
+    included, whether it reads the RK register from shared or global memory)."""
+    prob = make(phys, N)
+    uo, _, _, _ = oracle.Oracle(prob).run(5)
+    for v, desc in variants(phys, N, prec):
+        s = Solver(prob, precision=prec, variant=v)
+        s.step(5)
+        s.sync()
+        err = rel(s.get_state(), uo)
+        print(f"{desc}: 5 steps rel L2 {err:.3e}")
+        assert err < STATE_TOL[prec], (desc, err)
+        s.close()
+
+
 def test_variant_of_other_precision_is_rejected():
     from exadglm_b200.capi import DglmError
     prob = make("euler", 4)
