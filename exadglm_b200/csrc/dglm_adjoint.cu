@@ -474,7 +474,45 @@ struct DCfg {
   }
 };
 
-template <int PHYS, int N, int E_, int MG_, int MINB, bool SPLIT>
+// Transposed-operator contraction with every warp on all NT n-tiles: warp w
+// takes m-tiles w, w + WARPS, ... of the MTX m-tiles (A fragments [kstep]
+// [mtile][lane] from global memory, one load per k-step for NT DMMAs), the B
+// fragments come from the mu rows in shared memory; results for rows below
+// `rows` go to sOut[(v E + e) RLD + row].
+template <class C>
+__device__ __forceinline__ void adj_contract_all_n(const double *A, int MTX, int rows,
+                                                   const double *sB, double *sOut, int warp,
+                                                   int lane) {
+  constexpr int NT = C::NT, E = C::E;
+  // rows k0 + (lane & 3), k0 % 4 == 0: the swizzle bit is lane bit 1
+  const double *Bb = sB + (lane & 3) * C::BLD + C::bcol(lane & 3, lane >> 2);
+  for (int mt = warp; mt < MTX; mt += C::WARPS) {
+    double acc[NT][2];
+#pragma unroll
+    for (int j = 0; j < NT; j++) acc[j][0] = acc[j][1] = 0.0;
+    const double *Ab = A + (long)mt * 32 + lane;
+    double an = __ldg(Ab);
+#pragma unroll 3
+    for (int ks = 0; ks < C::KS; ks++) {
+      const double av = an;
+      if (ks + 1 < C::KS) an = __ldg(Ab + (long)(ks + 1) * MTX * 32);
+#pragma unroll
+      for (int j = 0; j < NT; j++) adj_dmma(acc[j], av, Bb[ks * 4 * C::BLD + j * 8]);
+    }
+    const int row = mt * 8 + (lane >> 2);
+    if (row < rows) {
+#pragma unroll
+      for (int j = 0; j < NT; j++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int col = j * 8 + (lane & 3) * 2 + h, v = col / E, e = col - v * E;
+          sOut[(v * E + e) * C::RLD + row] = acc[j][h];
+        }
+    }
+  }
+}
+
+template <int PHYS, int N, int E_, int MG_, int MINB, bool SPLIT, bool ALLN = false>
 __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_, SPLIT>::T, MINB)
     adjoint_dmma_kernel(const AdjArgs a) {
   using C = DCfg<PHYS, N, E_, MG_, SPLIT>;
@@ -602,6 +640,9 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_, SPLIT>::T, MINB)
     }
 
     // ---- nu = [WD^T] mu on the tensor cores --------------------------------
+    if constexpr (ALLN) {
+      adj_contract_all_n<C>(a.AV, C::MTV, 3 * Np, sB, sOut, warp, lane);
+    } else {
     double acc[C::WMV][2];
 #pragma unroll
     for (int i = 0; i < C::WMV; i++) acc[i][0] = acc[i][1] = 0.0;
@@ -627,6 +668,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_, SPLIT>::T, MINB)
           sOut[(v * E + e) * C::RLD + row] = acc[i][h];
         }
       }
+    }
     }
   }
   __syncthreads();
@@ -694,6 +736,9 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_, SPLIT>::T, MINB)
 
   if (a.phi_next) {
     // ---- phi' = -LIFT^T mu' on the tensor cores -> sOut[fj][v][e] -----------
+    if constexpr (ALLN) {
+      adj_contract_all_n<C>(a.AL, C::MTL, NFF, sB, sOut, warp, lane);
+    } else {
     double acc[C::WML][2];
 #pragma unroll
     for (int i = 0; i < C::WML; i++) acc[i][0] = acc[i][1] = 0.0;
@@ -718,6 +763,7 @@ __global__ void __launch_bounds__(DCfg<PHYS, N, E_, MG_, SPLIT>::T, MINB)
           sOut[(v * E + e) * C::RLD + row] = acc[i][h];
         }
       }
+    }
     }
     __syncthreads();
     for (int v = 0; v < NV; v++) {
@@ -783,7 +829,8 @@ struct AdjVariant {
   int IPV, IPL;              // SIMT: padded rows of the k-major operators
   int MTV, MTL, KS;          // DMMA: m-tiles and k-steps of the fragments
   cudaError_t (*launch)(const AdjArgs &, cudaStream_t);
-  int split = 0;             // 1: face terms by adjoint_face_kernel into the tape's fw
+  int split = 0;             // 1: face terms by adjoint_face_kernel into the tape's fw;
+                             // 2: the same, every warp on all n-tiles of the contractions
 };
 
 template <int PHYS, int N, int E, int MINB>
@@ -825,7 +872,7 @@ AdjVariant adj_dmma_variant() {
 }
 
 // face-point kernel, then the DMMA kernel without face buffers
-template <int PHYS, int N, int E, int MG, int MINB>
+template <int PHYS, int N, int E, int MG, int MINB, bool ALLN>
 cudaError_t launch_adj_split(const AdjArgs &a, cudaStream_t s) {
   using C = DCfg<PHYS, N, E, MG, true>;
   if (a.update) {
@@ -834,7 +881,7 @@ cudaError_t launch_adj_split(const AdjArgs &a, cudaStream_t s) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  auto k = adjoint_dmma_kernel<PHYS, N, E, MG, MINB, true>;
+  auto k = adjoint_dmma_kernel<PHYS, N, E, MG, MINB, true, ALLN>;
   cudaError_t e =
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -843,11 +890,11 @@ cudaError_t launch_adj_split(const AdjArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int MG, int MINB = 1>
+template <int PHYS, int N, int E, int MG, int MINB = 1, bool ALLN = false>
 AdjVariant adj_split_variant() {
   using C = DCfg<PHYS, N, E, MG, true>;
   return AdjVariant{1, E, C::T, MINB, C::SMEM, 0, 0, C::MTV, C::MTL, C::KS,
-                    launch_adj_split<PHYS, N, E, MG, MINB>, 1};
+                    launch_adj_split<PHYS, N, E, MG, MINB, ALLN>, ALLN ? 2 : 1};
 }
 
 // Tile shapes per (physics, N); the first is the default.
@@ -857,9 +904,10 @@ const std::vector<AdjVariant> &adjoint_variants(int physics, int N) {
       {adj_variant<A_EUL, 1, 16>()},
       {adj_variant<A_EUL, 2, 16>(), adj_dmma_variant<A_EUL, 2, 8, 1>()},
       {adj_variant<A_EUL, 3, 8>(), adj_dmma_variant<A_EUL, 3, 8, 2>()},
-      {adj_split_variant<A_EUL, 4, 8, 2, 3>(), adj_dmma_variant<A_EUL, 4, 8, 2, 2>(),
+      {adj_split_variant<A_EUL, 4, 8, 2, 3, true>(), adj_split_variant<A_EUL, 4, 8, 2, 3>(),
+       adj_dmma_variant<A_EUL, 4, 8, 2, 2>(),
        adj_variant<A_EUL, 4, 4, 4>(), adj_dmma_variant<A_EUL, 4, 8, 3>(),
-       adj_split_variant<A_EUL, 4, 8, 2, 2>()},
+       adj_split_variant<A_EUL, 4, 8, 2, 2>(), adj_split_variant<A_EUL, 4, 8, 2, 2, true>()},
       {adj_variant<A_EUL, 5, 8>(), adj_dmma_variant<A_EUL, 5, 8, 2>()},
       {adj_variant<A_EUL, 6, 4>()}};
   static const std::vector<AdjVariant> adv[6] = {
@@ -1364,7 +1412,11 @@ dglm_status dglm_adjoint_variant_describe(int physics, int N, int variant, char 
     return set_error(DGLM_ERR_INVALID, "dglm_adjoint_variant_describe: no such variant");
   const AdjVariant &v = vl[variant];
   snprintf(buf, len, "adjoint-%s E=%d threads=%d minblocks=%d smem=%zu",
-           v.kind == 0 ? "simt" : v.split ? "dmma-split" : "dmma", v.E, v.T, v.minb, v.smem);
+           v.kind == 0     ? "simt"
+           : v.split == 2  ? "dmma-split-alln"
+           : v.split       ? "dmma-split"
+                           : "dmma",
+           v.E, v.T, v.minb, v.smem);
   return DGLM_OK;
 }
 
