@@ -93,6 +93,24 @@ struct BT {
   static constexpr int KSTEPS = KVP / 4 + KFP / 4;   // A fragment k-steps
 };
 
+// 8- and 4-byte asynchronous global -> shared copies (all of a tile's staging
+// is issued before one wait)
+__device__ __forceinline__ void b_cp8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void b_cp4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void b_cp_wait() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 __device__ __forceinline__ void b_dmma(double (&d)[2], double a, double b) {
   asm volatile(
       "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -121,29 +139,52 @@ __device__ __forceinline__ void batch_tile(const BatchArgs &a, const BatchTile &
   const double *Afrag = a.ops[N];
   const double dt = a.sc[t.inst].dt;
 
-  for (int i = tid; i < NFF; i += T) sFm[i] = __ldg(a.Fmask[N] + i);
+  // this thread's RK register values for the update, fetched now so their
+  // latency overlaps the tile's work
+  constexpr int KPT = (E * Np + T - 1) / T;
+  double kr[KPT];
+#pragma unroll
+  for (int q = 0; q < KPT; q++) {
+    const int g = tid + q * T;
+    kr[q] = g < ne * Np ? a.kreg[nb + g] : 0.0;
+  }
+  // staging: every copy is issued before one wait; padding is zero-filled
+  for (int i = tid; i < NFF; i += T) b_cp4(sFm + i, a.Fmask[N] + i);
   for (int g = tid; g < E * Np; g += T) {
     const int e = g / Np, i = g - e * Np;
-    sU[i * EP + e] = g < ne * Np ? a.u_in[nb + g] : 0.0;
+    if (g < ne * Np)
+      b_cp8(sU + i * EP + e, a.u_in + nb + g);
+    else
+      sU[i * EP + e] = 0.0;
   }
   for (int g = tid; g < 9 * E; g += T) {
     const int m = g / E, e = g - m * E;
-    sGeo[g] = e < ne ? __ldg(a.geo + (long)m * a.gs + eg0 + e) : 0.0;
+    if (e < ne)
+      b_cp8(sGeo + g, a.geo + (long)m * a.gs + eg0 + e);
+    else
+      sGeo[g] = 0.0;
   }
   for (int g = tid; g < 4 * E; g += T) {
     const int e = g >> 2, f = g & 3;
-    const bool ok = e < ne;
     const long gf = (eg0 + e) * 4 + f;
-    sFace[(0 * 4 + f) * E + e] = ok ? __ldg(a.nrm + gf) : 0.0;
-    sFace[(1 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 4 * a.gs + gf) : 0.0;
-    sFace[(2 * 4 + f) * E + e] = ok ? __ldg(a.nrm + 8 * a.gs + gf) : 0.0;
-    sFace[(3 * 4 + f) * E + e] = ok ? __ldg(a.fscale + gf) : 0.0;
+    if (e < ne) {
+      b_cp8(sFace + (0 * 4 + f) * E + e, a.nrm + gf);
+      b_cp8(sFace + (1 * 4 + f) * E + e, a.nrm + 4 * a.gs + gf);
+      b_cp8(sFace + (2 * 4 + f) * E + e, a.nrm + 8 * a.gs + gf);
+      b_cp8(sFace + (3 * 4 + f) * E + e, a.fscale + gf);
+    } else {
+      for (int q = 0; q < 4; q++) sFace[(q * 4 + f) * E + e] = 0.0;
+    }
   }
   const long fp0 = I.fp_off + (long)t.e0 * NFF;
   for (int g = tid; g < E * NFF; g += T) {
     const int e = g / NFF, fj = g - e * NFF;
-    sVm[e * C::VMLD + fj] = g < ne * NFF ? __ldg(a.vmapP + fp0 + g) : 0;
+    if (g < ne * NFF)
+      b_cp4(sVm + e * C::VMLD + fj, a.vmapP + fp0 + g);
+    else
+      sVm[e * C::VMLD + fj] = 0;
   }
+  b_cp_wait();
   __syncthreads();
 
   // volume fluxes -> B rows [0, 3Np)
@@ -222,9 +263,12 @@ __device__ __forceinline__ void batch_tile(const BatchArgs &a, const BatchTile &
     }
   }
   __syncthreads();
-  for (int g = tid; g < ne * Np; g += T) {
+#pragma unroll
+  for (int q = 0; q < KPT; q++) {
+    const int g = tid + q * T;
+    if (g >= ne * Np) continue;
     const int e = g / Np, i = g - e * Np;
-    const double kn = a.rka * a.kreg[nb + g] + dt * sR[i * EP + e];
+    const double kn = a.rka * kr[q] + dt * sR[i * EP + e];
     a.kreg[nb + g] = kn;
     a.u_out[nb + g] = sU[i * EP + e] + a.rkb * kn;
   }
