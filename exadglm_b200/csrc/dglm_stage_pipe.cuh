@@ -359,20 +359,11 @@ __global__ void __launch_bounds__(
           for (int j = 0; j < C::WN; j++) dmma_8x8x4(acc[i][j], av[i], bv[j]);
     }
   };
-  int it = grp;
-  for (int t = blockIdx.x + grp * gridDim.x; ok && t < ntiles; t += C::NG * gridDim.x, it += C::NG) {
-    const int b = it % C::NB;
-    if (!consumer_all(mbar_wait(&full[b], (it / C::NB) & 1), TC)) {
-      ok = false;
-      break;
-    }
-    const long e0 = (long)t * E;
-    const int ne = (int)min((long)E, (long)a.K - e0);
-    double *B = buf(b);
-    double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
-    double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
-
-    // 1. volume fluxes -> sB rows [0, 3Np), zero padding rows
+  // phase bodies shared by the tile orders below
+  // volume fluxes of the tile in ring buffer B -> operand rows [0, 3Np)
+  auto vol_flux = [&](double *B) {
+    const double *bU = B, *bG = B + C::S_U + C::S_K + C::S_UP;
+    const double *bV = bG + C::S_GEO + C::S_FACE;
     for (int itm = tid; itm < E * Np; itm += TC) {
       const int i = itm / E, e = itm - i * E;
       const double *g = bG + e;
@@ -402,31 +393,11 @@ __global__ void __launch_bounds__(
     }
     for (int g = tid; g < (C::KVP - C::KV) * BLD; g += TC) sB[C::KV * BLD + g] = 0.0;
 
-    // 2. volume contraction (FUSE: part of the one pass after the face fluxes)
-    if constexpr (!C::FUSE) consumer_sync(TC);
-    if constexpr (C::FUSE) {
-    } else if constexpr (C::M16) {
-#pragma unroll
-      for (int i = 0; i < QM; i++)
-#pragma unroll
-        for (int j = 0; j < QN; j++)
-#pragma unroll
-          for (int c = 0; c < 4; c++) {
-            acc16[i][j][c] = 0.f;
-            tot16[i][j][c] = 0.0;
-          }
-      contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), 0, C::KSV16, sB, acc16,
-                           tot16, warp, lane);
-    } else {
-#pragma unroll
-      for (int i = 0; i < C::WM; i++)
-#pragma unroll
-        for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-      dmma_phase(0, C::KVP / 4);
-    }
-    if constexpr (!C::FUSE) consumer_sync(TC);
-
-    // 3. face fluxes -> sB rows [FR0, FR0 + NFF)
+  };
+  // face fluxes of the tile in ring buffer B -> operand rows [FR0, FR0 + NFF)
+  auto face_flux = [&](double *B) {
+    const double *bU = B, *bUP = B + C::S_U + C::S_K, *bF = bUP + C::S_UP + C::S_GEO;
+    const double *bV = bF + C::S_FACE;
     for (int itm = tid; itm < E * NFF; itm += TC) {
       // 4 x 4 blocks of (element, face node), element blocks fastest
       const int blk = itm >> 4, eb = blk % (E / 4), fb = blk / (E / 4);
@@ -462,24 +433,9 @@ __global__ void __launch_bounds__(
     }
     for (int g = tid; g < (C::KFP - C::KF) * BLD; g += TC)
       sB[(C::FR0 + C::KF) * BLD + g] = 0.0;
-    consumer_sync(TC);
-
-    // 4. lift contraction (FUSE: the whole stacked contraction)
-    if constexpr (C::FUSE) {
-#pragma unroll
-      for (int i = 0; i < C::WM; i++)
-#pragma unroll
-        for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-      dmma_phase(0, C::KVP / 4 + C::KFP / 4);
-    } else if constexpr (C::M16) {
-      contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), C::KSV16, C::KSF16, sB,
-                           acc16, tot16, warp, lane);
-    } else {
-      dmma_phase((long)(C::KVP / 4) * C::MT * 32, C::KFP / 4);
-    }
-    consumer_sync(TC);
-
-    // 5. epilogue: rhs -> sB as [v][e][IP], then the coalesced LSERK update
+  };
+  // this warp's accumulators -> partial sums at sRb ([kc][v][e][IP])
+  auto store_partials = [&](double *sRb) {
     if constexpr (C::M16) {
       const int mg = warp % C::MG16, ng = warp / C::MG16;
       const int g = lane >> 2, t = lane & 3;
@@ -493,11 +449,11 @@ __global__ void __launch_bounds__(
             const int i = (mg * C::WM16 + ii) * 16 + g + (c >= 2 ? 8 : 0);
             const int col = (ng * C::WN + jj) * 8 + 2 * t + (c & 1);
             const int v = col / E, e = col - v * E;
-            if (i < Np) sB[(v * E + e) * C::IP + i] = tot16[ii][jj][c];
+            if (i < Np) sRb[(v * E + e) * C::IP + i] = tot16[ii][jj][c];
           }
       }
     } else {
-      double *sR = sB + kc * C::S_R;   // this warp's k-chunk partial
+      double *sR = sRb + kc * C::S_R;   // this warp's k-chunk partial
 #pragma unroll
       for (int ii = 0; ii < C::WM; ii++) {
         const int i = (m0 + ii) * 8 + (lane >> 2);
@@ -513,7 +469,13 @@ __global__ void __launch_bounds__(
         }
       }
     }
-    consumer_sync(TC);
+  };
+  // LSERK update of the tile in ring buffer B (elements e0.., ne of them)
+  // from the partial sums at sRb, then the fused wave speed on the last
+  // stage (scratch at sRb)
+  auto update = [&](double *B, long e0, int ne, double *sRb) {
+    double *bU = B;
+    const double *bK = B + C::S_U, *bF = B + C::S_U + C::S_K + C::S_UP + C::S_GEO;
     // the new state goes back to shared memory only for the fused wave speed
     const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
     // one flat loop over (variable, node): every thread has independent
@@ -523,9 +485,9 @@ __global__ void __launch_bounds__(
       const int e = g / Np, i = g - e * Np;
       const long gi = v * vs + e0 * Np + g;
       const int ri = (v * E + e) * C::IP + i;
-      double rhs = sB[ri];
+      double rhs = sRb[ri];
 #pragma unroll
-      for (int c = 1; c < C::KSP; c++) rhs += sB[c * C::S_R + ri];
+      for (int c = 1; c < C::KSP; c++) rhs += sRb[c * C::S_R + ri];
       if (a.rhs_only) {
         a.u_out[gi] = rhs;
       } else {
@@ -541,7 +503,7 @@ __global__ void __launch_bounds__(
       // fused calc_maxv on the new state
       // |v|^2 and c^2 at every face node in parallel (into the rhs staging
       // buffer, free by now), then the per-face max
-      double *sW = sB;
+      double *sW = sRb;
       for (int it = tid; it < 4 * E * Nfp; it += TC) {
         const int fe = it / Nfp, j = it - fe * Nfp, f = fe / E, e = fe - f * E;
         double v2 = 0.0, c2 = 0.0;
@@ -577,6 +539,64 @@ __global__ void __launch_bounds__(
         vmax = bits > vmax ? bits : vmax;
       }
     }
+  };
+  int it = grp;
+  for (int t = blockIdx.x + grp * gridDim.x; ok && t < ntiles; t += C::NG * gridDim.x, it += C::NG) {
+    const int b = it % C::NB;
+    if (!consumer_all(mbar_wait(&full[b], (it / C::NB) & 1), TC)) {
+      ok = false;
+      break;
+    }
+    const long e0 = (long)t * E;
+    const int ne = (int)min((long)E, (long)a.K - e0);
+    double *B = buf(b);
+    vol_flux(B);
+
+    // 2. volume contraction (FUSE: part of the one pass after the face fluxes)
+    if constexpr (!C::FUSE) consumer_sync(TC);
+    if constexpr (C::FUSE) {
+    } else if constexpr (C::M16) {
+#pragma unroll
+      for (int i = 0; i < QM; i++)
+#pragma unroll
+        for (int j = 0; j < QN; j++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            acc16[i][j][c] = 0.f;
+            tot16[i][j][c] = 0.0;
+          }
+      contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), 0, C::KSV16, sB, acc16,
+                           tot16, warp, lane);
+    } else {
+#pragma unroll
+      for (int i = 0; i < C::WM; i++)
+#pragma unroll
+        for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+      dmma_phase(0, C::KVP / 4);
+    }
+    if constexpr (!C::FUSE) consumer_sync(TC);
+
+    face_flux(B);
+    consumer_sync(TC);
+
+    // 4. lift contraction (FUSE: the whole stacked contraction)
+    if constexpr (C::FUSE) {
+#pragma unroll
+      for (int i = 0; i < C::WM; i++)
+#pragma unroll
+        for (int j = 0; j < C::WN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+      dmma_phase(0, C::KVP / 4 + C::KFP / 4);
+    } else if constexpr (C::M16) {
+      contract_m16<C, PR_>(reinterpret_cast<const uint4 *>(a.AT), C::KSV16, C::KSF16, sB,
+                           acc16, tot16, warp, lane);
+    } else {
+      dmma_phase((long)(C::KVP / 4) * C::MT * 32, C::KFP / 4);
+    }
+    consumer_sync(TC);
+
+    store_partials(sB);
+    consumer_sync(TC);
+    update(B, e0, ne, sB);
     // release the buffer (generic-proxy writes into it precede the next TMA)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncwarp();
