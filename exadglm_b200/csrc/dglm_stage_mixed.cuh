@@ -127,6 +127,11 @@ struct MCfg {
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
   static constexpr int E = E_, EP = E_ + 1, NCOL = NV * E;
   static constexpr int M = NCOL <= 64 ? 64 : 128;            // MMA rows
+  // rows stored per operand image: the MMA reads M rows, but rows past NCOL
+  // only feed accumulator rows that are never read back, so an image keeps
+  // its NCOL rows (in 8-row groups) and the MMA's reads of the rest land in
+  // the next image or the FP64 buffers behind it (any bit pattern will do)
+  static constexpr int MA = (NCOL + 7) / 8 * 8;
   static constexpr int NPAD = M == 64 ? (Np + 7) / 8 * 8 : (Np + 15) / 16 * 16;   // MMA N
   // NACC accumulators, each summing the terms of a slice of K in FP32; the
   // slices are added in FP64 when the tile is read back
@@ -168,9 +173,9 @@ struct MCfg {
   // separate volume and lift operands let the face phase overlap the volume
   // MMAs; used where they fit next to the rest
   static constexpr bool SEPL =
-      (size_t)BIMG + (size_t)NPARTS * M * (KVA + KFA) * S + FP64_BYTES <= 232448;
-  static constexpr int AV_BYTES = M * (SEPL ? KVA : KAM) * S;   // one part, volume (or shared)
-  static constexpr int AF_BYTES = SEPL ? M * KFA * S : 0;       // one part, lift
+      (size_t)BIMG + (size_t)NPARTS * MA * (KVA + KFA) * S + FP64_BYTES <= 232448;
+  static constexpr int AV_BYTES = MA * (SEPL ? KVA : KAM) * S;  // one part, volume (or shared)
+  static constexpr int AF_BYTES = SEPL ? MA * KFA * S : 0;      // one part, lift
   static constexpr int SBO_AV = (SEPL ? KVA : KAM) / T * 128, SBO_AF = (SEPL ? KFA : KAM) / T * 128;
   static constexpr int A_BYTES = AV_BYTES + AF_BYTES;           // one part
   static constexpr size_t SMEM = (size_t)BIMG + (size_t)NPARTS * A_BYTES + FP64_BYTES;
@@ -188,6 +193,10 @@ struct MCfg {
   static_assert(NWC >= NISS && NACC % NISS == 0, "issuers split the accumulators evenly");
   static_assert(PHYS != EUL || S_R >= 8 * E * Nfp, "wave-speed terms reuse the rhs buffer");
   static_assert(SMEM < (1u << 18), "descriptor start addresses must fit 14 bits (>> 4)");
+  // the MMA's reads of rows [MA, M) of the last image stay inside the CTA's
+  // shared memory (the FP64 buffers follow the operand images)
+  static_assert((size_t)(M - MA) / 8 * (KAM > KVA ? KAM : KVA) / T * 128 <= FP64_BYTES,
+                "reads past the last operand image stay in shared memory");
 };
 
 // byte offset of element (r, k) in a K-major core-matrix image with 8-row
@@ -265,7 +274,8 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
-  // zero every operand part once: padding rows and K columns stay zero
+  // zero every operand part once: its K padding columns stay zero (rows past
+  // NCOL are not stored, see MCfg::MA)
   for (int i = tid; i < C::NPARTS * C::A_BYTES / 16; i += C::THREADS)
     reinterpret_cast<uint4 *>(sA)[i] = make_uint4(0, 0, 0, 0);
   if (warp == 0) tmem_alloc(sTmem, C::TCOLS);
