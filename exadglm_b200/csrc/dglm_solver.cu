@@ -746,12 +746,16 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
              v.prec == DGLM_PREC_TF32X3 ? "tf32x3" : v.prec == DGLM_PREC_BF16X6 ? "bf16x6"
                                                                                 : "bf16x3",
              v.E, v.CPT, v.WM, v.threads, v.smem);
-  else if (v.mode == MODE_MIXED)
-    snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
-             v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"
-             : v.prec == DGLM_PREC_BF16X6 ? "tcgen05-bf16x6"
-                                          : "tcgen05-bf16x3",
-             v.E, v.npad, v.threads, v.smem);
+  else if (v.mode == MODE_MIXED) {
+    const int n = snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
+                           v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"
+                           : v.prec == DGLM_PREC_BF16X6 ? "tcgen05-bf16x6"
+                                                        : "tcgen05-bf16x3",
+                           v.E, v.npad, v.threads, v.smem);
+    // producer warps are named only when there is more than one
+    if (v.producers > 1 && n > 0 && (size_t)n < len)
+      snprintf(buf + n, len - n, " prod=%d", v.producers);
+  }
   else {
     const int n = snprintf(buf, len, "%s E=%d WN=%d WM=%d threads=%d smem=%zu%s",
                            v.mode == MODE_PIPE ? (v.groups == 2 ? "pipe2-dmma" : "pipe-dmma")

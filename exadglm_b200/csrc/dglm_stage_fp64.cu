@@ -773,10 +773,10 @@ static Variant make_pipe() {
   return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>};
 }
 
-template <int PHYS, int N, int E, int PREC, int NWC>
+template <int PHYS, int N, int E, int PREC, int NWC, int PW>
 static cudaError_t launch_mixed(const StageArgs &a, cudaStream_t s) {
-  using C = MCfg<PHYS, N, E, PREC, NWC>;
-  auto k = stage_mixed_kernel<PHYS, N, E, PREC, NWC>;
+  using C = MCfg<PHYS, N, E, PREC, NWC, PW>;
+  auto k = stage_mixed_kernel<PHYS, N, E, PREC, NWC, PW>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -786,9 +786,9 @@ static cudaError_t launch_mixed(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int PREC, int NWC = 8>
+template <int PHYS, int N, int E, int PREC, int NWC = 8, int PW = 1>
 static Variant make_mixed() {
-  using C = MCfg<PHYS, N, E, PREC, NWC>;
+  using C = MCfg<PHYS, N, E, PREC, NWC, PW>;
   StageVariantInfo i{};
   i.mode = MODE_MIXED;
   i.E = E;
@@ -801,7 +801,8 @@ static Variant make_mixed() {
   i.kva = C::KVA;
   i.kfa = C::KFA;
   i.bimg = C::BIMG;
-  return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC>};
+  i.producers = PW;
+  return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC, PW>};
 }
 
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
@@ -853,6 +854,8 @@ static const std::vector<Variant> &variants();
 #define V_M16(P, NN, E, WN, WM, PR) make_v<P, NN, MODE_MMA16, E, 1, WN, WM, PR>()
 #define V_PM16(P, NN, E, WN, WM, PR) make_pipe<P, NN, E, WN, WM, false, 1, PR>()
 #define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
+// tcgen05 variants with PW producer warps
+#define V_MXP(P, NN, E, PREC, W, PW) make_mixed<P, NN, E, PREC, W, PW>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -872,6 +875,7 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPE2(EUL, 4, 8, 1, 5, true), V_PIPE2(EUL, 4, 8, 1, 3, true),
               V_TF32W(EUL, 4, 8, 16), V_BF16W(EUL, 4, 8, 16), V_BF16X6(EUL, 4, 8, 16),
               V_TF32(EUL, 4, 8), V_BF16(EUL, 4, 8), V_BF16X6(EUL, 4, 8, 8),
+              V_MXP(EUL, 4, 8, PREC_BF16, 15, 2), V_MXP(EUL, 4, 8, PREC_BF16X6, 8, 2),
               V_M16(EUL, 4, 8, 1, 3, 2), V_M16(EUL, 4, 8, 1, 1, 1), V_M16(EUL, 4, 8, 1, 1, 3),
               V_PM16(EUL, 4, 8, 1, 3, 1), V_PIPER(EUL, 4, 8, 1, 2, true, 2, 2),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),

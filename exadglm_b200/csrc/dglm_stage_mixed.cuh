@@ -120,10 +120,10 @@ __device__ __forceinline__ void split_bf16x3(double x, unsigned short (&p)[3]) {
   p[2] = __bfloat16_as_ushort(b2);
 }
 
-template <int PHYS, int N, int E_, int PREC, int NWC_ = 8>
+template <int PHYS, int N, int E_, int PREC, int NWC_ = 8, int PW_ = 1>
 struct MCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
-  static constexpr int NB = 2, PW = 1;   // tile ring and producer warps (pipe_producer)
+  static constexpr int NB = 2, PW = PW_;   // tile ring and producer warps (pipe_producer)
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
   static constexpr int E = E_, EP = E_ + 1, NCOL = NV * E;
   static constexpr int M = NCOL <= 64 ? 64 : 128;            // MMA rows
@@ -159,7 +159,7 @@ struct MCfg {
   // byte sizes
   static constexpr int BV_BYTES = NPAD * KVA * S, BF_BYTES = NPAD * KFA * S;
   static constexpr int BIMG = NPARTS * (BV_BYTES + BF_BYTES);   // part 0, part 1, ...
-  static constexpr int NWC = NWC_, TC = 32 * NWC, THREADS = TC + 32;
+  static constexpr int NWC = NWC_, TC = 32 * NWC, THREADS = TC + 32 * PW;
   // FP64 pipeline buffers (as in PCfg)
   // neighbour traces [v][e][UPS], written by pipe_producer (conflict-free
   // gathers and face-flux reads)
@@ -243,10 +243,10 @@ __device__ __forceinline__ void prod_parts(int q, int &pa, int &pb) {
   }
 }
 
-template <int PHYS, int N, int E_, int PREC, int NWC_>
-__global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
+template <int PHYS, int N, int E_, int PREC, int NWC_, int PW_>
+__global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1)
     stage_mixed_kernel(const StageArgs a, int ntiles) {
-  using C = MCfg<PHYS, N, E_, PREC, NWC_>;
+  using C = MCfg<PHYS, N, E_, PREC, NWC_, PW_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, EP = C::EP,
                 TC = C::TC;
   extern __shared__ __align__(16) double smem[];
@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
   const long vs = a.vs;
 
   if (tid == 0) {
-    mbar_init(&full[0], 33);
-    mbar_init(&full[1], 33);
+    mbar_init(&full[0], 1 + 32 * C::PW);
+    mbar_init(&full[1], 1 + 32 * C::PW);
     mbar_init(&empty[0], C::NWC);
     mbar_init(&empty[1], C::NWC);
     mbar_init(abar, 1);
@@ -285,8 +285,9 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_>::THREADS, 1)
   tc_fence_after();
   const unsigned tmem = *sTmem;
 
-  if (warp == C::NWC) {
-    pipe_producer<C, PHYS>(a, ntiles, sBimg, sBuf0, full, empty, abar, C::BIMG, 0, lane);
+  if (warp >= C::NWC) {
+    pipe_producer<C, PHYS>(a, ntiles, sBimg, sBuf0, full, empty, abar, C::BIMG, warp - C::NWC,
+                           lane);
     return;
   }
 
