@@ -306,7 +306,9 @@ def mixed_section(a, p, stream, fp64_ms_per_step):
                      for v in range(p.nvar)]
         out[prec] = {
             "value": per_step / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-            "speedup_vs_fp64": fp64_ms_per_step / ms,
+            # null when the FP64 path was not timed in this run (--only mixed)
+            "speedup_vs_fp64": (fp64_ms_per_step / ms if fp64_ms_per_step is not None
+                                else None),
             "rel_l2_vs_fp64": float(np.linalg.norm(um - u64) / np.linalg.norm(u64)),
             "rel_l2_per_field": per_field,
             "kernel": variants("euler", p.N)[s.variant()],
@@ -507,7 +509,7 @@ def main():
     p = build_problem(a)
     stream = torch.cuda.Stream()
     if a.only in ("mixed", "adjoint", "batch", "precision"):
-        res = (mixed_section(a, p, stream, float("nan")) if a.only == "mixed"
+        res = (mixed_section(a, p, stream, None) if a.only == "mixed"
                else adjoint_section(a, stream) if a.only == "adjoint"
                else precision_section(a, stream) if a.only == "precision"
                else batch_section(a, stream))
