@@ -898,10 +898,13 @@ DGLM_VARIANTS(ADV, 4, V_SIMT(ADV, 4, 64, 5, 4), V_DMMA(ADV, 4, 64, 2, 5),
 DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7),
               V_PIPEF(ADV, 5, 16, 1, false, 4, 2))
 DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6),
+              V_PIPEF(ADV, 6, 8, 1, false, 8, 2), V_PIPEF(ADV, 6, 8, 1, false, 12, 2),
               V_M16(ADV, 6, 32, 1, 2, 2), V_M16(ADV, 6, 32, 1, 2, 1),
               V_M16(ADV, 6, 32, 1, 2, 3))
-DGLM_VARIANTS(ADV, 7, V_SIMT(ADV, 7, 16, 8, 4), V_DMMA(ADV, 7, 16, 1, 5))
-DGLM_VARIANTS(ADV, 8, V_SIMT(ADV, 8, 16, 8, 4), V_DMMA(ADV, 8, 16, 1, 7))
+DGLM_VARIANTS(ADV, 7, V_SIMT(ADV, 7, 16, 8, 4), V_DMMA(ADV, 7, 16, 1, 5),
+              V_PIPEF(ADV, 7, 8, 1, false, 8, 2))
+DGLM_VARIANTS(ADV, 8, V_SIMT(ADV, 8, 16, 8, 4), V_DMMA(ADV, 8, 16, 1, 7),
+              V_PIPEF(ADV, 8, 8, 1, false, 6, 2))
 
 static const std::vector<Variant> *variant_list(int physics, int N) {
 #define CASE(P, NN) \
