@@ -126,6 +126,7 @@ struct StageVariantInfo {
   int producers;   // PIPE: producer warps sharing the neighbour gathers (1 to 4)
   int ksplit;      // PIPE: k-chunks of the DMMA contraction summed in the epilogue
   int fused;       // PIPE: 1 = volume and lift contractions in one DMMA pass
+  int k_global;    // PIPE: 1 = the RK register is fetched by the update, not staged
   int op_global;   // PIPE: 1 = operator fragments read through L1, not staged in shared memory
 };
 

@@ -768,7 +768,8 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
         (size_t)n < len) {
       const int m = snprintf(buf + n, len - n, " ring=%d prod=%d", v.ring, v.producers);
       if (v.ksplit > 1 && m > 0 && (size_t)(n + m) < len)
-        snprintf(buf + n + m, len - n - m, " ksplit=%d%s", v.ksplit, v.fused ? " fused" : "");
+        snprintf(buf + n + m, len - n - m, " ksplit=%d%s%s", v.ksplit, v.fused ? " fused" : "",
+                 v.k_global ? " k=global" : "");
     }
   }
   return DGLM_OK;

@@ -730,10 +730,10 @@ static int sm_count() {
 }
 
 template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG, int PR, int NB, int PW,
-          int KSP, bool FU>
+          int KSP, bool FU, bool KG>
 static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>;
-  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>;
+  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -744,9 +744,9 @@ static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
 }
 
 template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1, int PR = 0, int NB = 2,
-          int PW = 1, int KSP = 1, bool FU = false>
+          int PW = 1, int KSP = 1, bool FU = false, bool KG = false>
 static Variant make_pipe() {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>;
   StageVariantInfo i{};
   i.mode = PR ? MODE_MMA16 : MODE_PIPE;
   i.E = E;
@@ -765,12 +765,13 @@ static Variant make_pipe() {
   i.producers = PW;
   i.ksplit = KSP;
   i.fused = FU ? 1 : 0;
+  i.k_global = KG ? 1 : 0;
   i.op_global = AS ? 0 : 1;
   if (PR) {
     i.prec = PR == 2 ? DGLM_PREC_TF32X3 : PR == 3 ? DGLM_PREC_BF16X6 : DGLM_PREC_BF16X3;
     i.kstep = C::KSTEP16;
   }
-  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU>};
+  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>};
 }
 
 template <int PHYS, int N, int E, int PREC, int NWC, int PW>
@@ -846,6 +847,9 @@ static const std::vector<Variant> &variants();
 // as V_PIPEK with the volume and lift contractions fused into one pass
 #define V_PIPEF(P, NN, E, WN, AS, KSP, PW) \
   make_pipe<P, NN, E, WN, 99, AS, 1, 0, 2, PW, KSP, true>()
+// separate volume and lift passes, KSP k-chunks, the RK register fetched by the update
+#define V_PIPEG(P, NN, E, WN, AS, KSP, PW) \
+  make_pipe<P, NN, E, WN, 99, AS, 1, 0, 2, PW, KSP, false, true>()
 #define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define V_TF32W(P, NN, E, W) make_mixed<P, NN, E, PREC_TF32, W>()
@@ -884,6 +888,7 @@ DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
+              V_PIPEG(EUL, 6, 8, 1, false, 2, 2), V_PIPEG(EUL, 6, 8, 1, false, 2, 1),
               V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 // N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB

@@ -108,7 +108,7 @@ __device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
 }
 
 template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1, int PR_ = 0,
-          int NB_ = 2, int PW_ = 1, int KSP_ = 1, bool FU_ = false>
+          int NB_ = 2, int PW_ = 1, int KSP_ = 1, bool FU_ = false, bool KG_ = false>
 struct PCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -133,6 +133,9 @@ struct PCfg {
   // FUSE: face-flux rows sit below the volume rows, both flux phases run
   // back to back and one DMMA pass covers the stacked k range
   static constexpr bool FUSE = FU_;
+  // KG: the RK register is not staged; the update fetches it from global
+  // memory (orders whose staged tiles would not fit twice otherwise)
+  static constexpr bool KG = KG_;
   static constexpr int NWC = (M16 ? MG16 : MGROUPS) * (NT / WN) * KSP;   // consumer warps per group
   static constexpr int TC = 32 * NWC;                   // consumer threads per group
   static constexpr int THREADS = NG * TC + 32 * PW;     // + producer warps
@@ -158,7 +161,7 @@ struct PCfg {
   static constexpr int UPS = NFF % 8 == 4 ? NFF : NFF + 4;
   // shared memory segments, in doubles (operator A fragments when ASMEM)
   static constexpr int S_AF = !ASMEM ? 0 : M16 ? KST16 * MT16 * NPARTS16 * 64 : KS * MT * 32;
-  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * E * UPS;
+  static constexpr int S_U = NV * E * Np, S_K = KG ? 0 : NV * E * Np, S_UP = NV * E * UPS;
   static constexpr int S_GEO = 9 * E, S_FACE = 5 * 4 * E;
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
@@ -229,7 +232,8 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
       mbar_arrive_expect_tx(&full[b], C::TX);
       for (int v = 0; v < NV; v++) {
         bulk_g2s(bU + v * E * Np, a.u_in + v * vs + e0 * Np, 8u * E * Np, &full[b]);
-        bulk_g2s(bK + v * E * Np, a.kreg + v * vs + e0 * Np, 8u * E * Np, &full[b]);
+        if (C::S_K)   // configurations that fetch k in the update stage none
+          bulk_g2s(bK + v * E * Np, a.kreg + v * vs + e0 * Np, 8u * E * Np, &full[b]);
       }
       for (int m = 0; m < 9; m++) bulk_g2s(bG + m * E, a.geo + m * gs + e0, 8u * E, &full[b]);
       for (int q = 0; q < 3; q++)
@@ -270,11 +274,11 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
 }
 
 template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_, int PR_, int NB_,
-          int PW_, int KSP_, bool FU_>
+          int PW_, int KSP_, bool FU_, bool KG_>
 __global__ void __launch_bounds__(
-    PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_>::THREADS, 1)
+    PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_, KG_>::THREADS, 1)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
-  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_>;
+  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_, KG_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E,
                 BLD = C::BLD, TC = C::TC;
   extern __shared__ __align__(16) double smem[];
@@ -480,7 +484,8 @@ __global__ void __launch_bounds__(
     const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
     // one flat loop over (variable, node): every thread has independent
     // updates in flight
-    for (int vg = tid; vg < NV * ne * Np; vg += TC) {
+    const int tot = NV * ne * Np;
+    auto item = [&](int vg, double kold) {
       const int v = vg / (ne * Np), g = vg - v * (ne * Np);
       const int e = g / Np, i = g - e * Np;
       const long gi = v * vs + e0 * Np + g;
@@ -491,11 +496,31 @@ __global__ void __launch_bounds__(
       if (a.rhs_only) {
         a.u_out[gi] = rhs;
       } else {
-        const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
+        const double kn = a.rka * kold + dt * rhs;
         const double un = bU[v * E * Np + g] + a.rkb * kn;
         a.kreg[gi] = kn;
         a.u_out[gi] = un;
         if (keep_u) bU[v * E * Np + g] = un;
+      }
+    };
+    if constexpr (C::KG) {
+      // every k of this thread is requested before the first is used
+      constexpr int IPT = (NV * E * Np + TC - 1) / TC;
+      double kr[IPT];
+#pragma unroll
+      for (int q = 0; q < IPT; q++) {
+        const int vg = tid + q * TC;
+        kr[q] = 0.0;
+        if (vg < tot && !a.rhs_only)
+          kr[q] = a.kreg[(vg / (ne * Np)) * vs + e0 * Np + vg % (ne * Np)];
+      }
+#pragma unroll
+      for (int q = 0; q < IPT; q++)
+        if (tid + q * TC < tot) item(tid + q * TC, kr[q]);
+    } else {
+      for (int vg = tid; vg < tot; vg += TC) {
+        const int v = vg / (ne * Np), g = vg - v * (ne * Np);
+        item(vg, C::S_K ? bK[v * E * Np + g] : 0.0);
       }
     }
     if (PHYS == EUL && a.last_stage && !a.rhs_only) {
