@@ -850,6 +850,9 @@ static const std::vector<Variant> &variants();
 // separate volume and lift passes, KSP k-chunks, the RK register fetched by the update
 #define V_PIPEG(P, NN, E, WN, AS, KSP, PW) \
   make_pipe<P, NN, E, WN, 99, AS, 1, 0, 2, PW, KSP, false, true>()
+// pipelined split-precision mma.sync engine with the RK register fetched by the update
+#define V_PM16G(P, NN, E, WN, WM, PR, PW) \
+  make_pipe<P, NN, E, WN, WM, false, 1, PR, 2, PW, 1, false, true>()
 #define V_TF32(P, NN, E) make_mixed<P, NN, E, PREC_TF32>()
 #define V_BF16(P, NN, E) make_mixed<P, NN, E, PREC_BF16>()
 #define V_TF32W(P, NN, E, W) make_mixed<P, NN, E, PREC_TF32, W>()
@@ -889,6 +892,8 @@ DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEG(EUL, 6, 8, 1, false, 2, 2), V_PIPEG(EUL, 6, 8, 1, false, 2, 1),
+              V_PM16G(EUL, 6, 8, 1, 2, 1, 2), V_PM16G(EUL, 6, 8, 1, 2, 2, 2),
+              V_PM16G(EUL, 6, 8, 1, 2, 3, 2),
               V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 // N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB

@@ -87,7 +87,7 @@ def test_mixed_steps_error(phys, N, prec):
 
 
 @pytest.mark.parametrize("prec", ["tf32x3", "bf16x3", "bf16x6"])
-@pytest.mark.parametrize("phys,N", CASES[:2])
+@pytest.mark.parametrize("phys,N", CASES)
 def test_every_mixed_variant_steps(phys, N, prec):
     """Every tile shape of the mode through full steps (the LSERK epilogue
     included, whether it reads the RK register from shared or global memory)."""
