@@ -889,7 +889,8 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
-              V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2))
+              V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),
+              V_PM16G(EUL, 5, 8, 1, 2, 1, 2))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEG(EUL, 6, 8, 1, false, 2, 2), V_PIPEG(EUL, 6, 8, 1, false, 2, 1),
               V_PM16G(EUL, 6, 8, 1, 2, 1, 2), V_PM16G(EUL, 6, 8, 1, 2, 2, 2),
@@ -910,7 +911,8 @@ DGLM_VARIANTS(ADV, 5, V_SIMT(ADV, 5, 32, 7, 4), V_DMMA(ADV, 5, 32, 1, 7),
 DGLM_VARIANTS(ADV, 6, V_SIMT(ADV, 6, 32, 7, 4), V_DMMA(ADV, 6, 32, 1, 6),
               V_PIPEF(ADV, 6, 8, 1, false, 8, 2), V_PIPEF(ADV, 6, 8, 1, false, 12, 2),
               V_M16(ADV, 6, 32, 1, 2, 2), V_M16(ADV, 6, 32, 1, 2, 1),
-              V_M16(ADV, 6, 32, 1, 2, 3))
+              V_M16(ADV, 6, 32, 1, 2, 3), V_PM16G(ADV, 6, 16, 1, 2, 1, 2),
+              V_PM16G(ADV, 6, 16, 1, 2, 2, 2), V_PM16G(ADV, 6, 16, 1, 2, 3, 2))
 DGLM_VARIANTS(ADV, 7, V_SIMT(ADV, 7, 16, 8, 4), V_DMMA(ADV, 7, 16, 1, 5),
               V_PIPEF(ADV, 7, 8, 1, false, 8, 2))
 DGLM_VARIANTS(ADV, 8, V_SIMT(ADV, 8, 16, 8, 4), V_DMMA(ADV, 8, 16, 1, 7),
