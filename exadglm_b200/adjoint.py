@@ -1,9 +1,9 @@
 """Gradients of final-time objectives through the DGLM time integration.
 
-``evolve(u0, solver, nsteps)`` advances the state ``u0`` (a CUDA float64
-tensor of shape (nvar, K*Np), the reference's nodal layout) by ``nsteps``
-LSERK steps on ``solver`` and returns u(T) as a differentiable tensor.  The
-backward pass is the library's discrete adjoint (``dglm_adjoint_backward``):
+``evolve(u0, solver, nsteps)`` (the autograd Function ``DGLMStep``) advances
+the state ``u0`` (a CUDA float64 tensor of shape (nvar, K*Np), the
+reference's nodal layout) by ``nsteps`` LSERK steps on ``solver`` and returns
+u(T) as a differentiable tensor.  The backward pass is the library's discrete adjoint (``dglm_adjoint_backward``):
 the exact transpose of the FP64 step with dt and the face penalty tau held at
 the values of the forward run.  Those two are maxima over the state (a global
 CFL max and per-face wave speeds), so they are frozen rather than
@@ -23,7 +23,10 @@ import torch
 from .capi import Solver
 
 
-class _Evolve(torch.autograd.Function):
+class DGLMStep(torch.autograd.Function):
+    """``DGLMStep.apply(u0, solver, nsteps, checkpoint_every)``: u(T) after
+    ``nsteps`` CFL steps from u0; its backward is the discrete adjoint."""
+
     @staticmethod
     def forward(ctx, u0, solver, nsteps, checkpoint_every):
         nv = solver.p.nvar
@@ -57,7 +60,7 @@ class _Evolve(torch.autograd.Function):
 
 def evolve(u0: torch.Tensor, solver: Solver, nsteps: int, checkpoint_every: int = 50):
     """u(T) after nsteps CFL steps from u0, differentiable with respect to u0."""
-    return _Evolve.apply(u0, solver, nsteps, checkpoint_every)
+    return DGLMStep.apply(u0, solver, nsteps, checkpoint_every)
 
 
 def density_misfit(uT: torch.Tensor, rho_target: torch.Tensor) -> torch.Tensor:
