@@ -207,12 +207,12 @@ class Mesh3D:
 
     @staticmethod
     def _points(v, rst):
+        # x = sum_q lambda_q(r, s, t) v_q with the affine weights
+        # lambda = (-(r+s+t+1), r+1, s+1, t+1) / 2: one (K,4) x (4,Np) product
+        # per coordinate
         r, s, t = rst[:, 0], rst[:, 1], rst[:, 2]
-        out = []
-        for d in range(3):
-            out.append(0.5 * (-np.outer(v[0][:, d], r + s + t + 1) + np.outer(v[1][:, d], r + 1)
-                              + np.outer(v[2][:, d], s + 1) + np.outer(v[3][:, d], t + 1)))
-        return out
+        lam = 0.5 * np.stack([-(r + s + t + 1), r + 1, s + 1, t + 1])        # (4,Np)
+        return [np.stack([v[q][:, d] for q in range(4)], axis=1) @ lam for d in range(3)]
 
     def _vmaps(self):
         ref, K, Np, Nfp = self.ref, self.Nelem, self.Np, self.Nfp

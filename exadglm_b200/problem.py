@@ -74,7 +74,7 @@ def euler_state(rho, vx, vy, vz, p, gamma):
 
 def advection_gaussian(n=8, N=3, v=(1.0, 0.5, 0.25), center=(0.5, 0.5, 0.5), width2=0.01,
                        cfl=0.5, tau_scale=1.2, tmax=1000.0, mesh=None):
-    mesh = mesh or Mesh3D(N, UniformBox(n + 1, n + 1, n + 1))
+    mesh = mesh or Mesh3D(N, UniformBox(n + 1, n + 1, n + 1), high_order=False)
     x, y, z = _nodes(mesh)
     r2 = (x - center[0]) ** 2 + (y - center[1]) ** 2 + (z - center[2]) ** 2
     u0 = np.exp(-r2 / width2)[None, :]
@@ -101,7 +101,7 @@ def batch_instances(count=256, seed=0, n_range=(4, 24), orders=(2, 6), cfl=0.5,
         c = rng.uniform(0.0, 1.0, 3)
         w = float(rng.uniform(0.05, 0.2))
         if (n, N) not in meshes:
-            meshes[(n, N)] = Mesh3D(N, UniformBox(n + 1, n + 1, n + 1))
+            meshes[(n, N)] = Mesh3D(N, UniformBox(n + 1, n + 1, n + 1), high_order=False)
         mesh = meshes[(n, N)]
         x, y, z = _nodes(mesh)
         r2 = (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2
@@ -114,7 +114,7 @@ def batch_instances(count=256, seed=0, n_range=(4, 24), orders=(2, 6), cfl=0.5,
 
 def euler_sine(n=32, N=4, v=(1.0, 0.5, 0.25), p=1.0, gamma=1.4, cfl=0.4, tau_scale=1.2,
                tmax=1000.0, noise=0.0, seed=0, mesh=None):
-    mesh = mesh or Mesh3D(N, UniformBox(n + 1, n + 1, n + 1))
+    mesh = mesh or Mesh3D(N, UniformBox(n + 1, n + 1, n + 1), high_order=False)
     x, y, z = _nodes(mesh)
     rho = 1 + 0.2 * np.sin(2 * np.pi * (x + y + z))
     one = np.ones_like(x)
