@@ -22,7 +22,8 @@ PRECISIONS = {"fp64": PREC_FP64, "tf32x3": PREC_TF32X3, "bf16x3": PREC_BF16X3,
 EXPORTS = (
     "dglm_last_error", "dglm_abi_version", "dglm_order_supported", "dglm_create",
     "dglm_destroy", "dglm_set_stream", "dglm_upload_mesh", "dglm_set_state", "dglm_get_state",
-    "dglm_step", "dglm_step_fixed_dt", "dglm_stage", "dglm_sync", "dglm_get_time", "dglm_get_dt_history",
+    "dglm_step", "dglm_step_fixed_dt", "dglm_stage", "dglm_sync", "dglm_get_time", "dglm_set_time",
+    "dglm_get_dt_history",
     "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
@@ -87,6 +88,7 @@ def lib():
         L.dglm_destroy.argtypes = [_P]
         L.dglm_get_time.argtypes = [_P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_int)]
+        L.dglm_set_time.argtypes = [_P, C.c_double, C.c_int]
         L.dglm_get_dt_history.argtypes = [_P, C.c_int, C.c_int, _P]
         L.dglm_rhs.argtypes = [_P, _P, _P]
         L.dglm_variant_describe.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
@@ -288,6 +290,10 @@ class Solver:
         t, dt, ts = C.c_double(), C.c_double(), C.c_int()
         check(self.L.dglm_get_time(self.h, C.byref(t), C.byref(dt), C.byref(ts)))
         return t.value, dt.value, ts.value
+
+    def set_time(self, t, tstep):
+        """Continue a saved run: time and step counter after set_state."""
+        check(self.L.dglm_set_time(self.h, float(t), int(tstep)))
 
     def dt_history(self, first, count):
         out = np.zeros(count)

@@ -684,6 +684,19 @@ dglm_status dglm_get_time(dglm_handle *h, double *t, double *dt, int *tstep) {
   return DGLM_OK;
 }
 
+dglm_status dglm_set_time(dglm_handle *h, double t, int tstep) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_set_time: NULL handle");
+  if (!(t >= 0) || tstep < 0) return set_error(DGLM_ERR_INVALID, "dglm_set_time: t < 0 or tstep < 0");
+  if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_set_time: set the state first");
+  DeviceGuard g(h->dev);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&h->sc->t, &t, sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&h->sc->tstep, &tstep, sizeof(int), cudaMemcpyHostToDevice);
+  return cuda_check(e, "dglm_set_time");
+}
+
 dglm_status dglm_get_dt_history(dglm_handle *h, int first, int count, double *dt_out) {
   if (!h || !dt_out || first < 0 || count < 0 || count > kHistory)
     return set_error(DGLM_ERR_INVALID, "dglm_get_dt_history: bad argument");

@@ -574,12 +574,13 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
       const double u1 = sU[(0 * Np + nd) * EP + e], u2 = sU[(1 * Np + nd) * EP + e],
                    u3 = sU[(2 * Np + nd) * EP + e], u4 = sU[(3 * Np + nd) * EP + e],
                    u5 = sU[(4 * Np + nd) * EP + e];
-      const double ir = 1.0 / u1;
-      const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
+      // divisions as in face_maxv_kernel, so dt does not depend on which
+      // kernel computed maxv (a restarted run repeats the original bit for bit)
+      const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
       const double v2 = vx * vx + vy * vy + vz * vz;
       mv2 = v2 > mv2 ? v2 : mv2;
       const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-      const double c2 = fabs(a.gamma * pres * ir);
+      const double c2 = fabs(a.gamma * pres / u1);
       mc2 = c2 > mc2 ? c2 : mc2;
       bad |= (v2 != v2) || (c2 != c2);
     }

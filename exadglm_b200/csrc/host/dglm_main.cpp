@@ -11,10 +11,19 @@
 //   --datain DIR --dataout DIR --physics euler|advection --tmax T
 //   [--cfl 0.8] [--gamma 1.4] [--tau-scale 1.2] [--device 0]
 //   [--matrix-order f|c] [--precision fp64|tf32x3|bf16x3] [--variant V]
+// Full state and restart (not in the reference, which writes only u1):
+//   --full-state            every snapshot also writes the other fields
+//                           (u2..u5_NNNNNNN.bin for Euler) and t_NNNNNNN.bin
+//                           (three doubles: t, the step number and the print
+//                           interval, 0 before the first step)
+//   --restart-dir DIR --restart-step S
+//                           start from DIR's full-state snapshot of step S
+//                           and continue the step numbering from there
 // The initial state is datain/u0.bin (nvar x K x Np doubles) when present,
 // otherwise the reference's own init_u (euler_init.cpp:5-35,
 // advec_init.cpp:5-25); the advection velocity is datain/v{x,y,z}.bin when
 // present, otherwise (1, 1, 1) as in advec_init.cpp.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -68,6 +77,17 @@ int find_print_tstep(double tmax, double dt, int base) {
   return r > 0 ? (int)r : 1;
 }
 
+// name of field v (0-based) of a snapshot: u_ (advection), u1_..u5_ (Euler)
+std::string field_name(int v, int tstep, bool euler) {
+  const std::string s = std::to_string(tstep);
+  return std::string(euler ? "u" + std::to_string(v + 1) + "_" : "u_") +
+         std::string(7 - s.size(), '0') + s + ".bin";
+}
+std::string time_name(int tstep) {
+  const std::string s = std::to_string(tstep);
+  return "t_" + std::string(7 - s.size(), '0') + s + ".bin";
+}
+
 std::string snap_name(int tstep, bool euler) {
   std::string s = std::to_string(tstep);
   return std::string(euler ? "u1_" : "u_") + std::string(7 - s.size(), '0') + s + ".bin";
@@ -88,8 +108,10 @@ int fail(const char *what) {
 
 int main(int argc, char **argv) {
   std::string datain, dataout, physics = "euler", order = "f", precision = "fp64";
+  std::string restart_dir;
   double cfl = 0.8, gamma = 1.4, tau_scale = 1.2, tmax = -1;
-  int device = 0, variant = -1;
+  int device = 0, variant = -1, restart_step = -1;
+  bool full_state = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     auto next = [&]() -> std::string {
@@ -110,6 +132,9 @@ int main(int argc, char **argv) {
     else if (a == "--matrix-order") order = next();
     else if (a == "--precision") precision = next();
     else if (a == "--variant") variant = std::atoi(next().c_str());
+    else if (a == "--full-state") full_state = true;
+    else if (a == "--restart-dir") restart_dir = next();
+    else if (a == "--restart-step") restart_step = std::atoi(next().c_str());
     else {
       std::fprintf(stderr, "dglm_main: unknown argument %s\n", a.c_str());
       return 2;
@@ -121,8 +146,13 @@ int main(int argc, char **argv) {
                          "[--matrix-order f|c] [--precision fp64|tf32x3|bf16x3]\n");
     return 2;
   }
+  if (!restart_dir.empty() && restart_step < 0) {
+    std::fprintf(stderr, "dglm_main: --restart-dir needs --restart-step\n");
+    return 2;
+  }
   if (datain.back() != '/') datain += '/';
   if (dataout.back() != '/') dataout += '/';
+  if (!restart_dir.empty() && restart_dir.back() != '/') restart_dir += '/';
   const bool euler = physics == "euler";
   const int nvar = euler ? 5 : 1;
 
@@ -156,7 +186,21 @@ int main(int argc, char **argv) {
   const size_t n = (size_t)K * Np;
   std::vector<double> u0;
   std::vector<double> vel[3];
-  if (!read_bin(datain + "u0.bin", u0, nvar * n, false)) {
+  double t0 = 0;
+  int tstep0 = 0, print_tstep = 0;
+  if (!restart_dir.empty()) {   // a full-state snapshot: every field and t
+    u0.assign(nvar * n, 0.0);
+    for (int v = 0; v < nvar; v++) {
+      std::vector<double> f;
+      if (!read_bin(restart_dir + field_name(v, restart_step, euler), f, n)) return 1;
+      std::copy(f.begin(), f.end(), u0.begin() + v * n);
+    }
+    std::vector<double> tt;
+    if (!read_bin(restart_dir + time_name(restart_step), tt, 3)) return 1;
+    t0 = tt[0];
+    tstep0 = (int)std::llround(tt[1]);
+    print_tstep = (int)std::llround(tt[2]);   // keeps the original run's interval
+  } else if (!read_bin(datain + "u0.bin", u0, nvar * n, false)) {
     u0.assign(nvar * n, 0.0);
     for (size_t i = 0; i < n; i++) {
       const double x = px[i], y = py[i], z = pz[i];
@@ -206,39 +250,49 @@ int main(int argc, char **argv) {
   std::vector<const double *> up(nvar);
   for (int v = 0; v < nvar; v++) up[v] = u0.data() + v * n;
   if (dglm_set_state(h, up.data(), 0) != DGLM_OK) return fail("set_state");
+  if (!restart_dir.empty() && dglm_set_time(h, t0, tstep0) != DGLM_OK) return fail("set_time");
 
   std::vector<double> out(nvar * n);
   std::vector<double *> op(nvar);
   for (int v = 0; v < nvar; v++) op[v] = out.data() + v * n;
-  auto snapshot = [&](int tstep) -> bool {
-    if (dglm_get_state(h, op.data(), 0) != DGLM_OK) return false;
-    return write_bin(dataout + snap_name(tstep, euler), out.data(), n);
+  // the reference's snapshot (u_ or u1_); with --full-state every field and t
+  auto write_snapshot = [&](const double *u, int tstep, double t) -> bool {
+    if (!write_bin(dataout + snap_name(tstep, euler), u, n)) return false;
+    if (!full_state) return true;
+    for (int v = 1; v < nvar; v++)
+      if (!write_bin(dataout + field_name(v, tstep, euler), u + v * n, n)) return false;
+    const double tt[3] = {t, (double)tstep, (double)print_tstep};
+    return write_bin(dataout + time_name(tstep), tt, 3);
   };
-  if (!write_bin(dataout + snap_name(0, euler), u0.data(), n)) {
+  auto snapshot = [&](int tstep, double t) -> bool {
+    if (dglm_get_state(h, op.data(), 0) != DGLM_OK) return false;
+    return write_snapshot(out.data(), tstep, t);
+  };
+  if (restart_dir.empty() && !write_snapshot(u0.data(), 0, 0.0)) {
     std::fprintf(stderr, "dglm_main: cannot write to %s\n", dataout.c_str());
     return 1;
   }
 
-  double t = 0, dt = 0;
-  int tstep = 0, print_tstep = 0;
+  double t = t0, dt = 0;
+  int tstep = tstep0;
   while (t < tmax) {
     const int chunk = print_tstep ? print_tstep - tstep % print_tstep : 1;
     if (dglm_step(h, chunk) != DGLM_OK) return fail("step");
     if (dglm_sync(h) != DGLM_OK) return fail("step");
     if (dglm_get_time(h, &t, &dt, &tstep) != DGLM_OK) return fail("time");
-    if (tstep == 0) break;
+    if (tstep == tstep0) break;
     double last_dt = 0;
     if (dglm_get_dt_history(h, tstep - 1, 1, &last_dt) != DGLM_OK) return fail("time");
     if (print_tstep == 0) {
       double dt0 = 0;
-      dglm_get_dt_history(h, 0, 1, &dt0);
+      dglm_get_dt_history(h, tstep0, 1, &dt0);
       print_tstep = find_print_tstep(tmax, dt0, 30);
     }
     const bool last = !(t < tmax);
     if (tstep % print_tstep == 0 || last) {
       std::printf("tstep=%d, dt=%.8f, t=%.5f\n", tstep, last_dt, t);
       std::fflush(stdout);
-      if (!snapshot(tstep)) return fail("snapshot");
+      if (!snapshot(tstep, t)) return fail("snapshot");
     }
   }
   dglm_destroy(h);

@@ -130,6 +130,12 @@ dglm_status dglm_stage(dglm_handle *h, int stage, double dt);
 dglm_status dglm_sync(dglm_handle *h);
 /* Time, last dt and step counter (synchronises). */
 dglm_status dglm_get_time(dglm_handle *h, double *t, double *dt, int *tstep);
+/* Sets the simulated time and step counter after dglm_set_state, so that a
+ * run restarted from a saved state continues where it stopped (t clipped at
+ * tmax as usual, step numbering and dt history continuing from tstep).
+ * No counterpart in the reference, which has no restart; t >= 0 and
+ * tstep >= 0, else DGLM_ERR_INVALID.  Synchronises the handle's stream. */
+dglm_status dglm_set_time(dglm_handle *h, double t, int tstep);
 /* dt of steps [first, first+count) taken since dglm_set_state (synchronises);
  * the history keeps the most recent 65536 steps. */
 dglm_status dglm_get_dt_history(dglm_handle *h, int first, int count, double *dt_out);
