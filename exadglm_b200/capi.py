@@ -23,7 +23,7 @@ EXPORTS = (
     "dglm_last_error", "dglm_abi_version", "dglm_order_supported", "dglm_create",
     "dglm_destroy", "dglm_set_stream", "dglm_upload_mesh", "dglm_set_state", "dglm_get_state",
     "dglm_step", "dglm_step_fixed_dt", "dglm_stage", "dglm_sync", "dglm_get_time", "dglm_set_time",
-    "dglm_get_dt_history",
+    "dglm_get_dt_history", "dglm_run_ensemble",
     "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
@@ -89,6 +89,7 @@ def lib():
         L.dglm_get_time.argtypes = [_P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_int)]
         L.dglm_set_time.argtypes = [_P, C.c_double, C.c_int]
+        L.dglm_run_ensemble.argtypes = [_P, C.c_int, _P, _P, C.c_int, C.POINTER(C.c_int)]
         L.dglm_get_dt_history.argtypes = [_P, C.c_int, C.c_int, _P]
         L.dglm_rhs.argtypes = [_P, _P, _P]
         L.dglm_variant_describe.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
@@ -294,6 +295,35 @@ class Solver:
     def set_time(self, t, tstep):
         """Continue a saved run: time and step counter after set_state."""
         check(self.L.dglm_set_time(self.h, float(t), int(tstep)))
+
+    def run_ensemble_ptrs(self, in_ptrs, out_ptrs, nsteps):
+        """dglm_run_ensemble: member i reads the host fields in_ptrs[i] (nvar
+        pointers) and, after nsteps steps from t = 0, writes out_ptrs[i]; the
+        host<->device copies overlap the compute (page-locked memory).
+        Returns the index of the first non-finite member (an error is raised
+        with it) or -1."""
+        count = len(in_ptrs)
+        if len(out_ptrs) != count:
+            raise ValueError("run_ensemble: as many outputs as inputs")
+        tins = [ptr_table(p) for p in in_ptrs]
+        touts = [ptr_table(p) for p in out_ptrs]
+        tin = (C.c_void_p * max(count, 1))(*[C.cast(t, C.c_void_p) for t in tins])
+        tout = (C.c_void_p * max(count, 1))(*[C.cast(t, C.c_void_p) for t in touts])
+        bad = C.c_int(-1)
+        st = self.L.dglm_run_ensemble(self.h, count, tin, tout, int(nsteps), C.byref(bad))
+        self.first_bad = bad.value
+        check(st)
+        return bad.value
+
+    def run_ensemble(self, states, nsteps=1):
+        """Numpy front end: states is a sequence of (nvar, K*Np) arrays;
+        returns the evolved states (pageable memory: correct, not overlapped)."""
+        ins = [np.ascontiguousarray(u, dtype=np.float64).reshape(self.p.nvar, -1) for u in states]
+        outs = [np.empty_like(u) for u in ins]
+        self.run_ensemble_ptrs([[u[v].ctypes.data for v in range(self.p.nvar)] for u in ins],
+                               [[o[v].ctypes.data for v in range(self.p.nvar)] for o in outs],
+                               nsteps)
+        return outs
 
     def dt_history(self, first, count):
         out = np.zeros(count)

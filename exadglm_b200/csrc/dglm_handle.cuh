@@ -42,6 +42,14 @@ struct dglm_handle {
   std::vector<void *> allocs;
   AdjointTape *tape = nullptr;   // discrete adjoint (dglm_adjoint.cu)
   int adj_variant = 0;           // adjoint tile shape
+  // dglm_run_ensemble: double-buffered device copies of the members' input
+  // and output states, a copy-in and a copy-out stream, and their events
+  // (in_ready[2], in_free[2], out_ready[2], out_free[2])
+  double *ens_in[2] = {nullptr, nullptr}, *ens_out[2] = {nullptr, nullptr};
+  int *ens_flags = nullptr;
+  int ens_cap = 0;
+  cudaStream_t ens_cin = nullptr, ens_cout = nullptr;
+  cudaEvent_t ens_ev[8] = {};
 };
 
 

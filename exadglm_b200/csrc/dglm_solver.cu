@@ -424,6 +424,13 @@ dglm_status dglm_destroy(dglm_handle *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   drop_graphs(h);
   free_tape(h);
+  for (cudaStream_t cs : {h->ens_cin, h->ens_cout})
+    if (cs) {
+      cudaStreamSynchronize(cs);
+      cudaStreamDestroy(cs);
+    }
+  for (cudaEvent_t ev : h->ens_ev)
+    if (ev) cudaEventDestroy(ev);
   for (void *p : h->allocs) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -572,6 +579,136 @@ dglm_status dglm_get_state(dglm_handle *h, double *const *u, int on_device) {
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   return cuda_check(e, "dglm_get_state");
+}
+
+// Device-side part of dglm_set_state for a state already in h->u[0]: clear
+// t, tstep, k, the flags and the dt history, check the state for NaN/Inf and
+// compute its face wave speeds (and tau for advection).  Asynchronous.
+static cudaError_t reset_for_state(dglm_handle *h, cudaStream_t s) {
+  h->cur = 0;
+  cudaError_t e = cudaMemsetAsync(h->kreg, 0, sizeof(double) * h->nvar * h->vs, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->sc, 0, sizeof(DevScalars), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->dt_hist, 0, sizeof(double) * kHistory, s);
+  if (e == cudaSuccess)
+    e = launch_finite_check(h->u[0], h->vs, (long)h->d.K * h->Np, h->nvar, h->sc, s);
+  StageArgs a = stage_args(h, h->u[0], h->u[1], -1);
+  if (e == cudaSuccess) e = launch_face_maxv(h->d.physics, h->d.N, a, 0, s);
+  if (e == cudaSuccess && h->d.physics == DGLM_ADVECTION)
+    e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv, h->tau, s);
+  return e;
+}
+
+static dglm_status ensure_ensemble(dglm_handle *h, int count) {
+  if (!h->ens_cin) {
+    for (int b = 0; b < 2; b++) {
+      dglm_status st = dalloc(h, &h->ens_in[b], (size_t)h->nvar * h->vs);
+      if (st == DGLM_OK) st = dalloc(h, &h->ens_out[b], (size_t)h->nvar * h->vs);
+      if (st != DGLM_OK) return st;
+      // the tails past K*Np stay zero: whole buffers are copied into the state
+      cudaError_t e = cudaMemset(h->ens_in[b], 0, sizeof(double) * h->nvar * h->vs);
+      if (e != cudaSuccess) return cuda_check(e, "dglm_run_ensemble");
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&h->ens_cin, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->ens_cout, cudaStreamNonBlocking);
+    for (int i = 0; i < 8 && e == cudaSuccess; i++)
+      e = cudaEventCreateWithFlags(&h->ens_ev[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_check(e, "dglm_run_ensemble: streams/events");
+  }
+  if (count > h->ens_cap) {
+    const int cap = count > 2 * h->ens_cap ? count : 2 * h->ens_cap;
+    dglm_status st = dalloc(h, &h->ens_flags, (size_t)cap);
+    if (st != DGLM_OK) return st;
+    h->ens_cap = cap;
+  }
+  return DGLM_OK;
+}
+
+dglm_status dglm_run_ensemble(dglm_handle *h, int count, const double *const *const *in,
+                              double *const *const *out, int nsteps, int *first_bad) {
+  if (first_bad) *first_bad = -1;
+  if (!h || !in || !out) return set_error(DGLM_ERR_INVALID, "dglm_run_ensemble: NULL argument");
+  if (!h->mesh_ready) return set_error(DGLM_ERR_STATE, "dglm_run_ensemble: upload the mesh first");
+  if (count < 0 || nsteps < 0)
+    return set_error(DGLM_ERR_INVALID, "dglm_run_ensemble: negative count or step count");
+  for (int i = 0; i < count; i++) {
+    if (!in[i] || !out[i]) return set_error(DGLM_ERR_INVALID, "dglm_run_ensemble: NULL member");
+    for (int v = 0; v < h->nvar; v++)
+      if (!in[i][v] || !out[i][v])
+        return set_error(DGLM_ERR_INVALID, "dglm_run_ensemble: NULL variable pointer");
+  }
+  if (count == 0) return DGLM_OK;
+  DeviceGuard g(h->dev);
+  dglm_status st = ensure_ensemble(h, count);
+  if (st != DGLM_OK) return st;
+  // everything queued earlier on the handle's stream comes first
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_run_ensemble");
+  cudaEvent_t *in_ready = h->ens_ev, *in_free = h->ens_ev + 2, *out_ready = h->ens_ev + 4,
+              *out_free = h->ens_ev + 6;
+  const cudaStream_t S = h->stream, CI = h->ens_cin, CO = h->ens_cout;
+  const size_t n = (size_t)h->d.K * h->Np, whole = sizeof(double) * h->nvar * h->vs;
+  const int extra = h->d.physics == DGLM_ADVECTION ? 3 : 2;   // finite check, maxv, tau
+  long launches = 0;
+  h->launches = 0;
+  h->state_ready = true;   // run_steps checks it; each member sets its state first
+  // Every event is recorded (in host order) before any stream waits on that
+  // recording: member i's copy-in, compute, copy-out are enqueued in turn.
+  for (int i = 0; i < count && e == cudaSuccess; i++) {
+    const int b = i & 1;
+    // copy-in: waits until member i-2 has moved its input out of ens_in[b]
+    e = cudaStreamWaitEvent(CI, in_free[b], 0);
+    for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
+      e = cudaMemcpyAsync(h->ens_in[b] + (size_t)v * h->vs, in[i][v], sizeof(double) * n,
+                          cudaMemcpyHostToDevice, CI);
+    if (e == cudaSuccess) e = cudaEventRecord(in_ready[b], CI);
+    // compute
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(S, in_ready[b], 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->u[0], h->ens_in[b], whole, cudaMemcpyDeviceToDevice, S);
+    if (e == cudaSuccess) e = cudaEventRecord(in_free[b], S);
+    if (e == cudaSuccess) e = reset_for_state(h, S);
+    if (e != cudaSuccess) break;
+    st = run_steps(h, nsteps);
+    if (st != DGLM_OK) {
+      cudaStreamSynchronize(CI);
+      cudaStreamSynchronize(CO);
+      cudaStreamSynchronize(S);
+      return st;
+    }
+    launches += extra + h->launches;
+    h->launches = 0;
+    e = cudaStreamWaitEvent(S, out_free[b], 0);   // member i-2's copy-out is done
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h->ens_out[b], h->u[h->cur], whole, cudaMemcpyDeviceToDevice, S);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h->ens_flags + i, &h->sc->flags, sizeof(int), cudaMemcpyDeviceToDevice, S);
+    if (e == cudaSuccess) e = cudaEventRecord(out_ready[b], S);
+    // copy-out
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(CO, out_ready[b], 0);
+    for (int v = 0; v < h->nvar && e == cudaSuccess; v++)
+      e = cudaMemcpyAsync(out[i][v], h->ens_out[b] + (size_t)v * h->vs, sizeof(double) * n,
+                          cudaMemcpyDeviceToHost, CO);
+    if (e == cudaSuccess) e = cudaEventRecord(out_free[b], CO);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(CI);
+  cudaError_t e3 = cudaStreamSynchronize(S);
+  cudaError_t e4 = cudaStreamSynchronize(CO);
+  if (e == cudaSuccess) e = e2 != cudaSuccess ? e2 : (e3 != cudaSuccess ? e3 : e4);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_run_ensemble");
+  h->launches = launches;
+  std::vector<int> flags(count);
+  e = cudaMemcpy(flags.data(), h->ens_flags, sizeof(int) * count, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_run_ensemble");
+  for (int i = 0; i < count; i++) {
+    if (!(flags[i] & 7)) continue;
+    if (first_bad) *first_bad = i;
+    if (flags[i] & 4)
+      return set_error(DGLM_ERR_CUDA, "dglm_run_ensemble: a bounded wait in a pipelined "
+                                      "stage kernel expired; results are invalid");
+    return set_error(DGLM_ERR_NONFINITE,
+                     "dglm_run_ensemble: member " + std::to_string(i) +
+                         " met a non-finite wave speed, dt or state");
+  }
+  return DGLM_OK;
 }
 
 }  // extern "C"

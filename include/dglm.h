@@ -136,6 +136,21 @@ dglm_status dglm_get_time(dglm_handle *h, double *t, double *dt, int *tstep);
  * No counterpart in the reference, which has no restart; t >= 0 and
  * tstep >= 0, else DGLM_ERR_INVALID.  Synchronises the handle's stream. */
 dglm_status dglm_set_time(dglm_handle *h, double t, int tstep);
+/* Runs `count` independent initial states through the handle, each for
+ * nsteps CFL steps from t = 0: per member the work of dglm_set_state,
+ * dglm_step and dglm_get_state, without their host synchronisations.  in[i]
+ * and out[i] are HOST arrays of nvar pointers to K*Np doubles in host
+ * memory.  Member i+1's host->device copy and member i-1's device->host copy
+ * run on their own streams while member i computes (double-buffered device
+ * copies of the states), so with page-locked host memory the transfers
+ * overlap the compute and each other.  Returns when every result is in
+ * out[]; the handle then holds the last member's state and time.
+ * DGLM_ERR_NONFINITE when a member's input or steps met a non-finite value,
+ * with *first_bad (may be NULL) the first such member, else -1.  Holds
+ * 4 state-sized device buffers from the first call on.  No counterpart in
+ * the reference (one initial state per run of its executable). */
+dglm_status dglm_run_ensemble(dglm_handle *h, int count, const double *const *const *in,
+                              double *const *const *out, int nsteps, int *first_bad);
 /* dt of steps [first, first+count) taken since dglm_set_state (synchronises);
  * the history keeps the most recent 65536 steps. */
 dglm_status dglm_get_dt_history(dglm_handle *h, int first, int count, double *dt_out);

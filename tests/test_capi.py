@@ -83,6 +83,7 @@ def test_null_arguments():
     assert L.dglm_step(None, 1) == capi.ERR_INVALID
     assert L.dglm_set_state(None, None, 0) == capi.ERR_INVALID
     assert L.dglm_set_time(None, 0.5, 3) == capi.ERR_INVALID
+    assert L.dglm_run_ensemble(None, 1, None, None, 1, None) == capi.ERR_INVALID
     assert L.dglm_destroy(None) == capi.OK
 
 
