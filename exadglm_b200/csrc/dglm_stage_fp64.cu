@@ -541,23 +541,30 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
   __syncthreads();
 
   const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
-  // one flat loop over (variable, node): independent updates in flight
-  for (int vg = tid; vg < NV * ne * Np; vg += T) {
-    const int v = vg / (ne * Np), g = vg - v * (ne * Np);
-    const int e = g / Np, i = g - e * Np;
-    const int s = (v * Np + i) * EP + e;
-    const long gi = v * vs + e0 * Np + g;
-    const double rhs = sR[s];
-    if (a.rhs_only) {
-      a.u_out[gi] = rhs;
-    } else {
-      const double kn = a.rka * a.kreg[gi] + dt * rhs;
-      const double un = sU[s] + a.rkb * kn;
-      a.kreg[gi] = kn;
-      a.u_out[gi] = un;
-      sU[s] = un;
+  // one flat loop over (variable, node): independent updates in flight;
+  // nep = ne * Np is a literal for full tiles (divisions by a constant)
+  auto items = [&](const int nep) {
+    for (int vg = tid; vg < NV * nep; vg += T) {
+      const int v = vg / nep, g = vg - v * nep;
+      const int e = g / Np, i = g - e * Np;
+      const int s = (v * Np + i) * EP + e;
+      const long gi = v * vs + e0 * Np + g;
+      const double rhs = sR[s];
+      if (a.rhs_only) {
+        a.u_out[gi] = rhs;
+      } else {
+        const double kn = a.rka * a.kreg[gi] + dt * rhs;
+        const double un = sU[s] + a.rkb * kn;
+        a.kreg[gi] = kn;
+        a.u_out[gi] = un;
+        sU[s] = un;
+      }
     }
-  }
+  };
+  if (ne == E)
+    items(E * Np);
+  else
+    items(ne * Np);
   if (PHYS != EUL || !a.last_stage || a.rhs_only) return;
   __syncthreads();
 

@@ -470,22 +470,29 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
     //    shared memory only when the fused wave-speed pass reads it
     const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
     // one flat loop over (variable, node): every thread has independent
-    // updates in flight
-    for (int vg = tid; vg < NV * ne * Np; vg += TC) {
-      const int v = vg / (ne * Np), g = vg - v * (ne * Np);
-      const int e = g / Np, i = g - e * Np;
-      const long gi = v * vs + e0 * Np + g;
-      const double rhs = sR[(v * Np + i) * EP + e];
-      if (a.rhs_only) {
-        a.u_out[gi] = rhs;
-      } else {
-        const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
-        const double un = bU[v * E * Np + g] + a.rkb * kn;
-        a.kreg[gi] = kn;
-        a.u_out[gi] = un;
-        if (keep_u) bU[v * E * Np + g] = un;
+    // updates in flight.  nep = ne * Np is a literal for full tiles, so the
+    // index divisions become multiplications.
+    auto items = [&](const int nep) {
+      for (int vg = tid; vg < NV * nep; vg += TC) {
+        const int v = vg / nep, g = vg - v * nep;
+        const int e = g / Np, i = g - e * Np;
+        const long gi = v * vs + e0 * Np + g;
+        const double rhs = sR[(v * Np + i) * EP + e];
+        if (a.rhs_only) {
+          a.u_out[gi] = rhs;
+        } else {
+          const double kn = a.rka * bK[v * E * Np + g] + dt * rhs;
+          const double un = bU[v * E * Np + g] + a.rkb * kn;
+          a.kreg[gi] = kn;
+          a.u_out[gi] = un;
+          if (keep_u) bU[v * E * Np + g] = un;
+        }
       }
-    }
+    };
+    if (ne == E)
+      items(E * Np);
+    else
+      items(ne * Np);
     if (PHYS == EUL && a.last_stage && !a.rhs_only) {
       consumer_sync(TC);
       // |v|^2 and c^2 at every face node in parallel (into the rhs staging

@@ -483,10 +483,10 @@ __global__ void __launch_bounds__(
     // the new state goes back to shared memory only for the fused wave speed
     const bool keep_u = PHYS == EUL && a.last_stage && !a.rhs_only;
     // one flat loop over (variable, node): every thread has independent
-    // updates in flight
-    const int tot = NV * ne * Np;
-    auto item = [&](int vg, double kold) {
-      const int v = vg / (ne * Np), g = vg - v * (ne * Np);
+    // updates in flight.  nep = ne * Np is passed as a literal for full tiles
+    // (ne == E), so the index divisions become multiplications.
+    auto item = [&](int vg, double kold, const int nep) {
+      const int v = vg / nep, g = vg - v * nep;
       const int e = g / Np, i = g - e * Np;
       const long gi = v * vs + e0 * Np + g;
       const int ri = (v * E + e) * C::IP + i;
@@ -503,26 +503,32 @@ __global__ void __launch_bounds__(
         if (keep_u) bU[v * E * Np + g] = un;
       }
     };
-    if constexpr (C::KG) {
-      // every k of this thread is requested before the first is used
-      constexpr int IPT = (NV * E * Np + TC - 1) / TC;
-      double kr[IPT];
+    auto items = [&](const int nep) {
+      const int tot = NV * nep;
+      if constexpr (C::KG) {
+        // every k of this thread is requested before the first is used
+        constexpr int IPT = (NV * E * Np + TC - 1) / TC;
+        double kr[IPT];
 #pragma unroll
-      for (int q = 0; q < IPT; q++) {
-        const int vg = tid + q * TC;
-        kr[q] = 0.0;
-        if (vg < tot && !a.rhs_only)
-          kr[q] = a.kreg[(vg / (ne * Np)) * vs + e0 * Np + vg % (ne * Np)];
-      }
+        for (int q = 0; q < IPT; q++) {
+          const int vg = tid + q * TC;
+          kr[q] = 0.0;
+          if (vg < tot && !a.rhs_only) kr[q] = a.kreg[(vg / nep) * vs + e0 * Np + vg % nep];
+        }
 #pragma unroll
-      for (int q = 0; q < IPT; q++)
-        if (tid + q * TC < tot) item(tid + q * TC, kr[q]);
-    } else {
-      for (int vg = tid; vg < tot; vg += TC) {
-        const int v = vg / (ne * Np), g = vg - v * (ne * Np);
-        item(vg, C::S_K ? bK[v * E * Np + g] : 0.0);
+        for (int q = 0; q < IPT; q++)
+          if (tid + q * TC < tot) item(tid + q * TC, kr[q], nep);
+      } else {
+        for (int vg = tid; vg < tot; vg += TC) {
+          const int v = vg / nep, g = vg - v * nep;
+          item(vg, C::S_K ? bK[v * E * Np + g] : 0.0, nep);
+        }
       }
-    }
+    };
+    if (ne == E)
+      items(E * Np);
+    else
+      items(ne * Np);
     if (PHYS == EUL && a.last_stage && !a.rhs_only) {
       consumer_sync(TC);
       // fused calc_maxv on the new state
