@@ -858,6 +858,11 @@ static const std::vector<Variant> &variants();
 // separate volume and lift passes, KSP k-chunks, the RK register fetched by the update
 #define V_PIPEG(P, NN, E, WN, AS, KSP, PW) \
   make_pipe<P, NN, E, WN, 99, AS, 1, 0, 2, PW, KSP, false, true>()
+// as V_PIPEF / V_PIPEG with WM m-tiles per warp (m-groups x n-blocks x k-chunks)
+#define V_PIPEFW(P, NN, E, WN, WM, AS, KSP, PW) \
+  make_pipe<P, NN, E, WN, WM, AS, 1, 0, 2, PW, KSP, true>()
+#define V_PIPEGW(P, NN, E, WN, WM, KSP, PW) \
+  make_pipe<P, NN, E, WN, WM, false, 1, 0, 2, PW, KSP, false, true>()
 // pipelined split-precision mma.sync engine with the RK register fetched by the update
 #define V_PM16G(P, NN, E, WN, WM, PR, PW) \
   make_pipe<P, NN, E, WN, WM, false, 1, PR, 2, PW, 1, false, true>()
@@ -898,12 +903,15 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),
-              V_PM16G(EUL, 5, 8, 1, 2, 1, 2))
+              V_PM16G(EUL, 5, 8, 1, 2, 1, 2), V_PIPEFW(EUL, 5, 8, 5, 1, false, 1, 2),
+              V_PIPEFW(EUL, 5, 8, 5, 1, false, 2, 2), V_PIPEFW(EUL, 5, 8, 5, 2, false, 3, 2))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEG(EUL, 6, 8, 1, false, 2, 2), V_PIPEG(EUL, 6, 8, 1, false, 2, 1),
               V_PM16G(EUL, 6, 8, 1, 2, 1, 2), V_PM16G(EUL, 6, 8, 1, 2, 2, 2),
               V_PM16G(EUL, 6, 8, 1, 2, 3, 2),
-              V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3))
+              V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3),
+              V_PIPEGW(EUL, 6, 8, 5, 1, 1, 2), V_PIPEGW(EUL, 6, 8, 5, 1, 2, 2),
+              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 2))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 // N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB
 DGLM_VARIANTS(EUL, 8, V_SIMT(EUL, 8, 4, 8, 5), V_SIMT(EUL, 8, 4, 6, 5))

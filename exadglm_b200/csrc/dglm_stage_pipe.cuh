@@ -126,9 +126,10 @@ struct PCfg {
   static constexpr int NG = NG_;                        // consumer groups (ping-pong)
   static constexpr int NB = NB_;                        // tile buffers in the ring
   static constexpr int PW = PW_;                        // producer warps
-  // KSP > 1: each DMMA warp takes all m-tiles of its n-block over one of KSP
+  // KSP > 1: each DMMA warp takes its m-group x n-block over one of KSP
   // k-chunks of each contraction and stores a partial rhs; the epilogue sums
-  // the KSP partials (no padded m-tiles, fewer operand loads per DMMA)
+  // the KSP partials (with all m-tiles per warp: no padded m-tiles, fewer
+  // operand loads per DMMA)
   static constexpr int KSP = KSP_;
   // FUSE: face-flux rows sit below the volume rows, both flux phases run
   // back to back and one DMMA pass covers the stacked k range
@@ -183,7 +184,7 @@ struct PCfg {
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
   static_assert(NG == 1 || NG == 2, "one or two consumer groups");
   static_assert(NB >= 2 && NB <= 4 && PW >= 1 && PW <= 4, "ring of 2..4, 1..4 producers");
-  static_assert(KSP == 1 || (!M16 && MGROUPS == 1), "k-split takes all m-tiles per warp");
+  static_assert(KSP == 1 || !M16, "the k-split is a DMMA path");
   static_assert(!(FUSE && M16), "the fused contraction is a DMMA path");
   static_assert(FR0 % 4 == 0, "face rows start on a k-step");
   static_assert(NWC <= 32, "per-warp wave-speed maxima fit one warp");
@@ -334,11 +335,14 @@ __global__ void __launch_bounds__(
   bool ok = true;
   if (ASMEM) ok = consumer_all(mbar_wait(abar, 0), TC);
   const double *Afrag = ASMEM ? sAF : a.AT;
-  // DMMA warp roles: m-group, n-block and k-chunk (KSP > 1: one m-group)
+  // DMMA warp roles: m-group, n-block and k-chunk.  With WN = NT a warp
+  // feeds each operator fragment it loads to all n-tiles of the tile (the
+  // fragments come from global memory for the orders whose operator does
+  // not fit in shared memory)
   constexpr int NBLK = C::NT / C::WN;
-  const int mg = C::KSP > 1 ? 0 : warp % C::MGROUPS;
-  const int ng = C::KSP > 1 ? warp % NBLK : warp / C::MGROUPS;
-  const int kc = C::KSP > 1 ? warp / NBLK : 0;
+  const int mg = warp % C::MGROUPS;
+  const int ng = (warp / C::MGROUPS) % NBLK;
+  const int kc = warp / (C::MGROUPS * NBLK);
   const int m0 = mg * C::WM, n0 = ng * C::WN;
   // acc += A[:, k-steps of this warp's chunk of [0, nks)] x sB rows; the A
   // fragments of k-step ks start at Afrag + a_off + ks * MT * 32
