@@ -911,7 +911,9 @@ DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PM16G(EUL, 6, 8, 1, 2, 3, 2),
               V_M16(EUL, 6, 8, 1, 2, 2), V_M16(EUL, 6, 8, 1, 2, 1), V_M16(EUL, 6, 8, 1, 2, 3),
               V_PIPEGW(EUL, 6, 8, 5, 1, 1, 2), V_PIPEGW(EUL, 6, 8, 5, 1, 2, 2),
-              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 2))
+              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 2), V_PIPEGW(EUL, 6, 8, 5, 2, 3, 2),
+              V_PIPEGW(EUL, 6, 8, 5, 3, 2, 2), V_PIPEGW(EUL, 6, 8, 5, 3, 3, 2),
+              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 1))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 // N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB
 DGLM_VARIANTS(EUL, 8, V_SIMT(EUL, 8, 4, 8, 5), V_SIMT(EUL, 8, 4, 6, 5))
