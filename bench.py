@@ -172,6 +172,14 @@ def build_problem(a):
     return P.euler_sine(n=a.n, N=a.order, cfl=0.4)
 
 
+def workload_config(a, p, world):
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": f"euler_sine N={p.N} K={p.K} (n={a.n}^3 x 6) CFL 0.4, "
+                        f"{a.precision}, one replica per GPU",
+            "K": p.K, "N": p.N, "Np": p.Np, "nvar": p.nvar, "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (state 3 x 275 MB)"}
+
+
 def dof_stages_per_step(p):
     return p.K * p.Np * p.nvar * 5
 
@@ -234,8 +242,7 @@ def run_reference_arm(a):
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * el / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"euler_sine N={p.N} K={p.K} (n={a.n}) CFL 0.4, 1 LSERK step",
-                   "K": p.K, "N": p.N, "Np": p.Np, "nvar": 5},
+        "config": workload_config(a, p, a.gpus),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{a.steps} full LSERK steps of the K={p.K} mesh"},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -627,10 +634,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"euler_sine N={p.N} K={p.K} (n={a.n}^3 x 6) CFL 0.4, "
-                               f"{a.precision}, one replica per GPU",
-                   "K": p.K, "N": p.N, "Np": p.Np, "nvar": 5, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (state 3 x 275 MB)"},
+        "config": workload_config(a, p, world),
         "roofline": roof, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
     }
     if a.only is None and a.precision == "fp64":
