@@ -5,7 +5,7 @@
  * (nvar = 5) on one tetrahedral mesh partition.
  *
  * The reference has no library interface: its single-GPU solver is a main()
- * that reads datain/*.bin, loops runRK() and writes dataout/ snapshots
+ * that reads the .bin files of datain/, loops runRK() and writes dataout/ snapshots
  * (dim3/src/cuda/euler_nopad_main.cu:4-20), with kernels that take raw
  * device pointers (dim3/src/cuda/euler_nopad_dglm.cu, euler_nopad_time.cu).
  * This header is the boundary that replaces it:
@@ -80,7 +80,7 @@ typedef struct {
     int device;        /* CUDA device ordinal (DEVID); -1 keeps the current */
 } dglm_desc;
 
-/* Mesh and operator arrays (datain/*.bin), all HOST pointers. */
+/* Mesh and operator arrays (the .bin files of datain/), all HOST pointers. */
 typedef struct {
     const double *WDr, *WDs, *WDt;        /* Np x Np */
     const double *LIFT;                   /* Np x 4Nfp */
