@@ -143,8 +143,10 @@ dglm_status dglm_set_time(dglm_handle *h, double t, int tstep);
  * memory.  Member i+1's host->device copy and member i-1's device->host copy
  * run on their own streams while member i computes (double-buffered device
  * copies of the states), so with page-locked host memory the transfers
- * overlap the compute and each other.  Returns when every result is in
- * out[]; the handle then holds the last member's state and time.
+ * overlap the compute and each other; no in[] buffer may overlap an out[]
+ * buffer (the copies of different members run concurrently).  Returns when
+ * every result is in out[]; the handle then holds the last member's state
+ * and time.
  * DGLM_ERR_NONFINITE when a member's input or steps met a non-finite value,
  * with *first_bad (may be NULL) the first such member, else -1.  Holds
  * 4 state-sized device buffers from the first call on.  No counterpart in
