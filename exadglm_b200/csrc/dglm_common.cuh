@@ -128,6 +128,7 @@ struct StageVariantInfo {
   int fused;       // PIPE: 1 = volume and lift contractions in one DMMA pass
   int k_global;    // PIPE: 1 = the RK register is fetched by the update, not staged
   int op_global;   // PIPE: 1 = operator fragments read through L1, not staged in shared memory
+  int ctas_per_sm; // PIPE: persistent CTAs per SM (2: two independent pipelines per SM)
 };
 
 // fused FP64 stage launcher (dglm_stage_fp64.cu)

@@ -915,14 +915,17 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
     // ring depth, producer warps and k-split are named only when they differ
     // from 2, 1 and 1; the fused pass and the global RK register always
     if (v.mode == MODE_PIPE &&
-        (v.ring > 2 || v.producers > 1 || v.ksplit > 1 || v.fused || v.k_global) && n > 0 &&
+        (v.ring > 2 || v.producers > 1 || v.ksplit > 1 || v.fused || v.k_global ||
+         v.ctas_per_sm > 1) && n > 0 &&
         (size_t)n < len) {
       int m = snprintf(buf + n, len - n, " ring=%d prod=%d", v.ring, v.producers);
       if (v.ksplit > 1 && m > 0 && (size_t)(n + m) < len)
         m += snprintf(buf + n + m, len - n - m, " ksplit=%d", v.ksplit);
       if (m > 0 && (size_t)(n + m) < len)
-        snprintf(buf + n + m, len - n - m, "%s%s", v.fused ? " fused" : "",
-                 v.k_global ? " k=global" : "");
+        m += snprintf(buf + n + m, len - n - m, "%s%s", v.fused ? " fused" : "",
+                      v.k_global ? " k=global" : "");
+      if (v.ctas_per_sm > 1 && m > 0 && (size_t)(n + m) < len)
+        snprintf(buf + n + m, len - n - m, " ctas=%d", v.ctas_per_sm);
     }
   }
   return DGLM_OK;

@@ -738,23 +738,23 @@ static int sm_count() {
 }
 
 template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG, int PR, int NB, int PW,
-          int KSP, bool FU, bool KG>
+          int KSP, bool FU, bool KG, int CPS>
 static cudaError_t launch_pipe(const StageArgs &a, cudaStream_t s) {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>;
-  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG, CPS>;
+  auto k = stage_pipe_kernel<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG, CPS>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
   const int ntiles = (a.K + E - 1) / E;
-  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  const int grid = ntiles < CPS * sm_count() ? ntiles : CPS * sm_count();
   k<<<grid, C::THREADS, C::SMEM, s>>>(a, ntiles);
   return cudaGetLastError();
 }
 
 template <int PHYS, int N, int E, int WN, int WM, bool AS, int NG = 1, int PR = 0, int NB = 2,
-          int PW = 1, int KSP = 1, bool FU = false, bool KG = false>
+          int PW = 1, int KSP = 1, bool FU = false, bool KG = false, int CPS = 1>
 static Variant make_pipe() {
-  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>;
+  using C = PCfg<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG, CPS>;
   StageVariantInfo i{};
   i.mode = PR ? MODE_MMA16 : MODE_PIPE;
   i.E = E;
@@ -775,11 +775,12 @@ static Variant make_pipe() {
   i.fused = FU ? 1 : 0;
   i.k_global = KG ? 1 : 0;
   i.op_global = AS ? 0 : 1;
+  i.ctas_per_sm = CPS;
   if (PR) {
     i.prec = PR == 2 ? DGLM_PREC_TF32X3 : PR == 3 ? DGLM_PREC_BF16X6 : DGLM_PREC_BF16X3;
     i.kstep = C::KSTEP16;
   }
-  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG>};
+  return Variant{i, &launch_pipe<PHYS, N, E, WN, WM, AS, NG, PR, NB, PW, KSP, FU, KG, CPS>};
 }
 
 template <int PHYS, int N, int E, int PREC, int NWC, int PW>
@@ -863,6 +864,9 @@ static const std::vector<Variant> &variants();
   make_pipe<P, NN, E, WN, WM, AS, 1, 0, 2, PW, KSP, true>()
 #define V_PIPEGW(P, NN, E, WN, WM, KSP, PW) \
   make_pipe<P, NN, E, WN, WM, false, 1, 0, 2, PW, KSP, false, true>()
+// two persistent CTAs per SM: separate passes, RK register from global memory
+#define V_PIPE2C(P, NN, E, WN, WM, KSP, PW) \
+  make_pipe<P, NN, E, WN, WM, false, 1, 0, 2, PW, KSP, false, true, 2>()
 // pipelined split-precision mma.sync engine with the RK register fetched by the update
 #define V_PM16G(P, NN, E, WN, WM, PR, PW) \
   make_pipe<P, NN, E, WN, WM, false, 1, PR, 2, PW, 1, false, true>()
@@ -899,7 +903,8 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_M16(EUL, 4, 8, 1, 3, 2), V_M16(EUL, 4, 8, 1, 1, 1), V_M16(EUL, 4, 8, 1, 1, 3),
               V_PM16(EUL, 4, 8, 1, 3, 1), V_PIPER(EUL, 4, 8, 1, 2, true, 2, 2),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
-              V_PIPEF(EUL, 4, 8, 1, true, 3, 1))
+              V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
+              V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),

@@ -2,8 +2,8 @@
 // dglm_stage_fp64.cu, which defines EUL/ADV, euler_flux_fast and
 // dmma_8x8x4).
 //
-// One CTA per SM walks the element tiles t = blockIdx.x, +gridDim.x, ...
-// with a ring of two to four shared-memory tile buffers:
+// One CTA per SM (or two, CPS = 2) walks the element tiles t = blockIdx.x,
+// +gridDim.x, ... with a ring of two to four shared-memory tile buffers:
 //
 //   producer warps  TMA bulk copies (cp.async.bulk, mbarrier complete_tx) of
 //                   the next tile's state u, RK register k, metrics, face
@@ -108,7 +108,8 @@ __device__ __forceinline__ bool consumer_all(bool v, int nthreads) {
 }
 
 template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_ = 1, int PR_ = 0,
-          int NB_ = 2, int PW_ = 1, int KSP_ = 1, bool FU_ = false, bool KG_ = false>
+          int NB_ = 2, int PW_ = 1, int KSP_ = 1, bool FU_ = false, bool KG_ = false,
+          int CPS_ = 1>
 struct PCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -137,6 +138,9 @@ struct PCfg {
   // KG: the RK register is not staged; the update fetches it from global
   // memory (orders whose staged tiles would not fit twice otherwise)
   static constexpr bool KG = KG_;
+  // CPS: persistent CTAs per SM.  Two independent pipelines on one SM let
+  // one CTA's DMMA pass run while the other computes fluxes or updates
+  static constexpr int CPS = CPS_;
   static constexpr int NWC = (M16 ? MG16 : MGROUPS) * (NT / WN) * KSP;   // consumer warps per group
   static constexpr int TC = 32 * NWC;                   // consumer threads per group
   static constexpr int THREADS = NG * TC + 32 * PW;     // + producer warps
@@ -182,6 +186,8 @@ struct PCfg {
   static_assert(NCOL % 8 == 0 && NT % WN == 0, "n-tiles must split over the warps");
   static_assert((E * Np * 8) % 16 == 0 && (E * 8) % 16 == 0, "bulk copies need 16-byte sizes");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
+  static_assert(CPS == 1 || (CPS == 2 && 2 * (SMEM + 1024) <= 233472 && THREADS <= 1024),
+                "two CTAs per SM must share its 228 KB of shared memory");
   static_assert(NG == 1 || NG == 2, "one or two consumer groups");
   static_assert(NB >= 2 && NB <= 4 && PW >= 1 && PW <= 4, "ring of 2..4, 1..4 producers");
   static_assert(KSP == 1 || !M16, "the k-split is a DMMA path");
@@ -275,11 +281,11 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
 }
 
 template <int PHYS, int N, int E_, int WN_, int WM_, bool ASMEM, int NG_, int PR_, int NB_,
-          int PW_, int KSP_, bool FU_, bool KG_>
+          int PW_, int KSP_, bool FU_, bool KG_, int CPS_>
 __global__ void __launch_bounds__(
-    PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_, KG_>::THREADS, 1)
+    PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_, KG_, CPS_>::THREADS, CPS_)
     stage_pipe_kernel(const StageArgs a, int ntiles) {
-  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_, KG_>;
+  using C = PCfg<PHYS, N, E_, WN_, WM_, ASMEM, NG_, PR_, NB_, PW_, KSP_, FU_, KG_, CPS_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E,
                 BLD = C::BLD, TC = C::TC;
   extern __shared__ __align__(16) double smem[];
