@@ -325,6 +325,23 @@ class Solver:
                                nsteps)
         return outs
 
+    def save_full_state(self, dirpath, print_interval=0):
+        """Write the current state and time as a full-state snapshot (the
+        format of ``dglm_main --full-state``); returns the step number."""
+        from .datain import write_full_state
+        t, _, tstep = self.time()
+        write_full_state(dirpath, tstep, self.p.physics, self.get_state(), t, print_interval)
+        return tstep
+
+    def restart(self, dirpath, tstep):
+        """Continue from a full-state snapshot: set_state + set_time."""
+        from .datain import read_full_state
+        u, t, step, _ = read_full_state(dirpath, tstep, self.p.physics,
+                                        n=self.p.K * self.p.Np)
+        self.set_state(u)
+        self.set_time(t, step)
+        return t, step
+
     def dt_history(self, first, count):
         out = np.zeros(count)
         check(self.L.dglm_get_dt_history(self.h, int(first), int(count), _np_ptr(out)))

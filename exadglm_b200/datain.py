@@ -8,6 +8,11 @@ The four operator matrices are stored 'c' (row-major) for the CPU solver and
 every other array is stored flat in C order.  Snapshots are
 ``u_NNNNNNN.bin`` (advection) and ``u1_NNNNNNN.bin`` (Euler density) with a
 7-digit zero-padded step (advec_data.cpp:287-291, euler_data.cpp:287-294).
+
+Full state (not in the reference, which writes only the first variable and
+cannot restart): the other Euler variables as ``u2_`` .. ``u5_NNNNNNN.bin``
+and ``t_NNNNNNN.bin``, three float64 values (t, the step number, the print
+interval; 0 when unknown).  ``dglm_main --full-state`` writes the same bytes.
 """
 from __future__ import annotations
 
@@ -95,3 +100,69 @@ def write_snapshot(dirpath, tstep, physics, u_first_var):
     path = os.path.join(dirpath, snapshot_name(tstep, physics))
     np.ascontiguousarray(u_first_var, dtype=np.float64).tofile(path)
     return path
+
+
+def _step(tstep):
+    s = str(int(tstep))
+    if int(tstep) < 0 or len(s) > TDIGIT:
+        raise ValueError(f"step {tstep} does not fit the {TDIGIT}-digit snapshot names")
+    return "0" * (TDIGIT - len(s)) + s
+
+
+def field_name(v, tstep, physics):
+    """Snapshot file of variable v (0-based): ``u_`` (advection),
+    ``u1_`` .. ``u5_`` (Euler)."""
+    if physics == "euler":
+        if not 0 <= v < 5:
+            raise ValueError("Euler has variables 0..4")
+        return f"u{v + 1}_" + _step(tstep) + ".bin"
+    if v != 0:
+        raise ValueError("advection has one variable")
+    return "u_" + _step(tstep) + ".bin"
+
+
+def time_name(tstep):
+    return "t_" + _step(tstep) + ".bin"
+
+
+def write_full_state(dirpath, tstep, physics, u, t, print_interval=0):
+    """Every variable of u (nvar, K*Np) and the time file of step tstep."""
+    nvar = 5 if physics == "euler" else 1
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(nvar, -1)
+    os.makedirs(dirpath, exist_ok=True)
+    for v in range(nvar):
+        u[v].tofile(os.path.join(dirpath, field_name(v, tstep, physics)))
+    np.array([t, tstep, print_interval], dtype=np.float64).tofile(
+        os.path.join(dirpath, time_name(tstep)))
+
+
+def read_full_state(dirpath, tstep, physics, n=None):
+    """(u (nvar, n), t, tstep, print_interval) of a full-state snapshot;
+    n = K*Np is checked when given."""
+    nvar = 5 if physics == "euler" else 1
+    fields = []
+    for v in range(nvar):
+        f = np.fromfile(os.path.join(dirpath, field_name(v, tstep, physics)), dtype=np.float64)
+        if n is not None and f.size != n:
+            raise ValueError(f"{field_name(v, tstep, physics)} holds {f.size} values, "
+                             f"expected {n}")
+        if fields and f.size != fields[0].size:
+            raise ValueError("the fields of the snapshot differ in size")
+        fields.append(f)
+    tt = np.fromfile(os.path.join(dirpath, time_name(tstep)), dtype=np.float64)
+    if tt.size != 3 or int(round(tt[1])) != int(tstep):
+        raise ValueError(f"{time_name(tstep)} is not the time file of step {tstep}")
+    return np.stack(fields), float(tt[0]), int(round(tt[1])), int(round(tt[2]))
+
+
+def full_state_steps(dirpath, physics):
+    """Steps of dirpath that have every field and the time file."""
+    nvar = 5 if physics == "euler" else 1
+    steps = []
+    for name in sorted(os.listdir(dirpath)):
+        if name.startswith("t_") and name.endswith(".bin") and name[2:-4].isdigit():
+            k = int(name[2:-4])
+            if all(os.path.exists(os.path.join(dirpath, field_name(v, k, physics)))
+                   for v in range(nvar)):
+                steps.append(k)
+    return steps

@@ -125,12 +125,16 @@ class DGLM3DBase:
     def build(self, filename_list=None, verbose=1):
         _build.build(verbose=verbose >= 2)
 
-    def run(self, filename, omp_threads=None, verbose=1):
-        """Run the solver; returns (last_tstep, avg_dt, elapsed_time) parsed
-        from its stdout as the reference does (launcher :283-325)."""
+    def command(self, filename, full_state=False, restart_dir=None, restart_step=None):
+        """The dglm_main command line for the executable name the notebook
+        passes (advec_* or euler_*).  full_state writes every variable and
+        the time file with each snapshot; restart_dir/restart_step continue
+        from such a snapshot (neither is in the reference)."""
         physics = "advection" if os.path.basename(filename).startswith("advec") else "euler"
         if (physics == "euler") != (self.Nvar == 5):
             raise ValueError(f"{filename} does not match Nvar={self.Nvar}")
+        if (restart_dir is None) != (restart_step is None):
+            raise ValueError("restart_dir and restart_step go together")
         cmd = [_build.MAIN, "--datain", self.datain_dir, "--dataout", self.dataout_dir,
                "--physics", physics, "--tmax", repr(float(self.tmax)),
                "--cfl", repr(float(self.param["CFL"])),
@@ -139,6 +143,17 @@ class DGLM3DBase:
                "--device", str(getattr(self, "devid", 0)),
                "--matrix-order", getattr(self, "matrix_order", "c"),
                "--precision", self.precision]
+        if full_state:
+            cmd.append("--full-state")
+        if restart_dir is not None:
+            cmd += ["--restart-dir", str(restart_dir), "--restart-step", str(int(restart_step))]
+        return cmd
+
+    def run(self, filename, omp_threads=None, verbose=1, full_state=False, restart_dir=None,
+            restart_step=None):
+        """Run the solver; returns (last_tstep, avg_dt, elapsed_time) parsed
+        from its stdout as the reference does (launcher :283-325)."""
+        cmd = self.command(filename, full_state, restart_dir, restart_step)
         if verbose >= 1:
             print(" ".join(cmd))
         t0 = time.perf_counter()

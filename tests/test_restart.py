@@ -58,6 +58,28 @@ def test_solver_restart_is_bitwise(phys):
 
 
 @pytest.mark.gpu
+def test_solver_full_state_files_restart_bitwise(tmp_path):
+    """Solver.save_full_state at step 12, Solver.restart in a fresh handle,
+    18 more steps: the state of the straight 30-step run, bit for bit."""
+    from exadglm_b200.capi import Solver
+    prob = P.euler_sine(n=3, N=4, noise=1e-3, seed=1)
+    a = Solver(prob)
+    a.step(30)
+    ua, ta = a.get_state(), a.time()
+    a.close()
+    b = Solver(prob)
+    b.step(12)
+    assert b.save_full_state(str(tmp_path), print_interval=6) == 12
+    b.close()
+    c = Solver(prob)
+    assert c.restart(str(tmp_path), 12)[1] == 12
+    c.step(18)
+    np.testing.assert_array_equal(c.get_state(), ua)
+    assert c.time()[0] == ta[0] and c.time()[2] == 30
+    c.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("Nvar", [5, 1])
 def test_driver_restart_is_bitwise(tmp_path, Nvar):
     """dglm_main --full-state, then --restart-dir/--restart-step from an
