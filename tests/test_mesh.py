@@ -72,6 +72,38 @@ def test_volume_and_normals():
     np.testing.assert_allclose(nf + nf[F], 0.0, atol=1e-14)
 
 
+@pytest.mark.parametrize("N,n", [(3, 3), (4, 2)])
+def test_face_jacobian_matches_triangle_areas(N, n):
+    """2 sJ is the physical area of a face (the reference face has area 2 in
+    the face parametrisation, sum(Emat) = 8 over 4 faces), with sJ = Fscale J.
+    Summed over all faces it equals the summed surface areas of the tets
+    computed from their vertices (test_mesh_3d_common.py's sJ check, in a
+    form independent of the face numbering)."""
+    m = uniform_mesh(N, n)
+    sJ = m.Fscale * m.J[:, None]
+    V = np.stack([m.VX, m.VY, m.VZ], axis=1)[m.EtoV]             # (K, 4, 3)
+    area = 0.0
+    for tri in ((0, 1, 2), (0, 1, 3), (1, 2, 3), (0, 2, 3)):
+        a, b, c = V[:, tri[0]], V[:, tri[1]], V[:, tri[2]]
+        area += 0.5 * np.linalg.norm(np.cross(b - a, c - a), axis=1).sum()
+    assert (2.0 * sJ).sum() == pytest.approx(area, rel=1e-13)
+    assert np.all(sJ > 0)
+
+
+@pytest.mark.parametrize("N,n", [(3, 3), (5, 2)])
+def test_normals_orthogonal_to_their_faces(N, n):
+    """n is orthogonal to every chord between two nodes of its face
+    (test_mesh_3d_common.py's normal orthogonality)."""
+    m = uniform_mesh(N, n)
+    X = np.stack([m.PX, m.PY, m.PZ], axis=-1)                      # (K, Np, 3)
+    nrm = np.stack([m.NX, m.NY, m.NZ], axis=-1)                    # (K, 4, 3)
+    for f in range(4):
+        pts = X[:, m.ref.Fmask[f]]                                 # (K, Nfp, 3)
+        chords = pts - pts[:, :1]
+        dots = np.einsum("kjd,kd->kj", chords, nrm[:, f])
+        assert np.abs(dots).max() < 1e-13
+
+
 def test_element_counts():
     b = UniformBox(7, 7, 7)
     assert b.Nelem == 1296 and b.EtoV.shape == (1296, 4)
