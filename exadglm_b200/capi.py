@@ -404,6 +404,13 @@ class Solver:
             self.L.dglm_destroy(self.h)
             self.h = None
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
     def __del__(self):
         try:
             self.close()
@@ -477,6 +484,13 @@ class BatchSolver:
         if getattr(self, "h", None):
             self.L.dglm_batch_destroy(self.h)
             self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
 
     def __del__(self):
         try:

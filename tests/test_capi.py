@@ -104,3 +104,26 @@ def test_library_fails_loudly_when_missing(monkeypatch):
     monkeypatch.setattr(capi, "_lib", None)
     with pytest.raises(RuntimeError, match="missing"):
         capi.lib()
+
+
+def test_handles_close_once_in_with_blocks():
+    """Solver and BatchSolver release their handle on leaving a with block,
+    once, also when the block raises (checked with a fake library)."""
+    calls = []
+
+    class FakeLib:
+        def dglm_destroy(self, h):
+            calls.append(("solver", h))
+
+        def dglm_batch_destroy(self, h):
+            calls.append(("batch", h))
+
+    for cls, tag in ((capi.Solver, "solver"), (capi.BatchSolver, "batch")):
+        obj = cls.__new__(cls)
+        obj.L, obj.h = FakeLib(), 1234
+        with pytest.raises(RuntimeError):
+            with obj as o:
+                assert o is obj
+                raise RuntimeError("inside")
+        obj.close()
+        assert calls.count((tag, 1234)) == 1 and obj.h is None
