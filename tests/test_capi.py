@@ -127,3 +127,20 @@ def test_handles_close_once_in_with_blocks():
                 raise RuntimeError("inside")
         obj.close()
         assert calls.count((tag, 1234)) == 1 and obj.h is None
+
+
+def test_every_tuned_entry_resolves_to_its_variant(monkeypatch):
+    """Each entry of tuned.json names a compiled variant (matched by shape,
+    shared-memory size left out), so no pick silently falls back to variant 0
+    after a variant list or description changes."""
+    from exadglm_b200 import tune
+    table = tune.load_cache()
+    assert table, "tuned.json is empty"
+    for key, ent in table.items():
+        dev, physics, order, prec = key.split("|")
+        monkeypatch.setattr(tune, "_device_name", lambda device=0, d=dev: d)
+        v = tune.cached_variant(physics, int(order[1:]), prec)
+        assert v is not None, (key, ent["desc"])
+        desc = capi.variants(physics, int(order[1:]))[v]
+        assert tune._shape(desc) == tune._shape(ent["desc"]), key
+        assert capi.variant_precision(desc) == prec, (key, desc)
