@@ -87,3 +87,36 @@ def test_rk_coefficients():
     assert a[0] == 0.0 and c[0] == 0.0
     # consistency of the 2N-storage scheme: c_{s} = sum of b weights up to s
     assert c[1] == pytest.approx(b[0], rel=1e-15)
+
+
+def _integrals(p, u):
+    w = p.mesh.ref.M.sum(axis=0)
+    U = np.asarray(u).reshape(p.nvar, p.K, p.Np)
+    return (np.einsum("k,vki,i->v", p.mesh.J, U, w),
+            np.einsum("k,vki,i->v", np.abs(p.mesh.J), np.abs(U), np.abs(w)))
+
+
+@pytest.mark.parametrize("phys,N", [("euler", 4), ("euler", 6), ("advection", 3)])
+def test_oracle_conserves_every_variable(phys, N):
+    """On a periodic mesh the scheme conserves the mass-weighted integral of
+    each conserved variable up to rounding (the property the full-size GPU
+    runs are checked by)."""
+    p = (P.euler_sine(n=3, N=N, noise=1e-3, seed=N) if phys == "euler"
+         else P.advection_gaussian(n=3, N=N, width2=0.05))
+    i0, mag = _integrals(p, p.u0)
+    u, _, _, _ = oracle.Oracle(p).run(20)
+    i1, _ = _integrals(p, u)
+    assert np.all(np.abs(i1 - i0) / mag < 1e-13), np.abs(i1 - i0) / mag
+
+
+def test_oracle_restart_from_u_and_t_is_exact():
+    """(u, t, step) is a complete restart state: the first LSERK coefficient
+    is zero, so the RK register carries nothing across a step boundary, and dt
+    comes from the state.  12 + 18 steps equal 30 steps bit for bit."""
+    p = P.euler_sine(n=3, N=4, noise=1e-3, seed=3)
+    o = oracle.Oracle(p)
+    u30, _, c30, d30 = o.run(30)
+    u12, _, c12, d12 = o.run(12)
+    u18, _, c18, d18 = o.run(18, u=u12)
+    np.testing.assert_array_equal(u18, u30)
+    np.testing.assert_array_equal(np.concatenate([d12, d18]), d30)
