@@ -7,9 +7,13 @@ Modules:
   refelem   reference-tetrahedron nodes and operators (WDr/WDs/WDt, LIFT, Fmask)
   mesh      uniform box meshes and their DG geometry (vmapP, metrics, normals)
   problem   problem set-ups (initial states, parameters) and the L2 error
-  datain    the reference's datain/dataout binary formats
-  capi      ctypes binding of libdglm.so (Solver handle, per-kernel entry points)
+  datain    the reference's datain/dataout binary formats, plus full-state
+            snapshots (every variable and t) for restart
+  capi      ctypes binding of libdglm.so (Solver and BatchSolver handles,
+            ensembles with overlapped host copies, per-kernel entry points)
+  adjoint   discrete adjoint behind torch.autograd (DGLMStep, evolve)
+  tune      timing of the compiled tile shapes, tuned.json lookup
   launcher  drop-in for the reference's DGLM3DSingleGPU launcher class
-  build     nvcc build of libdglm.so
+  build     nvcc build of libdglm.so and the dglm_main driver
 """
 __version__ = "0.1.0"
