@@ -88,3 +88,16 @@ def test_ensemble_reports_first_nonfinite_member():
     for i, r in zip((0, 1, 3), ref):
         np.testing.assert_array_equal(outs[i], r)
     s.close()
+
+
+def test_ensemble_on_a_fresh_handle():
+    """The first call on a handle captures the step graph inside the
+    pipelined loop (copies and event waits still queued on its stream)."""
+    from exadglm_b200.capi import Solver
+    prob = P.euler_sine(n=3, N=4, noise=1e-3, seed=7)
+    states = members(prob, 3, seed=5)
+    with Solver(prob) as fresh, Solver(prob) as ref_solver:
+        got = fresh.run_ensemble(states, 4)
+        ref = sequential(ref_solver, states, 4)
+        for i, (a, b) in enumerate(zip(got, ref)):
+            np.testing.assert_array_equal(a, b, err_msg=f"member {i}")
