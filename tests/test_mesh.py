@@ -112,3 +112,21 @@ def test_element_counts():
 def test_rejects_degenerate_periodic_axis():
     with pytest.raises(ValueError):
         UniformBox(2, 4, 4)
+
+
+def test_l2_error_matches_per_element_loop():
+    """The vectorised mass-weighted L2 error (a14) against a loop over the
+    elements written as dglm_3d_launcher.py:328-355 computes it:
+    sum_e J_e (u_ref - interpM u_num)^T high_M (u_ref - interpM u_num)."""
+    from exadglm_b200 import problem as P
+    p = P.euler_sine(n=2, N=3)
+    ref = p.mesh.ref
+    rng = np.random.default_rng(4)
+    u_num = rng.standard_normal(p.K * p.Np)
+    u_ref = rng.standard_normal(p.K * ref.high_Np)
+    total = 0.0
+    for e in range(p.K):
+        E = u_ref[e * ref.high_Np:(e + 1) * ref.high_Np] - ref.interpM @ u_num[e * p.Np:(e + 1) * p.Np]
+        total += p.mesh.J[e] * (E @ ref.high_M @ E)
+    assert P.l2_error(p, u_ref, u_num, apply_sqrt=False) == pytest.approx(total, rel=1e-13)
+    assert P.l2_error(p, u_ref, u_num) == pytest.approx(np.sqrt(total), rel=1e-13)
