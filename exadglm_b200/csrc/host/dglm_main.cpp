@@ -39,7 +39,8 @@ namespace {
 const double kPi = 3.14159265358979323846;
 
 template <typename T>
-bool read_bin(const std::string &path, std::vector<T> &v, size_t count, bool required = true) {
+bool read_bin(const std::string &path, std::vector<T> &v, size_t count, bool required = true,
+              bool exact = false) {
   std::ifstream f(path, std::ios::binary | std::ios::ate);
   if (!f) {
     if (required) std::fprintf(stderr, "dglm_main: cannot read %s\n", path.c_str());
@@ -47,7 +48,7 @@ bool read_bin(const std::string &path, std::vector<T> &v, size_t count, bool req
   }
   const size_t bytes = (size_t)f.tellg();
   if (count == 0) count = bytes / sizeof(T);
-  if (bytes < count * sizeof(T)) {
+  if (bytes < count * sizeof(T) || (exact && bytes != count * sizeof(T))) {
     std::fprintf(stderr, "dglm_main: %s holds %zu bytes, expected %zu\n", path.c_str(), bytes,
                  count * sizeof(T));
     return false;
@@ -192,13 +193,19 @@ int main(int argc, char **argv) {
     u0.assign(nvar * n, 0.0);
     for (int v = 0; v < nvar; v++) {
       std::vector<double> f;
-      if (!read_bin(restart_dir + field_name(v, restart_step, euler), f, n)) return 1;
+      if (!read_bin(restart_dir + field_name(v, restart_step, euler), f, n, true, true))
+        return 1;
       std::copy(f.begin(), f.end(), u0.begin() + v * n);
     }
     std::vector<double> tt;
-    if (!read_bin(restart_dir + time_name(restart_step), tt, 3)) return 1;
+    if (!read_bin(restart_dir + time_name(restart_step), tt, 3, true, true)) return 1;
     t0 = tt[0];
     tstep0 = (int)std::llround(tt[1]);
+    if (tstep0 != restart_step || !(t0 >= 0)) {
+      std::fprintf(stderr, "dglm_main: %s holds step %d at t=%g, not step %d\n",
+                   time_name(restart_step).c_str(), tstep0, t0, restart_step);
+      return 1;
+    }
     print_tstep = (int)std::llround(tt[2]);   // keeps the original run's interval
   } else if (!read_bin(datain + "u0.bin", u0, nvar * n, false)) {
     u0.assign(nvar * n, 0.0);

@@ -24,6 +24,32 @@ def test_driver_rejects_restart_dir_without_step(tmp_path):
     assert r.returncode == 2 and "--restart-step" in r.stderr
 
 
+def test_driver_rejects_mismatched_snapshots(tmp_path):
+    """A field file of the wrong size or a time file of another step stops
+    dglm_main before it touches the GPU."""
+    if not os.path.exists(_build.MAIN):
+        pytest.skip("dglm_main not built")
+    from exadglm_b200.datain import field_name, time_name, write_full_state
+    dg, _ = notebook_launcher(tmp_path, 5, nx=4, N=3, tmax=0.5)
+    n = dg.Nelem * dg.Np
+    snap = str(tmp_path / "snap")
+    write_full_state(snap, 5, "euler", np.ones((5, n)), 0.1, 2)
+    base = [_build.MAIN, "--datain", dg.datain_dir, "--dataout", str(tmp_path), "--physics",
+            "euler", "--tmax", "1", "--matrix-order", "f", "--restart-dir", snap,
+            "--restart-step", "5"]
+
+    def run():
+        return subprocess.run(base, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+
+    np.ones(n + 1).tofile(os.path.join(snap, field_name(2, 5, "euler")))
+    r = run()
+    assert r.returncode != 0 and "expected" in r.stderr and field_name(2, 5, "euler") in r.stderr
+    np.ones(n).tofile(os.path.join(snap, field_name(2, 5, "euler")))
+    np.array([0.1, 6.0, 2.0]).tofile(os.path.join(snap, time_name(5)))
+    r = run()
+    assert r.returncode != 0 and "holds step 6" in r.stderr, r.stderr
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("phys", ["euler", "advection"])
 def test_solver_restart_is_bitwise(phys):
