@@ -275,6 +275,50 @@ class Mesh3D:
         }
 
 
+def compact_face_maps(vmapP, ref, Np):
+    """Compact form of a face map: per face (e, f) the neighbour element
+    EtoE, its face EtoF and an orientation index EtoR into the table T of
+    _face_node_perm, with vmapP[e, f, j] = EtoE Np + Fmask[EtoF, T[f, EtoF,
+    EtoR, j]].  Derived from vmapP alone (any datain/vmapP.bin of this
+    order); faces mapped onto themselves (vmapP = vmapM) get (e, f, 0).
+    6 bytes per face instead of 4 Nfp.  Raises ValueError when a face's
+    trace is not one whole face of one element."""
+    Nfp = ref.Nfp
+    vP = np.asarray(vmapP, dtype=np.int64).reshape(-1, 4, Nfp)
+    e2 = vP // Np
+    if np.any(e2 != e2[:, :, :1]):
+        raise ValueError("a face's trace spans several elements")
+    local = vP % Np
+    T, _ = _face_node_perm(ref)
+    EtoF = np.full(vP.shape[:2], -1, np.int64)
+    jpos = np.zeros_like(local)
+    for g in range(4):
+        inv = np.full(Np, -1, np.int64)
+        inv[ref.Fmask[g]] = np.arange(Nfp)
+        pos = inv[local]
+        whole = np.all(pos >= 0, axis=2)
+        EtoF[whole] = g
+        jpos[whole] = pos[whole]
+    if np.any(EtoF < 0):
+        raise ValueError("a face's trace is not one face of its neighbour")
+    f = np.broadcast_to(np.arange(4), EtoF.shape)
+    cand = T[f, EtoF]                                               # (K,4,6,Nfp)
+    match = np.all(cand == jpos[:, :, None, :], axis=3)             # (K,4,6)
+    if not np.all(match.any(axis=2)):
+        raise ValueError("a face's node order is no rotation or reflection of its neighbour's")
+    EtoR = match.argmax(axis=2)
+    return e2[:, :, 0].astype(np.int32), EtoF.astype(np.uint8), EtoR.astype(np.uint8)
+
+
+def expand_face_maps(EtoE, EtoF, EtoR, ref, Np):
+    """vmapP (K, 4, Nfp) int32 from the compact form of compact_face_maps."""
+    T, _ = _face_node_perm(ref)
+    EtoE, EtoF, EtoR = (np.asarray(x, dtype=np.int64) for x in (EtoE, EtoF, EtoR))
+    f = np.broadcast_to(np.arange(4), EtoF.shape)
+    j2 = T[f, EtoF, EtoR]                                           # (K,4,Nfp)
+    return (EtoE[:, :, None] * Np + ref.Fmask[EtoF[:, :, None], j2]).astype(np.int32)
+
+
 def uniform_mesh(N, n, interpN=2, high_order=False, lo=0.0, hi=1.0, bc=None):
     """Periodic (by default) unit-cube mesh of n^3 hexahedra x 6 tets."""
     box = UniformBox(n + 1, n + 1, n + 1, lo, hi, lo, hi, lo, hi, bc=bc)

@@ -130,3 +130,32 @@ def test_l2_error_matches_per_element_loop():
         total += p.mesh.J[e] * (E @ ref.high_M @ E)
     assert P.l2_error(p, u_ref, u_num, apply_sqrt=False) == pytest.approx(total, rel=1e-13)
     assert P.l2_error(p, u_ref, u_num) == pytest.approx(np.sqrt(total), rel=1e-13)
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("tag", ["pbc", "mixed"])
+def test_compact_face_maps_regenerate_vmapP(N, tag):
+    """(EtoE, EtoF, orientation) per face regenerates vmapP exactly, for
+    periodic faces and for boundary faces that map onto themselves; 24 bytes
+    per element against 16 Nfp."""
+    from exadglm_b200.mesh import compact_face_maps, expand_face_maps
+    m = Mesh3D(N, UniformBox(4, 3, 3, bc=CASES[tag]), high_order=False)
+    EtoE, EtoF, EtoR = compact_face_maps(m.vmapP, m.ref, m.Np)
+    np.testing.assert_array_equal(expand_face_maps(EtoE, EtoF, EtoR, m.ref, m.Np), m.vmapP)
+    assert EtoE.nbytes + EtoF.nbytes + EtoR.nbytes == 24 * m.Nelem
+    inner = m.EtoE >= 0
+    np.testing.assert_array_equal(EtoE[inner], m.EtoE[inner])
+    np.testing.assert_array_equal(EtoF[inner], m.EtoF[inner])
+
+
+def test_compact_face_maps_reject_broken_maps():
+    from exadglm_b200.mesh import compact_face_maps
+    m = uniform_mesh(3, 2)
+    bad = m.vmapP.copy()
+    bad[0, 0, 0] = bad[5, 2, 0]          # one node from another element
+    with pytest.raises(ValueError):
+        compact_face_maps(bad, m.ref, m.Np)
+    bad = m.vmapP.copy()
+    bad[0, 0, [1, 2]] = bad[0, 0, [2, 1]]  # not a rotation or reflection
+    with pytest.raises(ValueError):
+        compact_face_maps(bad, m.ref, m.Np)
