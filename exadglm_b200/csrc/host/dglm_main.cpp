@@ -10,7 +10,7 @@
 // The compile-time common.h parameters of the reference become flags:
 //   --datain DIR --dataout DIR --physics euler|advection --tmax T
 //   [--cfl 0.8] [--gamma 1.4] [--tau-scale 1.2] [--device 0]
-//   [--matrix-order f|c] [--precision fp64|tf32x3|bf16x3] [--variant V]
+//   [--matrix-order f|c] [--precision fp64|tf32x3|bf16x3|bf16x6] [--variant V]
 // Full state and restart (not in the reference, which writes only u1):
 //   --full-state            every snapshot also writes the other fields
 //                           (u2..u5_NNNNNNN.bin for Euler) and t_NNNNNNN.bin
@@ -144,7 +144,13 @@ int main(int argc, char **argv) {
   if (datain.empty() || dataout.empty() || tmax <= 0) {
     std::fprintf(stderr, "usage: dglm_main --datain DIR --dataout DIR --physics euler|advection "
                          "--tmax T [--cfl C] [--gamma G] [--tau-scale S] [--device D] "
-                         "[--matrix-order f|c] [--precision fp64|tf32x3|bf16x3]\n");
+                         "[--matrix-order f|c] [--precision fp64|tf32x3|bf16x3|bf16x6]\n");
+    return 2;
+  }
+  if (precision != "fp64" && precision != "tf32x3" && precision != "bf16x3" &&
+      precision != "bf16x6") {
+    std::fprintf(stderr, "dglm_main: unknown precision %s (fp64, tf32x3, bf16x3, bf16x6)\n",
+                 precision.c_str());
     return 2;
   }
   if (!restart_dir.empty() && restart_step < 0) {
@@ -234,8 +240,10 @@ int main(int argc, char **argv) {
   d.N = N;
   d.physics = euler ? DGLM_EULER : DGLM_ADVECTION;
   d.K = (int)K;
-  d.precision = precision == "tf32x3" ? DGLM_PREC_TF32X3
-                : precision == "bf16x3" ? DGLM_PREC_BF16X3 : DGLM_PREC_FP64;
+  d.precision = precision == "tf32x3"   ? DGLM_PREC_TF32X3
+                : precision == "bf16x3" ? DGLM_PREC_BF16X3
+                : precision == "bf16x6" ? DGLM_PREC_BF16X6
+                                        : DGLM_PREC_FP64;
   d.cfl = cfl;
   d.gamma = gamma;
   d.tau_scale = tau_scale;

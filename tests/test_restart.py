@@ -24,6 +24,15 @@ def test_driver_rejects_restart_dir_without_step(tmp_path):
     assert r.returncode == 2 and "--restart-step" in r.stderr
 
 
+def test_driver_rejects_unknown_precision(tmp_path):
+    if not os.path.exists(_build.MAIN):
+        pytest.skip("dglm_main not built")
+    r = subprocess.run([_build.MAIN, "--datain", str(tmp_path), "--dataout", str(tmp_path),
+                        "--tmax", "1", "--precision", "fp16"],
+                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+    assert r.returncode == 2 and "unknown precision fp16" in r.stderr
+
+
 def test_driver_rejects_mismatched_snapshots(tmp_path):
     """A field file of the wrong size or a time file of another step stops
     dglm_main before it touches the GPU."""
