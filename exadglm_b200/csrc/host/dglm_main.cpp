@@ -147,6 +147,14 @@ int main(int argc, char **argv) {
                          "[--matrix-order f|c] [--precision fp64|tf32x3|bf16x3|bf16x6]\n");
     return 2;
   }
+  if (physics != "euler" && physics != "advection") {
+    std::fprintf(stderr, "dglm_main: unknown physics %s (euler, advection)\n", physics.c_str());
+    return 2;
+  }
+  if (order != "c" && order != "f") {
+    std::fprintf(stderr, "dglm_main: unknown matrix order %s (c, f)\n", order.c_str());
+    return 2;
+  }
   if (precision != "fp64" && precision != "tf32x3" && precision != "bf16x3" &&
       precision != "bf16x6") {
     std::fprintf(stderr, "dglm_main: unknown precision %s (fp64, tf32x3, bf16x3, bf16x6)\n",

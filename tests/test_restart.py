@@ -24,13 +24,17 @@ def test_driver_rejects_restart_dir_without_step(tmp_path):
     assert r.returncode == 2 and "--restart-step" in r.stderr
 
 
-def test_driver_rejects_unknown_precision(tmp_path):
+@pytest.mark.parametrize("flag,value,msg", [("--precision", "fp16", "unknown precision fp16"),
+                                            ("--physics", "maxwell", "unknown physics maxwell"),
+                                            ("--matrix-order", "x", "unknown matrix order x")])
+def test_driver_rejects_unknown_values(tmp_path, flag, value, msg):
+    """Flags with a fixed set of values fail instead of falling back."""
     if not os.path.exists(_build.MAIN):
         pytest.skip("dglm_main not built")
     r = subprocess.run([_build.MAIN, "--datain", str(tmp_path), "--dataout", str(tmp_path),
-                        "--tmax", "1", "--precision", "fp16"],
+                        "--tmax", "1", flag, value],
                        stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
-    assert r.returncode == 2 and "unknown precision fp16" in r.stderr
+    assert r.returncode == 2 and msg in r.stderr, r.stderr
 
 
 def test_driver_rejects_mismatched_snapshots(tmp_path):
