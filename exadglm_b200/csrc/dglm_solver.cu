@@ -341,6 +341,9 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
     return set_error(DGLM_ERR_UNSUPPORTED,
                      "dglm_create: order N=" + std::to_string(d.N) + " is not built (1..8)");
   if (d.K <= 0) return set_error(DGLM_ERR_INVALID, "dglm_create: K must be positive");
+  // node indices (vmapP, the reference's int32 format) must fit in int32
+  if ((long long)d.K * np_of(d.N) > 2147483647LL)
+    return set_error(DGLM_ERR_UNSUPPORTED, "dglm_create: K*Np exceeds the int32 node index range");
   if (d.precision != DGLM_PREC_FP64 && d.precision != DGLM_PREC_TF32X3 &&
       d.precision != DGLM_PREC_BF16X3 && d.precision != DGLM_PREC_BF16X6)
     return set_error(DGLM_ERR_INVALID, "dglm_create: unknown precision");

@@ -67,7 +67,8 @@ def _desc(**kw):
     ({"N": 0}, capi.ERR_UNSUPPORTED), ({"N": 9}, capi.ERR_UNSUPPORTED),
     ({"physics": 7}, capi.ERR_INVALID), ({"K": 0}, capi.ERR_INVALID),
     ({"cfl": -1.0}, capi.ERR_INVALID), ({"gamma": 1.0}, capi.ERR_INVALID),
-    ({"tmax": 0.0}, capi.ERR_INVALID),
+    ({"tmax": 0.0}, capi.ERR_INVALID), ({"precision": 9}, capi.ERR_INVALID),
+    ({"K": 2 ** 31 // 35 + 1}, capi.ERR_UNSUPPORTED),    # K*Np past the int32 node range
 ])
 def test_create_rejects_bad_descriptions(kw, status):
     L = capi.lib()
