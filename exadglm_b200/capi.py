@@ -27,7 +27,7 @@ EXPORTS = (
     "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
-    "dglm_set_variant", "dglm_get_variant", "dglm_adjoint_record", "dglm_adjoint_backward",
+    "dglm_set_variant", "dglm_get_variant", "dglm_set_wait_limit", "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
     "dglm_calc_maxv_dt_static", "dglm_adjoint_variant_count", "dglm_adjoint_variant_describe",
     "dglm_adjoint_set_variant", "dglm_batch_create", "dglm_batch_add", "dglm_batch_finalize",
@@ -95,6 +95,7 @@ def lib():
         L.dglm_variant_describe.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
         L.dglm_set_variant.argtypes = [_P, C.c_int]
         L.dglm_get_variant.argtypes = [_P]
+        L.dglm_set_wait_limit.argtypes = [_P, C.c_longlong]
         L.dglm_kernel_launches.argtypes = [_P]
         L.dglm_kernel_launches.restype = C.c_long
         L.dglm_device_bytes.argtypes = [_P]
@@ -153,6 +154,9 @@ def variant_precision(desc):
     for prec in ("tf32x3", "bf16x3", "bf16x6"):
         if desc.startswith(("tcgen05-" + prec, "mma16-" + prec, "pipe-mma16-" + prec)):
             return prec
+    # split TF32 with all four part products (the tensor-memory operator kernel)
+    if desc.startswith("tc-tmem-tf32"):
+        return "tf32x3"
     return "fp64"
 
 
@@ -392,6 +396,11 @@ class Solver:
 
     def variant(self):
         return int(self.L.dglm_get_variant(self.h))
+
+    def set_wait_limit(self, cycles):
+        """Bound (SM clock cycles) of the hand-off waits of the pipelined
+        stage kernels; 0 restores the default (about one second)."""
+        check(self.L.dglm_set_wait_limit(self.h, int(cycles)))
 
     def kernel_launches(self):
         return int(self.L.dglm_kernel_launches(self.h))

@@ -12,6 +12,9 @@ namespace dglm {
 
 constexpr int kMaxOrder = 8;
 constexpr int kHistory = 65536;          // dt history ring (steps)
+// bound of each wait of the pipelined stage kernels, in SM clock cycles
+// (~1 s at the B200 clock); on expiry a CTA sets flag bit 4 and leaves
+constexpr long long kWaitCycles = 2000000000LL;
 
 __host__ __device__ constexpr int np_of(int N) { return (N + 1) * (N + 2) * (N + 3) / 6; }
 __host__ __device__ constexpr int nfp_of(int N) { return (N + 1) * (N + 2) / 2; }
@@ -55,6 +58,9 @@ struct StageArgs {
   int last_stage;        // 1: also compute maxv of the new state (Euler)
   int rhs_only;          // 1: write the right-hand side to u_out, no LSERK update
   double dt_override;    // >= 0: use this dt instead of sc->dt
+  long long wait_cycles; // bound of the hand-off waits between the warps of the
+                         // pipelined kernels (kWaitCycles unless a test shortens it);
+                         // waits for copies or MMAs already in flight keep kWaitCycles
 };
 
 // Reference Euler flux (F, G, W) of the state q, in the arithmetic order of
@@ -96,12 +102,43 @@ __device__ __forceinline__ unsigned long long warp_max_bits(unsigned long long b
   return b;
 }
 
+// calc_maxv of face fi of element e (euler_nopad_dglm.cu:7-76,
+// advec_nopad_dglm.cu:7-62): the largest |v| over the face nodes plus, for
+// Euler, the largest sound speed, with the reference's divisions by rho.
+// U is any struct with a member array p[5] of per-variable field pointers.
+// Shared by the per-kernel entry point and the no-allocation variant, whose
+// results must agree bit for bit.
+template <class U>
+__device__ __forceinline__ double face_max_speed(int physics, int Np, int Nfp, double gamma,
+                                                 const int *__restrict__ Fmask, const U &u,
+                                                 const double *vx, const double *vy,
+                                                 const double *vz, long e, int fi) {
+  double mv2 = 0, mc2 = 0;
+  for (int j = 0; j < Nfp; j++) {
+    const long n = e * Np + Fmask[fi * Nfp + j];
+    if (physics == DGLM_EULER) {
+      const double u1 = u.p[0][n], u2 = u.p[1][n], u3 = u.p[2][n], u4 = u.p[3][n],
+                   u5 = u.p[4][n];
+      const double ax = u2 / u1, ay = u3 / u1, az = u4 / u1;
+      const double v2 = ax * ax + ay * ay + az * az;
+      if (v2 > mv2) mv2 = v2;
+      const double pres = (gamma - 1) * (u5 - 0.5 * u1 * v2);
+      const double c2 = fabs(gamma * pres / u1);
+      if (c2 > mc2) mc2 = c2;
+    } else {
+      const double v2 = vx[n] * vx[n] + vy[n] * vy[n] + vz[n] * vz[n];
+      if (v2 > mv2) mv2 = v2;
+    }
+  }
+  return physics == DGLM_EULER ? sqrt(mv2) + sqrt(mc2) : sqrt(mv2);
+}
+
 // error plumbing (dglm_solver.cu)
 dglm_status set_error(dglm_status s, const std::string &msg);
 dglm_status cuda_check(cudaError_t e, const char *what);
 
 // contraction engines of the fused stage kernel
-enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3, MODE_MMA16 = 4 };
+enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3, MODE_MMA16 = 4, MODE_TC = 5 };
 
 // One compiled tile shape of the fused stage kernel.
 struct StageVariantInfo {
@@ -116,9 +153,9 @@ struct StageVariantInfo {
   int threads;
   size_t smem;
   int prec;      // dglm_precision of the contraction (0 FP64, 1 TF32x3, 2 BF16x3)
-  int npad;      // MIXED: MMA N (output nodes, padded)
-  int kva, kfa;  // MIXED: volume / lift K extents of the operand images
-  int bimg;      // MIXED: bytes of the operator image (hi then lo)
+  int npad;      // MIXED: MMA N (output nodes, padded); TC: output nodes per lane quarter
+  int kva, kfa;  // MIXED, TC: volume / lift K extents of the operand images
+  int bimg;      // MIXED: bytes of the operator image (hi then lo); TC: tensor-memory image
   int groups;    // PIPE: consumer groups taking alternate tiles (1 or 2)
   int kstep;     // MMA16: K per mma.sync (8 TF32, 16 BF16)
   int persistent;  // 1: one CTA per SM walking the tiles (TMA-fed pipeline)

@@ -40,6 +40,7 @@ struct dglm_handle {
   long launches = 0;
   size_t bytes = 0;
   std::vector<void *> allocs;
+  long long wait_cycles = 0;     // > 0: shortened hand-off wait bound (dglm_set_wait_limit)
   AdjointTape *tape = nullptr;   // discrete adjoint (dglm_adjoint.cu)
   int adj_variant = 0;           // adjoint tile shape
   // dglm_run_ensemble: double-buffered device copies of the members' input

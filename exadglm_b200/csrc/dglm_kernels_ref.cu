@@ -45,26 +45,8 @@ __global__ void calc_maxv_k(int physics, int Np, int Nfp, long nfaces, double ga
                             double *maxv, double *maxv_fs) {
   const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (f >= nfaces) return;
-  const long e = f / 4;
-  const int fi = (int)(f % 4);
-  double mv2 = 0, mc2 = 0;
-  for (int j = 0; j < Nfp; j++) {
-    const long n = e * Np + Fmask[fi * Nfp + j];
-    if (physics == DGLM_EULER) {
-      const double u1 = u.p[0][n], u2 = u.p[1][n], u3 = u.p[2][n], u4 = u.p[3][n],
-                   u5 = u.p[4][n];
-      const double ax = u2 / u1, ay = u3 / u1, az = u4 / u1;
-      const double v2 = ax * ax + ay * ay + az * az;
-      if (v2 > mv2) mv2 = v2;
-      const double pres = (gamma - 1) * (u5 - 0.5 * u1 * v2);
-      const double c2 = fabs(gamma * pres / u1);
-      if (c2 > mc2) mc2 = c2;
-    } else {
-      const double v2 = vx[n] * vx[n] + vy[n] * vy[n] + vz[n] * vz[n];
-      if (v2 > mv2) mv2 = v2;
-    }
-  }
-  const double mv = physics == DGLM_EULER ? sqrt(mv2) + sqrt(mc2) : sqrt(mv2);
+  const double mv = face_max_speed(physics, Np, Nfp, gamma, Fmask, u, vx, vy, vz, f / 4,
+                                   (int)(f % 4));
   maxv[f] = mv;
   maxv_fs[f] = mv * Fscale[f];
 }

@@ -14,9 +14,13 @@
 // on one device (different streams or host threads) share the scratch and
 // race; callers serialise them.
 //
-// The device address of the scratch is looked up once per device, with that
-// device current, by the first call on it (cudaGetSymbolAddress, which may
-// load the module); make that first call before any stream capture.
+// The device address of the scratch is looked up once per device context,
+// with that device current, by the first call in it (cudaGetSymbolAddress,
+// which may load the module); make that first call before any stream
+// capture.  The lookup is keyed on the context's unique id, so after a
+// cudaDeviceReset (a new primary context, the module loaded anew) the next
+// call looks the address up again instead of using the old one.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -38,6 +42,7 @@ static __device__ __align__(256) unsigned long long g_maxv_partials[kStaticParti
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 unsigned long long *g_partials_ptr[kMaxDevices] = {};
+unsigned long long g_partials_ctx[kMaxDevices] = {};   // context id the address belongs to
 
 struct U5 {
   const double *p[5];
@@ -55,26 +60,8 @@ __global__ void __launch_bounds__(kFacesPerBlock)
   const long f = blockIdx.x * (long)kFacesPerBlock + threadIdx.x;
   unsigned long long b = 0ull;
   if (f < nfaces) {
-    const long e = f / 4;
-    const int fi = (int)(f % 4);
-    double mv2 = 0, mc2 = 0;
-    for (int j = 0; j < Nfp; j++) {
-      const long n = e * Np + Fmask[fi * Nfp + j];
-      if (physics == DGLM_EULER) {
-        const double u1 = u.p[0][n], u2 = u.p[1][n], u3 = u.p[2][n], u4 = u.p[3][n],
-                     u5 = u.p[4][n];
-        const double ax = u2 / u1, ay = u3 / u1, az = u4 / u1;
-        const double v2 = ax * ax + ay * ay + az * az;
-        if (v2 > mv2) mv2 = v2;
-        const double pres = (gamma - 1) * (u5 - 0.5 * u1 * v2);
-        const double c2 = fabs(gamma * pres / u1);
-        if (c2 > mc2) mc2 = c2;
-      } else {
-        const double v2 = vx[n] * vx[n] + vy[n] * vy[n] + vz[n] * vz[n];
-        if (v2 > mv2) mv2 = v2;
-      }
-    }
-    const double mv = physics == DGLM_EULER ? sqrt(mv2) + sqrt(mc2) : sqrt(mv2);
+    const double mv = face_max_speed(physics, Np, Nfp, gamma, Fmask, u, vx, vy, vz, f / 4,
+                                     (int)(f % 4));
     maxv[f] = mv;
     b = dbits(mv * Fscale[f]);
   }
@@ -111,7 +98,31 @@ __global__ void __launch_bounds__(1024)
   }
 }
 
-// Device address of the scratch on the current device (looked up once).
+// Unique id of the current context (driver entry points looked up through
+// the runtime, so the library needs no link against libcuda).
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// false when the queries are unavailable or no context is current yet
+bool current_context_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1{}, q2{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+        !f1 || !f2)
+      return false;
+    get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    get_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  CUcontext ctx = nullptr;
+  return get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of the scratch in the current context (looked up once per
+// device context).
 dglm_status partials_address(unsigned long long **out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -119,12 +130,18 @@ dglm_status partials_address(unsigned long long **out) {
   if (dev < 0 || dev >= kMaxDevices)
     return set_error(DGLM_ERR_UNSUPPORTED, "dglm_calc_maxv_dt_static: device index above 63");
   std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_partials_ptr[dev]) {
+  unsigned long long ctx = 0;
+  const bool have = current_context_id(&ctx);
+  if (!have || !g_partials_ptr[dev] || g_partials_ctx[dev] != ctx) {
+    // also makes the device's primary context current if none was yet
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_maxv_partials);
     if (e != cudaSuccess)
       return cuda_check(e, "dglm_calc_maxv_dt_static: cudaGetSymbolAddress of the scratch");
+    if (!current_context_id(&ctx))
+      return set_error(DGLM_ERR_CUDA, "dglm_calc_maxv_dt_static: no current CUDA context");
     g_partials_ptr[dev] = static_cast<unsigned long long *>(p);
+    g_partials_ctx[dev] = ctx;
   }
   *out = g_partials_ptr[dev];
   return DGLM_OK;

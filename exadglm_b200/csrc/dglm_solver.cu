@@ -80,6 +80,7 @@ StageArgs dglm::stage_args(dglm_handle *h, const double *u_in, double *u_out, in
   a.last_stage = (s == 4);
   a.rhs_only = 0;
   a.dt_override = -1.0;
+  a.wait_cycles = h->wait_cycles > 0 ? h->wait_cycles : kWaitCycles;
   return a;
 }
 
@@ -88,7 +89,7 @@ namespace {
 // Doubles of the device operator copy for a variant's layout.
 size_t op_doubles(const StageVariantInfo &v, int Np, int NFF) {
   if (v.mode == MODE_SIMT) return (size_t)(3 * Np + NFF) * v.IP;
-  if (v.mode == MODE_MIXED) return ((size_t)v.bimg + 7) / 8;
+  if (v.mode == MODE_MIXED || v.mode == MODE_TC) return ((size_t)v.bimg + 7) / 8;
   if (v.mode == MODE_MMA16) {
     const int parts = v.prec == DGLM_PREC_BF16X6 ? 3 : 2;
     return (size_t)(v.KVP / v.kstep + v.KFP / v.kstep) * v.MT * parts * 64;   // 512 B each
@@ -227,9 +228,49 @@ std::vector<uint32_t> m16_fragments(const dglm_handle *h, const StageVariantInfo
   return out;
 }
 
+// Tensor-memory operator image of the split-TF32 kernel (stage_tc_kernel):
+// 128 lanes x KT columns of TF32 bit patterns.  Lane 32q + 2j + p holds part
+// p (0: hi, 1: lo) of operator row i = npq q + j; column k is the kernel's K
+// order: volume k = (i'/4)*12 + d*4 + i'%4 for direction d and node i', face
+// k = kva + f*nfpp + j' (nfpp = kfa / 4).  Padding columns and unused lanes
+// are zero.  hi = TF32 rounding of x, lo = TF32 rounding of the exact FP64
+// residual.
+std::vector<uint32_t> tc_image(const dglm_handle *h, const StageVariantInfo &v) {
+  const int Np = h->Np, Nfp = h->Nfp, KA = 3 * Np + h->NFF;
+  const int KT = v.kva + v.kfa, npq = v.npad, nfpp = v.kfa / 4, ng = (Np + 3) / 4;
+  std::vector<uint32_t> img((size_t)128 * KT, 0u);
+  for (int k = 0; k < KT; k++) {
+    int col = -1;
+    if (k < v.kva) {
+      const int g = k / 12, d = (k % 12) / 4, i = g * 4 + k % 4;
+      if (g < ng && i < Np) col = d * Np + i;
+    } else {
+      const int f = (k - v.kva) / nfpp, j = (k - v.kva) % nfpp;
+      if (j < Nfp) col = 3 * Np + f * Nfp + j;
+    }
+    if (col < 0) continue;
+    for (int q = 0; q < 4; q++)
+      for (int j = 0; j < npq; j++) {
+        const int i = npq * q + j;
+        if (i >= Np) continue;
+        const double x = h->Ahost[(size_t)i * KA + col];
+        const uint32_t hi = tf32_rna((float)x);
+        const uint32_t lo = tf32_rna((float)(x - (double)f32_of(hi)));
+        img[(size_t)(32 * q + 2 * j) * KT + k] = hi;
+        img[(size_t)(32 * q + 2 * j + 1) * KT + k] = lo;
+      }
+  }
+  return img;
+}
+
 dglm_status upload_operator_layout(dglm_handle *h) {
   const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
   const StageVariantInfo &v = h->vinfo;
+  if (v.mode == MODE_TC) {
+    std::vector<uint32_t> img = tc_image(h, v);
+    return cuda_check(cudaMemcpy(h->AT, img.data(), img.size() * 4, cudaMemcpyHostToDevice),
+                      "operator upload");
+  }
   if (v.mode == MODE_MMA16) {
     std::vector<uint32_t> fr = m16_fragments(h, v);
     return cuda_check(cudaMemcpy(h->AT, fr.data(), fr.size() * 4, cudaMemcpyHostToDevice),
@@ -341,9 +382,18 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
     return set_error(DGLM_ERR_UNSUPPORTED,
                      "dglm_create: order N=" + std::to_string(d.N) + " is not built (1..8)");
   if (d.K <= 0) return set_error(DGLM_ERR_INVALID, "dglm_create: K must be positive");
-  // node indices (vmapP, the reference's int32 format) must fit in int32
-  if ((long long)d.K * np_of(d.N) > 2147483647LL)
-    return set_error(DGLM_ERR_UNSUPPORTED, "dglm_create: K*Np exceeds the int32 node index range");
+  // node indices (vmapP, the reference's int32 format) must fit in int32, and
+  // so must the face-point indices K*4*Nfp of the adjoint's partner map (4*Nfp
+  // > Np at every order); checked on K rounded up to whole 64-element tiles
+  {
+    const long long kp = ((long long)d.K + 63) / 64 * 64;
+    if (kp * np_of(d.N) > 2147483647LL)
+      return set_error(DGLM_ERR_UNSUPPORTED,
+                       "dglm_create: K*Np exceeds the int32 node index range");
+    if (kp * 4 * nfp_of(d.N) > 2147483647LL)
+      return set_error(DGLM_ERR_UNSUPPORTED,
+                       "dglm_create: K*4*Nfp exceeds the int32 face-point index range");
+  }
   if (d.precision != DGLM_PREC_FP64 && d.precision != DGLM_PREC_TF32X3 &&
       d.precision != DGLM_PREC_BF16X3 && d.precision != DGLM_PREC_BF16X6)
     return set_error(DGLM_ERR_INVALID, "dglm_create: unknown precision");
@@ -390,7 +440,8 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   chk(dalloc(h, &h->nrm, (size_t)12 * K));
   chk(dalloc(h, &h->tau, (size_t)4 * K));
   chk(dalloc(h, &h->maxv, (size_t)4 * K));
-  chk(dalloc(h, &h->vmapP, (size_t)d.K * h->NFF));
+  // padded to whole tiles: the tensor-core kernel bulk-copies vmapP per tile
+  chk(dalloc(h, &h->vmapP, (size_t)K * h->NFF));
   chk(dalloc(h, &h->vmapF, (size_t)4 * K));
   chk(dalloc(h, &h->Fmask, (size_t)h->NFF));
   if (d.physics == DGLM_ADVECTION) chk(dalloc(h, &h->vel, (size_t)3 * h->vs));
@@ -414,6 +465,7 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   for (void *p : {(void *)h->u[0], (void *)h->u[1], (void *)h->kreg})
     cudaMemset(p, 0, sizeof(double) * h->nvar * h->vs);
   cudaMemset(h->geo, 0, sizeof(double) * 9 * K);
+  cudaMemset(h->vmapP, 0, sizeof(int) * K * h->NFF);
   cudaMemset(h->nrm, 0, sizeof(double) * 12 * K);
   for (double *p : {h->fscale, h->tau, h->maxv}) cudaMemset(p, 0, sizeof(double) * 4 * K);
   if (h->vel) cudaMemset(h->vel, 0, sizeof(double) * 3 * h->vs);
@@ -899,6 +951,9 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
              v.prec == DGLM_PREC_TF32X3 ? "tf32x3" : v.prec == DGLM_PREC_BF16X6 ? "bf16x6"
                                                                                 : "bf16x3",
              v.E, v.CPT, v.WM, v.threads, v.smem);
+  else if (v.mode == MODE_TC)
+    snprintf(buf, len, "tc-tmem-tf32x4 E=%d threads=%d smem=%zu ring=%d", v.E, v.threads,
+             v.smem, v.ring);
   else if (v.mode == MODE_MIXED) {
     const int n = snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
                            v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"
@@ -951,6 +1006,16 @@ dglm_status dglm_set_variant(dglm_handle *h, int variant) {
 }
 
 int dglm_get_variant(dglm_handle *h) { return h ? h->variant : -1; }
+
+dglm_status dglm_set_wait_limit(dglm_handle *h, long long cycles) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_set_wait_limit: NULL handle");
+  if (cycles < 0) return set_error(DGLM_ERR_INVALID, "dglm_set_wait_limit: negative bound");
+  DeviceGuard g(h->dev);
+  cudaStreamSynchronize(h->stream);
+  drop_graphs(h);   // the captured steps carry the bound in their arguments
+  h->wait_cycles = cycles;
+  return DGLM_OK;
+}
 
 long dglm_kernel_launches(dglm_handle *h) { return h ? h->launches : 0; }
 size_t dglm_device_bytes(dglm_handle *h) { return h ? h->bytes : 0; }

@@ -610,6 +610,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 
 #include "dglm_stage_pipe.cuh"
 #include "dglm_stage_mixed.cuh"
+#include "dglm_stage_tc.cuh"
 
 // Standalone calc_maxv (initial state, advection velocity): maxv per face and
 // a device-wide max of maxv*Fscale into sc->acc[slot].
@@ -815,6 +816,37 @@ static Variant make_mixed() {
   return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC, PW>};
 }
 
+template <int PHYS, int N, int E, int NW, int NB>
+static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
+  using C = TCfg<PHYS, N, E, NW, NB>;
+  auto k = stage_tc_kernel<PHYS, N, E, NW, NB>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int ntiles = (a.K + E - 1) / E;
+  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  k<<<grid, C::THREADS, C::SMEM, s>>>(a, ntiles);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E, int NW, int NB>
+static Variant make_tc() {
+  using C = TCfg<PHYS, N, E, NW, NB>;
+  StageVariantInfo i{};
+  i.mode = MODE_TC;
+  i.E = E;
+  i.threads = C::THREADS;
+  i.smem = C::SMEM;
+  i.prec = DGLM_PREC_TF32X3;
+  i.npad = C::NPQ;
+  i.kva = C::KVA;
+  i.kfa = C::KFA;
+  i.bimg = 128 * C::KT * 4;
+  i.ring = NB;
+  i.persistent = 1;
+  return Variant{i, &launch_tc<PHYS, N, E, NW, NB>};
+}
+
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
 static Variant make_v() {
   using C = Cfg<PHYS, N, MODE, E, R, CPT, WM, PR>;
@@ -880,6 +912,8 @@ static const std::vector<Variant> &variants();
 #define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
 // tcgen05 variants with PW producer warps
 #define V_MXP(P, NN, E, PREC, W, PW) make_mixed<P, NN, E, PREC, W, PW>()
+// split-TF32 with the operator in tensor memory: E elements, NW compute warps, NB ring slots
+#define V_TC(P, NN, E, NW, NB) make_tc<P, NN, E, NW, NB>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -891,7 +925,8 @@ DGLM_VARIANTS(EUL, 1, V_SIMT(EUL, 1, 128, 4, 5), V_DMMA(EUL, 1, 64, 4, 1))
 DGLM_VARIANTS(EUL, 2, V_SIMT(EUL, 2, 64, 5, 5), V_DMMA(EUL, 2, 32, 4, 2))
 DGLM_VARIANTS(EUL, 3, V_DMMA(EUL, 3, 16, 2, 3), V_SIMT(EUL, 3, 32, 5, 5),
               V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true),
-              V_PIPEF(EUL, 3, 8, 1, true, 3, 2), V_PIPEF(EUL, 3, 16, 2, true, 3, 2))
+              V_PIPEF(EUL, 3, 8, 1, true, 3, 2), V_PIPEF(EUL, 3, 16, 2, true, 3, 2),
+              V_TC(EUL, 3, 16, 16, 3))
 DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_SIMT(EUL, 4, 16, 5, 5), V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
@@ -904,7 +939,8 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PM16(EUL, 4, 8, 1, 3, 1), V_PIPER(EUL, 4, 8, 1, 2, true, 2, 2),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
-              V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2))
+              V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2),
+              V_TC(EUL, 4, 16, 16, 3), V_TC(EUL, 4, 16, 8, 3))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),

@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
 
   if (warp >= C::NWC) {
     pipe_producer<C, PHYS>(a, ntiles, sBimg, sBuf0, full, empty, abar, C::BIMG, warp - C::NWC,
-                           lane);
+                           lane, kWaitCycles);
     return;
   }
 
@@ -299,6 +299,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
   unsigned long long vmax = 0ull;
   bool ok = consumer_all(mbar_wait(abar, 0), TC);
   int it = 0, mma_phase = 0;
+  bool mma_pending = false;   // a commit issued whose phase has not been observed
 
   // MMAs of one operand block (volume: k-steps [0, KSV), lift: [KSV, KST)),
   // issued by lane 0 of warps 0..NISS-1; MMA g of the tile (product q of
@@ -372,6 +373,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
     tc_fence_before();
     consumer_sync(TC);
     issue(aV, C::SBO_AV, opV, C::SBO_BV, 0, C::KSV);
+    mma_pending = true;
     if (!C::SEPL) {
       // the volume MMAs must have read the shared operand before it is reused
       if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
@@ -379,6 +381,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
         break;
       }
       mma_phase ^= 1;
+      mma_pending = false;
       tc_fence_after();
     }
 
@@ -424,15 +427,18 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
         break;
       }
       mma_phase ^= 1;
+      mma_pending = false;
       tc_fence_after();
     }
     issue(aF, C::SBO_AF, opF, C::SBO_BF, C::KSV, C::KSF);
+    mma_pending = true;
     // a commit arrives once all earlier MMAs of its thread are done
     if (!consumer_all(mbar_wait(mbar, mma_phase), TC)) {
       ok = false;
       break;
     }
     mma_phase ^= 1;
+    mma_pending = false;
     tc_fence_after();
 
     // 5. accumulator -> sR as [v][i][EP] (row m lives in TMEM lane
@@ -539,6 +545,8 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
     if (lane == 0) mbar_arrive(&empty[b]);
   }
   if (!ok && tid == 0) atomicOr(&a.sc->flags, 4);
+  // MMAs still in flight finish before the tensor memory is released
+  if (!ok && mma_pending) mbar_wait(mbar, mma_phase);
   if (PHYS == EUL && a.last_stage && !a.rhs_only) {
     vmax = warp_max_bits(vmax);
     if (lane == 0) sMax[warp] = vmax;

@@ -21,8 +21,6 @@
 // This header is included inside namespace dglm.
 #pragma once
 
-constexpr long long kWaitCycles = 2000000000LL;   // ~1 s at the B200 clock
-
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
@@ -50,11 +48,12 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned pa
   return ok != 0;
 }
 // bounded wait for the completion of the phase with the given parity
-__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity,
+                                          long long limit = kWaitCycles) {
   if (mbar_try_wait(b, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(b, parity))
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
 }
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes,
@@ -209,12 +208,14 @@ struct PCfg {
 // advection velocity), issued by producer warp 0, and cp.async gathers of the
 // neighbour traces, split over the C::PW producer warps.  full[b] completes
 // once the bulk bytes have landed and all 32 * PW lanes' gathers are done.
+// `limit` bounds the waits for a free buffer; the final waits for the
+// producer's own copies keep kWaitCycles.
 template <class C, int PHYS>
 __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, void *op_smem,
                                               double *sBuf0, unsigned long long *full,
                                               unsigned long long *empty,
                                               unsigned long long *abar, unsigned op_bytes,
-                                              int pw, int lane) {
+                                              int pw, int lane, long long limit) {
   constexpr int NV = C::NV, Np = C::Np, NFF = C::NFF, E = C::E, NB = C::NB;
   const long vs = a.vs, gs = a.gstride;
   const bool lead = pw == 0 && lane == 0;
@@ -226,7 +227,7 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
   bool ok = true;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
     const int b = it % NB;
-    if (it >= NB && !mbar_wait(&empty[b], ((it / NB) - 1) & 1)) {
+    if (it >= NB && !mbar_wait(&empty[b], ((it / NB) - 1) & 1, limit)) {
       ok = false;
       break;
     }
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(
   // ------------------------------------------------------------- producer
   if (twarp >= C::NG * C::NWC) {
     pipe_producer<C, PHYS>(a, ntiles, sAF, sBuf0, full, empty, abar, 8u * C::S_AF,
-                           twarp - C::NG * C::NWC, lane);
+                           twarp - C::NG * C::NWC, lane, a.wait_cycles);
     return;
   }
 
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(
   const double dt = a.dt_override >= 0 ? a.dt_override : a.sc->dt;
   unsigned long long vmax = 0ull;
   bool ok = true;
-  if (ASMEM) ok = consumer_all(mbar_wait(abar, 0), TC);
+  if (ASMEM) ok = consumer_all(mbar_wait(abar, 0, a.wait_cycles), TC);
   const double *Afrag = ASMEM ? sAF : a.AT;
   // DMMA warp roles: m-group, n-block and k-chunk.  With WN = NT a warp
   // feeds each operator fragment it loads to all n-tiles of the tile (the
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(
   int it = grp;
   for (int t = blockIdx.x + grp * gridDim.x; ok && t < ntiles; t += C::NG * gridDim.x, it += C::NG) {
     const int b = it % C::NB;
-    if (!consumer_all(mbar_wait(&full[b], (it / C::NB) & 1), TC)) {
+    if (!consumer_all(mbar_wait(&full[b], (it / C::NB) & 1, a.wait_cycles), TC)) {
       ok = false;
       break;
     }

@@ -220,7 +220,13 @@ int main(int argc, char **argv) {
                    time_name(restart_step).c_str(), tstep0, t0, restart_step);
       return 1;
     }
-    print_tstep = (int)std::llround(tt[2]);   // keeps the original run's interval
+    // the original run's print interval: a non-negative whole number of steps
+    if (!(tt[2] >= 0) || tt[2] != std::floor(tt[2]) || tt[2] > 2147483647.0) {
+      std::fprintf(stderr, "dglm_main: %s holds print interval %g, not a step count >= 0\n",
+                   time_name(restart_step).c_str(), tt[2]);
+      return 1;
+    }
+    print_tstep = (int)tt[2];   // keeps the original run's interval
   } else if (!read_bin(datain + "u0.bin", u0, nvar * n, false)) {
     u0.assign(nvar * n, 0.0);
     for (size_t i = 0; i < n; i++) {

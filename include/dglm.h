@@ -168,6 +168,16 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
 /* Selects the variant used by the handle (rebuilds the operator layout). */
 dglm_status dglm_set_variant(dglm_handle *h, int variant);
 int dglm_get_variant(dglm_handle *h);
+/* Bound, in SM clock cycles, of each hand-off wait between the warps of the
+ * pipelined stage kernels (a tile's copies landing, a buffer or an MMA
+ * result becoming free); 0 restores the default (2e9, about one second).
+ * When a wait runs out, the CTA sets an error flag, waits (with the default
+ * bound) for its own copies and MMAs in flight and leaves; dglm_sync and
+ * dglm_rhs then return DGLM_ERR_CUDA and the handle's state is invalid until
+ * the next dglm_set_state.  A short bound makes waits expire on purpose:
+ * this is how the expiry path is tested.  No counterpart in the reference,
+ * whose kernels have no waits between warps. */
+dglm_status dglm_set_wait_limit(dglm_handle *h, long long cycles);
 /* Number of kernels the last dglm_step call launched (for accounting). */
 long dglm_kernel_launches(dglm_handle *h);
 /* Device bytes held by the handle. */

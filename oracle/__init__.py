@@ -215,9 +215,33 @@ def rk_coefficients():
 # the reference itself (oracle/_ref)
 # ---------------------------------------------------------------------------
 
-def ref_lib_path(physics, N):
+def host_has_avx512():
+    """True when this host's CPU runs x86-64-v4 code (AVX-512 F/BW/CD/DQ/VL)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    return {"avx512f", "avx512bw", "avx512cd", "avx512dq",
+                            "avx512vl"} <= flags
+    except OSError:
+        pass
+    return False
+
+
+def ref_march(physics, N):
+    """The -march of the reference build that ref_lib_path loads here."""
     tag = "euler" if physics == "euler" else "advec"
-    return os.path.join(REF_DIR, f"libref_{tag}_N{N}.so")
+    v4 = os.path.join(REF_DIR, f"libref_{tag}_N{N}_v4.so")
+    return "x86-64-v4" if host_has_avx512() and os.path.exists(v4) else "x86-64-v3"
+
+
+def ref_lib_path(physics, N):
+    """The reference CPU solver built for this host: the AVX-512 build where
+    the CPU has it (the launcher compiles with -march=native), else AVX2."""
+    tag = "euler" if physics == "euler" else "advec"
+    suffix = "_v4" if ref_march(physics, N) == "x86-64-v4" else ""
+    return os.path.join(REF_DIR, f"libref_{tag}_N{N}{suffix}.so")
 
 
 def ref_available(physics, N):

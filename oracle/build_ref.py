@@ -1,14 +1,17 @@
 """Build recipe for ``oracle/_ref/``: the reference's own code, compiled from
-its sources where they lie under /root/reference (nothing is copied).
+its sources where they lie in the reference tree (nothing is copied).
 
 Products (all git-ignored, they travel with the working tree):
 
 * ``_ref/libref_{euler,advec}_N{n}.so`` -- the reference CPU single-partition
   solver (dim3/src/cpp/{euler,advec}_{data,dglm,time}.cpp, plus
   utils/src/cpp/io.cpp), compiled the way its launcher does
-  (dglm_3d_launcher.py:392: ``g++ -O3 -std=c++11 -fopenmp``; ``-march`` is
-  pinned to x86-64-v3 instead of ``native`` so the library also runs on the
-  host of another machine), with the generated ``common.h`` written here.
+  (dglm_3d_launcher.py:392: ``g++ -O3 -std=c++11 -fopenmp -march=native``),
+  with the generated ``common.h`` written here.  ``native`` would tie the
+  library to this machine's CPU, so two builds are made instead: one for
+  ``-march=x86-64-v3`` (AVX2) and one for ``-march=x86-64-v4`` (AVX-512,
+  suffix ``_v4``); oracle.ref_lib_path loads the v4 build on hosts whose
+  CPU has AVX-512 -- the closest portable stand-in for ``native``.
   ``ref_driver.cpp`` wraps its ``runRK`` in a fixed-step C entry point.
   ``CFL``, ``GAMMA``, ``TAU_SCALE`` and ``TMAX`` become run-time globals so
   one build serves every configuration of an order N; ``N``, ``NP``, ``NFP``,
@@ -30,8 +33,13 @@ import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("DGLM_REFERENCE_ROOT", "/root/reference")
-CXXFLAGS = ["-O3", "-std=c++11", "-fopenmp", "-march=x86-64-v3", "-shared", "-fPIC"]
+# the reference tree: $DGLM_REFERENCE_ROOT, else a "reference" directory
+# beside the repository
+REF = os.environ.get("DGLM_REFERENCE_ROOT",
+                     os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+CXXFLAGS = ["-O3", "-std=c++11", "-fopenmp", "-shared", "-fPIC"]
+# -march of each build and the suffix of its file
+ISAS = (("x86-64-v3", ""), ("x86-64-v4", "_v4"))
 
 COMMON_H = """#ifndef COMMON_H
 #define COMMON_H
@@ -78,15 +86,17 @@ def build_solver(phys: str, N: int, force=False) -> str:
     nvar = 5 if phys == "euler" else 1
     bdir = os.path.join(OUT, f"build_{phys}_N{N}")
     os.makedirs(bdir, exist_ok=True)
-    so = os.path.join(OUT, f"libref_{phys}_N{N}.so")
     drv = os.path.join(HERE, "ref_driver.cpp")
-    if not force and os.path.exists(so) and os.path.getmtime(so) > os.path.getmtime(drv):
-        return so
     with open(os.path.join(bdir, "common.h"), "w") as f:
         f.write(COMMON_H.format(N=N, NP=Np, NFP=Nfp, NVAR=nvar, REF=REF, P=phys))
     flag = "-DREF_EULER" if phys == "euler" else "-DREF_ADVEC"
-    _run(["g++", *CXXFLAGS, flag, "-I", bdir, drv, "-o", so])
-    return so
+    out = None
+    for march, suffix in ISAS:
+        so = os.path.join(OUT, f"libref_{phys}_N{N}{suffix}.so")
+        if force or not os.path.exists(so) or os.path.getmtime(so) <= os.path.getmtime(drv):
+            _run(["g++", *CXXFLAGS, f"-march={march}", flag, "-I", bdir, drv, "-o", so])
+        out = out or so
+    return out
 
 
 def build_mesh_cores() -> None:

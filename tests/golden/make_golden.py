@@ -27,7 +27,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("DGLM_REFERENCE_ROOT", "/root/reference")
+# the reference tree: $DGLM_REFERENCE_ROOT, else a "reference" directory
+# beside the repository
+REF = os.environ.get("DGLM_REFERENCE_ROOT",
+                     os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
+                         os.path.dirname(os.path.abspath(__file__))))), "reference"))
 sys.path.insert(0, ROOT)
 
 

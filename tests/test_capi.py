@@ -41,7 +41,7 @@ def test_variants_are_described():
             v = capi.variants(phys, N)
             assert len(v) >= 2
             assert all(d.startswith(("simt", "dmma", "pipe-dmma", "pipe2-dmma", "tcgen05-",
-                                      "mma16-", "pipe-mma16-")) for d in v)
+                                      "mma16-", "pipe-mma16-", "tc-tmem-")) for d in v)
             assert capi.variants(phys, N, "fp64")
 
 
@@ -69,6 +69,8 @@ def _desc(**kw):
     ({"cfl": -1.0}, capi.ERR_INVALID), ({"gamma": 1.0}, capi.ERR_INVALID),
     ({"tmax": 0.0}, capi.ERR_INVALID), ({"precision": 9}, capi.ERR_INVALID),
     ({"K": 2 ** 31 // 35 + 1}, capi.ERR_UNSUPPORTED),    # K*Np past the int32 node range
+    # K*4*Nfp (face points, N=1: 12 per element) past the int32 range while K*Np is not
+    ({"N": 1, "K": 2 ** 31 // 12 + 1}, capi.ERR_UNSUPPORTED),
 ])
 def test_create_rejects_bad_descriptions(kw, status):
     L = capi.lib()

@@ -61,6 +61,10 @@ def test_driver_rejects_mismatched_snapshots(tmp_path):
     np.array([0.1, 6.0, 2.0]).tofile(os.path.join(snap, time_name(5)))
     r = run()
     assert r.returncode != 0 and "holds step 6" in r.stderr, r.stderr
+    for bad in (-3.0, 2.5, np.nan):     # print interval: negative, fractional, NaN
+        np.array([0.1, 5.0, bad]).tofile(os.path.join(snap, time_name(5)))
+        r = run()
+        assert r.returncode != 0 and "print interval" in r.stderr, (bad, r.stderr)
 
 
 @pytest.mark.gpu

@@ -2,10 +2,14 @@
 allocation) against the existing pair dglm_calc_maxv + dglm_calc_dt on the
 same device fields, through the C ABI, on two calls in a row.
 
-Both compute maxv with the same arithmetic and dt from the same max (a max is
-independent of reduction order), so maxv and dt must agree exactly; the
-tolerance is 0.  The size limit is rejected on the host before any device
-call, so that check runs without a GPU."""
+Both compute maxv with the same arithmetic (one shared device function) and
+dt from the same max (a max is independent of reduction order), so maxv and
+dt must agree exactly; the tolerance is 0.  The calls after the first must
+not change the device's free memory (nothing is allocated), and a call on a
+second stream, ordered after the first, gives the same result (the scratch
+is shared by every call; serialised calls do not interfere).  The size limit
+is rejected on the host before any device call, so that check runs without a
+GPU."""
 import ctypes as C
 
 import numpy as np
@@ -65,15 +69,30 @@ def test_matches_calc_maxv_plus_calc_dt_twice(phys, N, n):
                               C.c_void_p(dt_ref.data_ptr()), None))
     torch.cuda.synchronize()
 
-    for call in range(2):
-        maxv = torch.full((4 * K,), -1.0, dtype=torch.float64, device=dev)
-        dt = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
+    maxv = torch.empty(4 * K, dtype=torch.float64, device=dev)
+    dt = torch.empty(1, dtype=torch.float64, device=dev)
+    side = torch.cuda.Stream()
+
+    def call_static(stream):
+        maxv.fill_(-1.0)
+        dt.fill_(-1.0)
+        torch.cuda.synchronize()
         capi.check(L.dglm_calc_maxv_dt_static(ph, N, K, gamma, cfl,
                                               C.c_void_p(Fmask.data_ptr()),
                                               C.c_void_p(Fscale.data_ptr()), u_tab, *vel,
                                               C.c_void_p(maxv.data_ptr()),
-                                              C.c_void_p(dt.data_ptr()), None))
+                                              C.c_void_p(dt.data_ptr()),
+                                              None if stream is None else
+                                              C.c_void_p(stream.cuda_stream)))
         torch.cuda.synchronize()
+
+    free_before = None
+    for call in range(3):
+        call_static(side if call == 2 else None)
+        if call == 0:
+            free_before = torch.cuda.mem_get_info()[0]
         assert torch.equal(maxv, maxv_ref), (phys, N, call)
         assert float(dt.item()) == float(dt_ref.item()), (call, dt.item(), dt_ref.item())
         assert float(dt.item()) > 0
+    # the calls after the first allocated nothing on the device
+    assert torch.cuda.mem_get_info()[0] == free_before
