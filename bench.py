@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint", "batch", "precision"],
+    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint", "batch", "precision",
+                                       "gpu_baseline"],
                     default=None,
                     help="run one section alone (profiling); prints that section's object")
     ap.add_argument("--accuracy-steps", type=int, default=200,
@@ -96,16 +97,27 @@ def flops_per_element_stage(nvar, Np, Nfp):
     return nvar * (6 * Np * Np + 2 * Np * 4 * Nfp)
 
 
-def read_traffic(kernel_tag):
-    """Per-launch DRAM bytes of the stage kernel from the committed ncu
-    summary (profiles/stage_traffic.txt: '<tag> <bytes_per_launch>')."""
+def variant_shape(desc):
+    """A variant description without its smem=<bytes> field (the shared-memory
+    size moves with layout changes that leave the tile shape alone)."""
+    return " ".join(w for w in desc.split() if not w.startswith("smem="))
+
+
+def read_traffic(desc, K):
+    """Per-launch DRAM bytes of the stage kernel variant `desc` on a K-element
+    mesh, from the committed ncu summary (profiles/stage_traffic.txt: lines
+    '<K> <bytes_per_launch> <variant shape>'); None when no capture of that
+    variant at that size is recorded."""
     path = os.path.join(ROOT, "profiles", "stage_traffic.txt")
     if not os.path.exists(path):
         return None
+    want = variant_shape(desc)
     with open(path) as f:
         for line in f:
-            parts = line.split()
-            if len(parts) >= 2 and parts[0] == kernel_tag and not line.startswith("#"):
+            if line.startswith("#") or not line.strip():
+                continue
+            parts = line.split(None, 2)
+            if len(parts) == 3 and parts[0] == str(K) and parts[2].strip() == want:
                 try:
                     return float(parts[1])
                 except ValueError:
@@ -244,7 +256,9 @@ def run_reference_arm(a):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(a, p, a.gpus),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{a.steps} full LSERK steps of the K={p.K} mesh"},
+                         "sample": f"{a.steps} full LSERK steps of the K={p.K} mesh",
+                         "compile": "g++ -O3 -std=c++11 -fopenmp -march="
+                                    + oracle.ref_march(p.physics, p.N)},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if have_ref:
@@ -308,6 +322,7 @@ def mixed_section(a, p, stream, fp64_ms_per_step):
         e1.synchronize()
         s.sync()
         ms = e0.elapsed_time(e1) / a.steps
+        stage_ms = stage_alone_ms(s, stream)
         s.set_state(p.u0)
         s.step(S)
         s.sync()
@@ -322,9 +337,63 @@ def mixed_section(a, p, stream, fp64_ms_per_step):
             "rel_l2_vs_fp64": float(np.linalg.norm(um - u64) / np.linalg.norm(u64)),
             "rel_l2_per_field": per_field,
             "kernel": variants("euler", p.N)[s.variant()],
+            "roofline": hbm_roofline(p, stage_ms, variants("euler", p.N)[s.variant()]),
         }
         s.close()
     return out
+
+
+def stage_alone_ms(s, stream, reps=25):
+    """Mean time of one stage-kernel launch (CUDA events on the solver's
+    stream, after warm-up launches), for the roofline."""
+    import torch
+    _, dt, _ = s.time()
+    for i in range(5):
+        s.stage(i % 5, dt)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream.synchronize()
+    e0.record(stream)
+    for i in range(reps):
+        s.stage(i % 5, dt)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def hbm_roofline(p, stage_ms, desc):
+    """Achieved algorithmic HBM bandwidth of one stage launch against the
+    measured copy peak (the bound of the mixed-precision path)."""
+    peaks, kind = load_peaks()
+    B = bytes_per_element_stage(p.nvar, p.Np, p.Nfp) * p.K
+    g = B / (stage_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": g, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": g / peaks["hbm_gbs"], "launch_ms": stage_ms,
+            "algorithmic_bytes_per_launch": B, "traffic": read_traffic(desc, p.K),
+            "peak_source": f"{kind} hbm_gbs"}
+
+
+def gpu_baseline_section(a, p, rank):
+    """The reference's own GPU path (its CUDA kernels and cuBLAS batched
+    DGEMMs, compiled for sm_100a from its sources into oracle/_ref) on the
+    same workload and GPU: steps timed with the host clock around its runRK
+    loop, which synchronises every step (calc_dt's blocking copy)."""
+    import oracle
+    if not oracle.gpu_ref_available(p.N):
+        return {"unavailable": "oracle/_ref holds no reference GPU build"}
+    ref = oracle.RefGpuSolver(p)
+    ref.run(a.warmup)
+    ref.set_state(p.u0)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    t0 = time.perf_counter()
+    done = ref.run(a.steps)
+    el = time.perf_counter() - t0
+    clk = clocks.stop()
+    ref.close()
+    return {"value": dof_stages_per_step(p) * done / el, "unit": UNIT,
+            "ms_per_step": 1e3 * el / done, "steps": done, "clocks": clk,
+            "what": "reference euler_nopad_*.cu (CUDA kernels + cuBLAS DgemmBatched), "
+                    "nvcc -O3 -arch sm_100a, same mesh and state, one process"}
 
 
 def adjoint_section(a, stream):
@@ -518,10 +587,11 @@ def main():
 
     p = build_problem(a)
     stream = torch.cuda.Stream()
-    if a.only in ("mixed", "adjoint", "batch", "precision"):
+    if a.only in ("mixed", "adjoint", "batch", "precision", "gpu_baseline"):
         res = (mixed_section(a, p, stream, None) if a.only == "mixed"
                else adjoint_section(a, stream) if a.only == "adjoint"
                else precision_section(a, stream) if a.only == "precision"
+               else gpu_baseline_section(a, p, rank) if a.only == "gpu_baseline"
                else batch_section(a, stream))
         if rank == 0:
             print(json.dumps({a.only: res}), flush=True)
@@ -553,29 +623,17 @@ def main():
     value = replica_rate(world, per_step, a.steps, ms_max)
 
     # ---- stage kernel alone, for the roofline -----------------------------
-    t, dt, _ = s.time()
-    reps = 25
-    for i in range(5):
-        s.stage(i % 5, dt)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stream.synchronize()
-    e0.record(stream)
-    for i in range(reps):
-        s.stage(i % 5, dt)
-    e1.record(stream)
-    e1.synchronize()
-    stage_ms = e0.elapsed_time(e1) / reps
+    stage_ms = stage_alone_ms(s, stream)
     peaks, peak_kind = load_peaks()
     B = bytes_per_element_stage(p.nvar, p.Np, p.Nfp) * p.K
     F = flops_per_element_stage(p.nvar, p.Np, p.Nfp) * p.K
     achieved_gbs = B / (stage_ms * 1e-3) / 1e9
     achieved_tf = F / (stage_ms * 1e-3) / 1e12
-    tag = f"euler_N{p.N}_K{p.K}_{a.precision}"
     vdesc = variants("euler", p.N)[s.variant()]
     roof = {
         "kernel": vdesc,
         "bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-        "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": read_traffic(tag),
+        "frac": achieved_gbs / peaks["hbm_gbs"], "traffic": read_traffic(vdesc, p.K),
         "peak_source": f"{peak_kind} hbm_gbs (burst, kernel timed alone)",
         "algorithmic_bytes_per_launch": B, "launch_ms": stage_ms,
         "binding_roof": "fp64",
@@ -640,12 +698,22 @@ def main():
     if a.only is None and a.precision == "fp64":
         line["mixed"] = mixed_section(a, p, stream, ms_max / a.steps)
         line["adjoint"] = adjoint_section(a, stream)
+        if rank == 0:
+            gb = gpu_baseline_section(a, p, rank)
+            if "value" in gb:
+                gb["ours_over_reference_gpu"] = value / world / gb["value"]
+            line["gpu_baseline"] = gb
+        line["precision"] = precision_section(a, stream)
+        line["batch"] = batch_section(a, stream)
     if rank == 0 and not a.no_cpu_baseline:
         sample_steps = 1
         rate, kind, cores, secs = cpu_reference_rate(p, sample_steps)
+        import oracle
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                                 "sample": f"{sample_steps} LSERK step of the K={p.K} mesh "
-                                          f"({secs:.1f} s)"}
+                                          f"({secs:.1f} s)",
+                                "compile": "g++ -O3 -std=c++11 -fopenmp -march="
+                                           + oracle.ref_march(p.physics, p.N)}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -952,8 +952,8 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
                                                                                 : "bf16x3",
              v.E, v.CPT, v.WM, v.threads, v.smem);
   else if (v.mode == MODE_TC)
-    snprintf(buf, len, "tc-tmem-tf32x4 E=%d threads=%d smem=%zu ring=%d", v.E, v.threads,
-             v.smem, v.ring);
+    snprintf(buf, len, "tc-tmem-tf32x4 E=%d flux=%d threads=%d smem=%zu ring=%d", v.E,
+             v.producers, v.threads, v.smem, v.ring);
   else if (v.mode == MODE_MIXED) {
     const int n = snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
                            v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"

@@ -816,10 +816,10 @@ static Variant make_mixed() {
   return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC, PW>};
 }
 
-template <int PHYS, int N, int E, int NW, int NB>
+template <int PHYS, int N, int E, int NF, int NB>
 static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
-  using C = TCfg<PHYS, N, E, NW, NB>;
-  auto k = stage_tc_kernel<PHYS, N, E, NW, NB>;
+  using C = TCfg<PHYS, N, E, NF, NB>;
+  auto k = stage_tc_kernel<PHYS, N, E, NF, NB>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -829,9 +829,9 @@ static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int NW, int NB>
+template <int PHYS, int N, int E, int NF, int NB>
 static Variant make_tc() {
-  using C = TCfg<PHYS, N, E, NW, NB>;
+  using C = TCfg<PHYS, N, E, NF, NB>;
   StageVariantInfo i{};
   i.mode = MODE_TC;
   i.E = E;
@@ -843,8 +843,9 @@ static Variant make_tc() {
   i.kfa = C::KFA;
   i.bimg = 128 * C::KT * 4;
   i.ring = NB;
+  i.producers = NF;   // flux warps
   i.persistent = 1;
-  return Variant{i, &launch_tc<PHYS, N, E, NW, NB>};
+  return Variant{i, &launch_tc<PHYS, N, E, NF, NB>};
 }
 
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
@@ -912,8 +913,8 @@ static const std::vector<Variant> &variants();
 #define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
 // tcgen05 variants with PW producer warps
 #define V_MXP(P, NN, E, PREC, W, PW) make_mixed<P, NN, E, PREC, W, PW>()
-// split-TF32 with the operator in tensor memory: E elements, NW compute warps, NB ring slots
-#define V_TC(P, NN, E, NW, NB) make_tc<P, NN, E, NW, NB>()
+// split-TF32 with the operator in tensor memory: E elements, NF flux warps, NB ring slots
+#define V_TC(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -926,7 +927,7 @@ DGLM_VARIANTS(EUL, 2, V_SIMT(EUL, 2, 64, 5, 5), V_DMMA(EUL, 2, 32, 4, 2))
 DGLM_VARIANTS(EUL, 3, V_DMMA(EUL, 3, 16, 2, 3), V_SIMT(EUL, 3, 32, 5, 5),
               V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true),
               V_PIPEF(EUL, 3, 8, 1, true, 3, 2), V_PIPEF(EUL, 3, 16, 2, true, 3, 2),
-              V_TC(EUL, 3, 16, 16, 3))
+              V_TC(EUL, 3, 8, 10, 3))
 DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_SIMT(EUL, 4, 16, 5, 5), V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
@@ -940,7 +941,7 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
               V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2),
-              V_TC(EUL, 4, 16, 16, 3), V_TC(EUL, 4, 16, 8, 3))
+              V_TC(EUL, 4, 8, 10, 3))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),

@@ -47,9 +47,30 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *b, unsigned pa
       : "memory");
   return ok != 0;
 }
-// bounded wait for the completion of the phase with the given parity
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the completion of the phase with the given parity.  With
+// the default bound the thread suspends in try_wait between checks; a
+// shortened bound (dglm_set_wait_limit) polls with the non-blocking
+// test_wait, so that the bound and not try_wait's own suspension time decides
+// when the wait gives up
 __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity,
                                           long long limit = kWaitCycles) {
+  if (limit < kWaitCycles) {
+    const long long t0 = clock64();
+    while (!mbar_test_wait(b, parity))
+      if (clock64() - t0 > limit) return false;
+    return true;
+  }
   if (mbar_try_wait(b, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(b, parity))

@@ -317,3 +317,76 @@ class RefSolver:
         if self._tmp is not None:
             self._tmp.cleanup()
             self._tmp = None
+
+
+# ---------------------------------------------------------------------------
+# the reference GPU path (oracle/_ref/libref_gpu_euler_N4.so): the second
+# baseline, the reference's own CUDA kernels and cuBLAS DGEMMs
+# ---------------------------------------------------------------------------
+
+def gpu_ref_lib_path(N=4):
+    return os.path.join(REF_DIR, f"libref_gpu_euler_N{N}.so")
+
+
+def gpu_ref_available(N=4):
+    return os.path.exists(gpu_ref_lib_path(N))
+
+
+class RefGpuSolver:
+    """The reference Euler GPU solver (euler_nopad_*.cu with cuBLAS),
+    compiled from its sources for one configuration (CFL, gamma and tau scale
+    are compile-time constants there: build_ref.build_gpu_solver), driven
+    through oracle/ref_gpu_driver.cu on the current CUDA device.  The datain
+    files are written in the GPU ('f') matrix order.  One live instance per
+    process (the shared object holds one global solver)."""
+
+    def __init__(self, problem, datain_dir=None):
+        from exadglm_b200.datain import write_datain
+        if problem.physics != "euler":
+            raise ValueError("the reference GPU build is the Euler path")
+        self.p = problem
+        path = gpu_ref_lib_path(problem.N)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} (run oracle/build_ref.py where the reference lives)")
+        L = C.CDLL(path)
+        L.ref_gpu_open.restype = C.c_int
+        L.ref_gpu_open.argtypes = [C.c_char_p]
+        for f in ("ref_gpu_cfl", "ref_gpu_gamma", "ref_gpu_tau_scale", "ref_gpu_time",
+                  "ref_gpu_last_dt"):
+            getattr(L, f).restype = C.c_double
+        built = (L.ref_gpu_cfl(), L.ref_gpu_gamma(), L.ref_gpu_tau_scale())
+        if built != (problem.cfl, problem.gamma, problem.tau_scale):
+            raise ValueError(f"reference GPU build is for (CFL, gamma, tau) = {built}")
+        self.L = L
+        self._tmp = None
+        if datain_dir is None:
+            self._tmp = tempfile.TemporaryDirectory(prefix="dglm_refgpu_")
+            datain_dir = self._tmp.name
+            write_datain(datain_dir, problem.datain_arrays(), matrix_order="f")
+        K = L.ref_gpu_open(datain_dir.encode())
+        assert K == problem.K, (K, problem.K)
+        self.set_state(problem.u0)
+
+    def set_state(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert self.L.ref_gpu_set_state(_ptr(u)) == 0
+
+    def get_state(self):
+        u = np.zeros((self.p.nvar, self.p.K * self.p.Np))
+        assert self.L.ref_gpu_get_state(_ptr(u)) == 0
+        return u
+
+    def run(self, nsteps):
+        done = self.L.ref_gpu_run(int(nsteps))
+        if done < 0:
+            raise RuntimeError("reference GPU path: CUDA error")
+        return done
+
+    def time(self):
+        return self.L.ref_gpu_time(), self.L.ref_gpu_last_dt(), self.L.ref_gpu_tstep()
+
+    def close(self):
+        self.L.ref_gpu_close()
+        if self._tmp is not None:
+            self._tmp.cleanup()
+            self._tmp = None
