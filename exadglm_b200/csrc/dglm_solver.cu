@@ -952,7 +952,7 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
                                                                                 : "bf16x3",
              v.E, v.CPT, v.WM, v.threads, v.smem);
   else if (v.mode == MODE_TC)
-    snprintf(buf, len, "tc-tmem-tf32x4 E=%d flux=%d threads=%d smem=%zu ring=%d", v.E,
+    snprintf(buf, len, "tc-tmem-tf32x4 E=%d compute=%d threads=%d smem=%zu ring=%d", v.E,
              v.producers, v.threads, v.smem, v.ring);
   else if (v.mode == MODE_MIXED) {
     const int n = snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",

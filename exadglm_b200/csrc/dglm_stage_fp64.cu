@@ -843,7 +843,7 @@ static Variant make_tc() {
   i.kfa = C::KFA;
   i.bimg = 128 * C::KT * 4;
   i.ring = NB;
-  i.producers = NF;   // flux warps
+  i.producers = NF;   // compute warps
   i.persistent = 1;
   return Variant{i, &launch_tc<PHYS, N, E, NF, NB>};
 }
@@ -913,7 +913,7 @@ static const std::vector<Variant> &variants();
 #define V_BF16W(P, NN, E, W) make_mixed<P, NN, E, PREC_BF16, W>()
 // tcgen05 variants with PW producer warps
 #define V_MXP(P, NN, E, PREC, W, PW) make_mixed<P, NN, E, PREC, W, PW>()
-// split-TF32 with the operator in tensor memory: E elements, NF flux warps, NB ring slots
+// split-TF32 with the operator in tensor memory: E elements, NF compute warps, NB ring slots
 #define V_TC(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
@@ -927,7 +927,7 @@ DGLM_VARIANTS(EUL, 2, V_SIMT(EUL, 2, 64, 5, 5), V_DMMA(EUL, 2, 32, 4, 2))
 DGLM_VARIANTS(EUL, 3, V_DMMA(EUL, 3, 16, 2, 3), V_SIMT(EUL, 3, 32, 5, 5),
               V_PIPE(EUL, 3, 8, 1, 3, true), V_PIPE(EUL, 3, 16, 1, 3, true),
               V_PIPEF(EUL, 3, 8, 1, true, 3, 2), V_PIPEF(EUL, 3, 16, 2, true, 3, 2),
-              V_TC(EUL, 3, 8, 10, 3))
+              V_TC(EUL, 3, 8, 14, 3))
 DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_SIMT(EUL, 4, 16, 5, 5), V_SIMT(EUL, 4, 16, 3, 5), V_DMMA(EUL, 4, 16, 1, 5),
               V_DMMA(EUL, 4, 16, 2, 5), V_PIPE(EUL, 4, 8, 1, 5, true),
@@ -941,7 +941,7 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
               V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2),
-              V_TC(EUL, 4, 8, 10, 3))
+              V_TC(EUL, 4, 8, 14, 3))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),

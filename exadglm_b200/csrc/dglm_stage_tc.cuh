@@ -9,12 +9,13 @@
 //       CTA): lane 32q + 2j + p holds part p (0: TF32 hi, 1: TF32 lo) of
 //       operator row i = NPQ q + j, so both parts of an output node sit in
 //       neighbouring lanes of one warp's lane quarter;
-//   B = the tile's fluxes in shared memory, one row per (variable, element),
-//       n = v E + e (rows NV E .. MN-1 stay zero), split x = hi + lo into
-//       two K-major images;
-//   D = FP32 accumulators in tensor memory, double-buffered across tiles.
-// Per k-step two MMAs (B hi, B lo) accumulate into the same D, so D holds
-// (A_hi + A_lo)(B_hi + B_lo): all four part products.
+//   B = the tile's fluxes in shared memory, split x = hi + lo; row
+//       n = p NCOL + v E + e holds part p of (variable v, element e), so one
+//       MMA per k-step multiplies both parts (rows past 2 NCOL stay zero);
+//   D = FP32 accumulators in tensor memory, double-buffered across tiles:
+//       column n of lane (i, p') holds A_p' . B_p of column n mod NCOL.
+// The right-hand side of (v, e) at node i is the sum of the four part
+// products D[(i,0)][c] + D[(i,0)][NCOL + c] + D[(i,1)][c] + D[(i,1)][NCOL + c].
 //
 // Centring.  Before the split every flux value of an element has that
 // element's flux at node 0 subtracted: fluxR/S/T - metric . F(u_0) and
@@ -27,52 +28,45 @@
 // representation and FP32 accumulation errors.
 //
 // K order.  Volume columns are node-group major, k = (i/4)*12 + d*4 + i%4
-// (d = r, s, t), so a thread that computes nodes i, i+1 stores 8 contiguous
-// bytes per (variable, direction); face columns follow at KVA + f NFPP + j.
+// (d = r, s, t); face columns follow at KVA + f NFPP + j.  A warp task covers
+// 8 elements x 4 consecutive nodes, so each store of the task fills one
+// 8-row x 16-byte core matrix.
 //
-// Warp roles (NF + 6 warps), handing off through mbarriers only:
-//   volume warps         one warp task each (8 elements x 4 node pairs) per
-//   0..VOL_WT-1          tile: volume fluxes -> arrive vol_done, after MMA
-//                        volume of the previous tile has read the images
-//                        (bar_v);
-//   face warps           the face tasks (8 elements x 4 nodes of one face)
-//   VOL_WT..NF-1         round-robin -> arrive face_done, after MMA face of
-//                        the previous tile (bar_f); the last one first
-//                        computes the node-0 fluxes of the next tile;
-//   producer warp NF     per tile, into a ring of NB buffers: bulk copies of
-//                        u, the RK register k, metrics and face data (one
-//                        copy per lane), cp.async gathers of the neighbour
-//                        traces u[vmapP]; full[b] completes when all landed.
-//   MMA warp NF+1        lane 0 issues the volume MMAs of tile t once
-//                        vol_done(t) and the accumulator D[t%2] is free
-//                        (d_free), then the face MMAs once face_done(t), and
-//                        commits to bar_v, bar_f and dfull[t%2].
-//   epilogue warps       one per tensor-memory lane quarter: wait dfull[t%2],
-//   NF+2..NF+5           add the operator parts of each node, LSERK update
-//                        from the staged u and k, coalesced-by-node stores;
-//                        arrive d_free[t%2] and empty[t%NB].
-// The tensor cores work on tile t while the flux warps start t+1 and the
-// epilogue warps finish t-1; nothing on the critical path reads global
-// memory.  Every wait is bounded; on expiry a warp sets flag bit 2, waits
-// (with the default bound) for the MMAs and copies it issued, and leaves.
+// Warps: NC compute warps, one producer warp, one MMA warp.
+//   producer    per tile, into a ring of NB buffers: bulk copies of u, the RK
+//               register k, metrics and face data (one copy per lane),
+//               cp.async gathers of the neighbour traces u[vmapP]; before
+//               each refill, the node-0 fluxes of the previous tile.
+//   MMA         lane 0: once the compute warps have written the operand
+//               images of tile t (flux_done) and the accumulator D[t%2] is
+//               free (d_free), the volume and face MMAs, committed to
+//               mma_done.
+//   compute     per tile t: volume and face flux tasks of t, after MMA(t-1)
+//               has read the images; then the
+//               epilogue of t-1: warps 0..3 read D[(t-1)%2] (one lane quarter
+//               each), add the parts into the rhs staging, and all compute
+//               warps do the LSERK update from the staged u and k with
+//               coalesced stores.
+// The tensor cores work on tile t while the compute warps finish t-1.
+// Every wait is bounded; on expiry a warp sets flag bit 2, waits (with the
+// default bound) for the MMAs and copies it issued, and leaves.
 #pragma once
 
-template <int PHYS, int N, int E_, int NF_, int NB_>
+template <int PHYS, int N, int E_, int NC_, int NB_>
 struct TCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
-  static constexpr int E = E_, NF = NF_, NB = NB_;
-  static constexpr int NCOL = NV * E;                    // used MMA columns
-  static constexpr int MN = (NCOL + 15) / 16 * 16;       // MMA N (multiple of 16 for M = 128)
+  static constexpr int E = E_, NC = NC_, NB = NB_;
+  static constexpr int NCOL = NV * E;                    // (variable, element) columns
+  static constexpr int MN = (2 * NCOL + 15) / 16 * 16;   // MMA N: both parts, padded to 16
   static constexpr int NPQ = (Np + 3) / 4;               // output nodes per lane quarter
   static constexpr int NG = (Np + 3) / 4;                // volume node groups of 4
-  static constexpr int NPAIR = 2 * NG;                   // volume node pairs
   static constexpr int KV = 12 * NG, KVA = (KV + 7) / 8 * 8;
   static constexpr int NFPP = (Nfp + 3) / 4 * 4;
   static constexpr int KFA = 4 * NFPP;
   static constexpr int KT = KVA + KFA, KSV = KVA / 8, KSF = KFA / 8;
   static constexpr int SBO_V = KVA / 4 * 128, SBO_F = KFA / 4 * 128;
-  static constexpr int BV_PART = MN / 8 * SBO_V, BF_PART = MN / 8 * SBO_F;
+  static constexpr int BV_BYTES = MN / 8 * SBO_V, BF_BYTES = MN / 8 * SBO_F;
   // tensor memory: D0, D1, then the operator
   static constexpr int D_COLS = MN, A_COL = 2 * MN;
   static constexpr int TMEM_COLS = 512;
@@ -85,28 +79,28 @@ struct TCfg {
   static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE);
   static constexpr int NCOPY = 2 * NV + 9 + 5;           // bulk copies per tile
   // node-0 flux terms per element: 3 volume directions + 4 faces, per
-  // variable; three slots (written for tile t+1 while tile t-1's face tasks
-  // may still read theirs)
+  // variable; three slots (the producer writes tile t+1's, or t+2's, while
+  // the compute warps read tile t's)
   static constexpr int NCEN = 7, NCS = 3;
   static constexpr int S_C = E * NV * NCEN;
-  // warp tasks: volume 8 elements x 4 node pairs (one volume warp each),
-  // face 8 elements x 4 nodes of one face (shared by the NFW face warps)
-  static constexpr int NEB = E / 8, NHB = (NPAIR + 3) / 4, NJB = NFPP / 4;
-  static constexpr int VOL_WT = NEB * NHB, FACE_WT = NEB * 4 * NJB;
-  static constexpr int NVW = VOL_WT, NFW = NF - VOL_WT;
-  static constexpr int PROD_WARP = NF, MMA_WARP = NF + 1, EPI_WARP = NF + 2, NWARPS = NF + 6;
-  static constexpr int THREADS = 32 * NWARPS;
-  // gathers per producer lane: E * NFF face points
-  static constexpr int GPL = (E * NFF + 31) / 32;
-  // epilogue: each lane of a node's pair takes half of the used columns
-  static constexpr int HALF = (NCOL + 1) / 2;
-  static constexpr size_t OFF_BV = 0, OFF_BF = 2 * (size_t)BV_PART;
-  static constexpr size_t OFF_RING = OFF_BF + 2 * (size_t)BF_PART;
+  // rhs staging [v][e][i] for the update
+  static constexpr int S_R = NV * E * Np;
+  // warp tasks per tile: volume (8 elements x one node group of 4), face
+  // (8 elements x 4 nodes of one face)
+  static constexpr int NEB = E / 8, NJB = NFPP / 4;
+  static constexpr int VOL_WT = NEB * NG, FACE_WT = NEB * 4 * NJB;
+  static constexpr int NTASK = VOL_WT + FACE_WT;
+  static constexpr int PROD_WARP = NC, MMA_WARP = NC + 1, NWARPS = NC + 2;
+  static constexpr int THREADS = 32 * NWARPS, TC = 32 * NC;
+  static constexpr int GPL = (E * NFF + 31) / 32;        // gathers per producer lane
+  static constexpr size_t OFF_BV = 0, OFF_BF = BV_BYTES;
+  static constexpr size_t OFF_RING = OFF_BF + (size_t)BF_BYTES;
   static constexpr size_t OFF_C = OFF_RING + 8 * (size_t)NB * S_BUF;
-  static constexpr size_t OFF_BAR = OFF_C + 8 * NCS * (size_t)S_C;
-  // barriers: full[NB], empty[NB], cen[NCS], vol_done, face_done, bar_v,
-  // bar_f, dfull[2], d_free[2]; then the tensor-memory address, Fmask, maxima
-  static constexpr int NBARS = 2 * NB + NCS + 8;
+  static constexpr size_t OFF_R = OFF_C + 8 * NCS * (size_t)S_C;
+  static constexpr size_t OFF_BAR = OFF_R + 8 * (size_t)S_R;
+  // barriers: full[NB], empty[NB], cen[NCS], flux_done, mma_done, d_free[2];
+  // then the tensor-memory address, Fmask, maxima
+  static constexpr int NBARS = 2 * NB + NCS + 4;
   static constexpr size_t SMEM = OFF_BAR + 8 * (NBARS + 1) + 4 * NFF + 8 * 32 + 64;
   // instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N, M = 128
   static constexpr unsigned IDESC =
@@ -115,14 +109,13 @@ struct TCfg {
   static_assert(E % 8 == 0 && MN <= 256, "MMA N for M = 128");
   static_assert(2 * NPQ <= 32, "both operator parts of a quarter's nodes fit its 32 lanes");
   static_assert(2 * D_COLS + KT <= TMEM_COLS, "accumulators and operator fit tensor memory");
-  static_assert(NF >= 4, "flux warps 0..3 load the operator into the four lane quarters");
-  static_assert(NFW >= 1, "at least one face warp");
+  static_assert(NC >= 4, "compute warps 0..3 cover the four tensor-memory lane quarters");
   static_assert(E <= 32, "one lane per element computes the node-0 fluxes");
   static_assert(NCOPY <= 32, "one producer lane per bulk copy");
-  static_assert(HALF <= 32, "an epilogue lane holds its columns in registers");
-  // NB >= 3: the producer refills a slot when the epilogue releases it; the
-  // node-0 fluxes of tile t+1 (computed during tile t) must not wait for
-  // the epilogue of tile t-1
+  static_assert(NCOL <= 64 && NCOL % 2 == 0,
+                "an epilogue lane holds both parts of its row's columns, split in halves");
+  // NB >= 3: the node-0 fluxes of tile t+1 are computed during tile t, while
+  // the slot of tile t-1 may still be held by its epilogue
   static_assert(NB >= 3 && NB <= 4, "ring of 3..4 tile buffers");
   static_assert((E * Np * 8) % 16 == 0, "16-byte bulk copies");
   static_assert(THREADS <= 1024 && NWARPS <= 32, "block size");
@@ -148,6 +141,15 @@ __device__ __forceinline__ void tmem_st8(unsigned taddr, const unsigned (&r)[8])
 __device__ __forceinline__ void tmem_st_wait() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_ld4(unsigned taddr, float *r) {
+  unsigned v[4];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr)
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < 4; i++) r[i] = __uint_as_float(v[i]);
+}
 // x = hi + lo as TF32 bit patterns (FP32 containers) of the FP32 value of x:
 // hi keeps the top 11 significant bits of FP32(x) (truncated), lo the exact
 // FP32 remainder, of which the MMA reads the top 11 bits
@@ -156,24 +158,23 @@ __device__ __forceinline__ void split_tf32_pair(double x, unsigned &hi, unsigned
   hi = __float_as_uint(f) & 0xffffe000u;
   lo = __float_as_uint(f - __uint_as_float(hi));
 }
-// named barrier 3 over the four epilogue warps
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 3, 128;" ::: "memory"); }
 
-template <int PHYS, int N, int E_, int NF_, int NB_>
-__global__ void __launch_bounds__(TCfg<PHYS, N, E_, NF_, NB_>::THREADS, 1)
+template <int PHYS, int N, int E_, int NC_, int NB_>
+__global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
     stage_tc_kernel(const StageArgs a, int ntiles) {
-  using C = TCfg<PHYS, N, E_, NF_, NB_>;
+  using C = TCfg<PHYS, N, E_, NC_, NB_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, NB = C::NB,
-                NF = C::NF;
+                NC = C::NC, TC = C::TC, NCOL = C::NCOL;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char *sBv = smem_raw + C::OFF_BV;             // [hi image][lo image]
+  unsigned char *sBv = smem_raw + C::OFF_BV;
   unsigned char *sBf = smem_raw + C::OFF_BF;
   double *sRing = reinterpret_cast<double *>(smem_raw + C::OFF_RING);
   double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
+  double *sR = reinterpret_cast<double *>(smem_raw + C::OFF_R);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
   unsigned long long *full = bars, *empty = bars + NB, *cen = bars + 2 * NB,
-                     *vol_done = cen + C::NCS, *face_done = vol_done + 1, *bar_v = vol_done + 2,
-                     *bar_f = vol_done + 3, *dfull = vol_done + 4, *d_free = vol_done + 6;
+                     *flux_done = cen + C::NCS, *mma_done = flux_done + 1,
+                     *d_free = flux_done + 2;
   unsigned *sTmem = reinterpret_cast<unsigned *>(bars + C::NBARS);
   int *sFm = reinterpret_cast<int *>(bars + C::NBARS + 1);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
@@ -188,22 +189,17 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NF_, NB_>::THREADS, 1)
   if (tid == 0) {
     for (int b = 0; b < NB; b++) {
       mbar_init(&full[b], 1 + 32);   // the byte-count arrive + each producer lane's gathers
-      mbar_init(&empty[b], 4);
+      mbar_init(&empty[b], NC);
     }
     for (int c = 0; c < C::NCS; c++) mbar_init(&cen[c], 1);
-    mbar_init(vol_done, C::NVW);
-    mbar_init(face_done, C::NFW);
-    mbar_init(bar_v, 1);
-    mbar_init(bar_f, 1);
-    for (int b = 0; b < 2; b++) {
-      mbar_init(&dfull[b], 1);
-      mbar_init(&d_free[b], 4);
-    }
+    mbar_init(flux_done, NC);
+    mbar_init(mma_done, 1);
+    for (int b = 0; b < 2; b++) mbar_init(&d_free[b], 4);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
   // the operand images start zeroed: the volume K padding [KV, KVA) and the
-  // rows past NV E are never written
+  // rows past 2 NCOL are never written
   for (int i = tid; i < (int)(C::OFF_RING / 16); i += C::THREADS)
     reinterpret_cast<uint4 *>(smem_raw)[i] = make_uint4(0, 0, 0, 0);
   if (warp == 0) tmem_alloc(sTmem, C::TMEM_COLS);
@@ -236,102 +232,91 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NF_, NB_>::THREADS, 1)
   unsigned long long vmax = 0ull;
   bool ok = true;
 
-  if (warp < NF) {
-    // ---------------------------------------------------------- flux warps
-    // node-0 fluxes of ring iteration `it` (lane e < E): the volume terms
-    // metric_d . F(u_0) and the face terms Fscale_f n_f . F(u_0), into centre
-    // slot it % NCS, then cen[it % NCS] is arrived on
-    auto centers = [&](int it) -> bool {
-      if (!mbar_wait(&full[it % NB], (it / NB) & 1, lim)) return false;
-      const int e = lane;
-      if (e < E) {
-        const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
-        const double *bU = ring(it), *bG = bU + C::S_U + C::S_K + C::S_UP, *bF = bG + C::S_GEO;
-        double *c = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN;
-        if (e < ne) {
-          double q[5], F[5], G[5], W[5];
+  // node-0 fluxes of ring iteration `it` (lane e < E of the producer warp):
+  // the volume terms metric_d . F(u_0) and the face terms Fscale_f n_f .
+  // F(u_0), into centre slot it % NCS
+  auto centers = [&](int it) {
+    const int e = lane;
+    if (e >= E) return;
+    const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
+    const double *bU = ring(it), *bG = bU + C::S_U + C::S_K + C::S_UP, *bF = bG + C::S_GEO;
+    double *c = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN;
+    if (e < ne) {
+      double q[5], F[5], G[5], W[5];
 #pragma unroll
-          for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
-          euler_flux_fast(gam, q, F, G, W);
-          double m[9];
-#pragma unroll
-          for (int i = 0; i < 9; i++) m[i] = bG[i * E + e];
-          double nf[4][4];
-#pragma unroll
-          for (int f = 0; f < 4; f++)
-#pragma unroll
-            for (int x = 0; x < 4; x++) nf[f][x] = bF[x * 4 * E + e * 4 + f];
-#pragma unroll
-          for (int v = 0; v < 5; v++) {
-#pragma unroll
-            for (int d = 0; d < 3; d++)
-              c[v * C::NCEN + d] = m[3 * d] * F[v] + m[3 * d + 1] * G[v] + m[3 * d + 2] * W[v];
-#pragma unroll
-            for (int f = 0; f < 4; f++)
-              c[v * C::NCEN + 3 + f] =
-                  (nf[f][0] * F[v] + nf[f][1] * G[v] + nf[f][2] * W[v]) * nf[f][3];
-          }
-        } else {
-#pragma unroll
-          for (int x = 0; x < NV * C::NCEN; x++) c[x] = 0.0;
-        }
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&cen[it % C::NCS]);
-      return true;
-    };
-
-    // volume fluxes of ring iteration `it`, warp task wt: 8 elements x 4
-    // node pairs, centred and split into the two volume images
-    auto vol_task = [&](int it, int wt, int ne) {
-      const int eb = wt / C::NHB, hb = wt - eb * C::NHB;
-      const int e = eb * 8 + (lane & 7), h = hb * 4 + (lane >> 3);
-      if (h >= C::NPAIR) return;
-      const bool live = e < ne;
-      const double *bU = ring(it), *bG = bU + C::S_U + C::S_K + C::S_UP;
-      const double *cn = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN;
+      for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
+      euler_flux_fast(gam, q, F, G, W);
       double m[9];
 #pragma unroll
       for (int i = 0; i < 9; i++) m[i] = bG[i * E + e];
-      unsigned h0[5][3], l0[5][3];
+      double nf[4][4];
 #pragma unroll
-      for (int r = 0; r < 2; r++) {
-        const int i = 2 * h + r;
-        const bool okn = live && i < Np;
-        double F[5], G[5], W[5];
-        if (okn) {
-          double q[5];
+      for (int f = 0; f < 4; f++)
 #pragma unroll
-          for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
-          euler_flux_fast(gam, q, F, G, W);
-        }
+        for (int x = 0; x < 4; x++) nf[f][x] = bF[x * 4 * E + e * 4 + f];
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+          c[v * C::NCEN + d] = m[3 * d] * F[v] + m[3 * d + 1] * G[v] + m[3 * d + 2] * W[v];
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+          c[v * C::NCEN + 3 + f] =
+              (nf[f][0] * F[v] + nf[f][1] * G[v] + nf[f][2] * W[v]) * nf[f][3];
+      }
+    } else {
+#pragma unroll
+      for (int x = 0; x < NV * C::NCEN; x++) c[x] = 0.0;
+    }
+  };
+
+  if (warp < NC) {
+    // ------------------------------------------------------- compute warps
+    // volume fluxes of ring iteration `it`, task wt: 8 elements x nodes
+    // 4g .. 4g+3, centred and split into the operand image
+    auto vol_task = [&](int it, int wt, int ne) {
+      const int eb = wt / C::NG, g = wt - eb * C::NG;
+      const int e = eb * 8 + (lane & 7), i = 4 * g + (lane >> 3);
+      const bool okn = e < ne && i < Np;
+      const double *bU = ring(it), *bG = bU + C::S_U + C::S_K + C::S_UP;
+      unsigned hv[5][3], lv[5][3];
+      if (okn) {
+        const double *cn = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN;
+        double q[5], F[5], G[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
+        euler_flux_fast(gam, q, F, G, W);
+        double m[9];
+#pragma unroll
+        for (int x = 0; x < 9; x++) m[x] = bG[x * E + e];
 #pragma unroll
         for (int v = 0; v < 5; v++)
 #pragma unroll
-          for (int d = 0; d < 3; d++) {
-            unsigned hi = 0u, lo = 0u;
+          for (int d = 0; d < 3; d++)
             // the node-0 term enters the first FMA of the metric combination
-            if (okn)
-              split_tf32_pair(fma(m[3 * d + 2], W[v],
-                                  fma(m[3 * d + 1], G[v], fma(m[3 * d], F[v],
-                                                              -cn[v * C::NCEN + d]))),
-                              hi, lo);
-            if (r == 0) {
-              h0[v][d] = hi;
-              l0[v][d] = lo;
-            } else {
-              const int n = v * E + e, k0 = (h >> 1) * 12 + d * 4 + (h & 1) * 2;
-              const int off =
-                  (n >> 3) * C::SBO_V + (k0 >> 2) * 128 + (n & 7) * 16 + (k0 & 3) * 4;
-              *reinterpret_cast<uint2 *>(sBv + off) = make_uint2(h0[v][d], hi);
-              *reinterpret_cast<uint2 *>(sBv + C::BV_PART + off) = make_uint2(l0[v][d], lo);
-            }
-          }
+            split_tf32_pair(fma(m[3 * d + 2], W[v],
+                                fma(m[3 * d + 1], G[v], fma(m[3 * d], F[v],
+                                                            -cn[v * C::NCEN + d]))),
+                            hv[v][d], lv[v][d]);
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+#pragma unroll
+          for (int d = 0; d < 3; d++) hv[v][d] = lv[v][d] = 0u;
       }
+#pragma unroll
+      for (int v = 0; v < 5; v++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const int n = v * E + e, k = g * 12 + d * 4 + (lane >> 3);
+          const int off = (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4;
+          *reinterpret_cast<unsigned *>(sBv + (n >> 3) * C::SBO_V + off) = hv[v][d];
+          *reinterpret_cast<unsigned *>(sBv + ((n + NCOL) >> 3) * C::SBO_V + off) = lv[v][d];
+        }
     };
 
-    // face fluxes of ring iteration `it`, warp task wt: each lane one face
-    // node of 8 elements x 4 nodes of one face, neighbour traces staged
+    // face fluxes of ring iteration `it`, task wt: each lane one face node
+    // of 8 elements x 4 nodes of one face, neighbour traces staged
     auto face_task = [&](int it, int wt, int ne) {
       const int eb = wt / (4 * C::NJB), f = (wt / C::NJB) & 3, jb = wt % C::NJB;
       const int e = eb * 8 + (lane & 7), j = jb * 4 + (lane >> 3);
@@ -365,45 +350,146 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NF_, NB_>::THREADS, 1)
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const int n = v * E + e;
-        const int off = (n >> 3) * C::SBO_F + (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4;
-        *reinterpret_cast<unsigned *>(sBf + off) = hv[v];
-        *reinterpret_cast<unsigned *>(sBf + C::BF_PART + off) = lv[v];
+        const int off = (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4;
+        *reinterpret_cast<unsigned *>(sBf + (n >> 3) * C::SBO_F + off) = hv[v];
+        *reinterpret_cast<unsigned *>(sBf + ((n + NCOL) >> 3) * C::SBO_F + off) = lv[v];
       }
     };
 
-    const bool volw = warp < C::NVW;
-    if (my_tiles > 0 && warp == NF - 1) ok = centers(0);
+    // epilogue of ring iteration `it` from accumulator buffer it % 2
+    auto epilogue = [&](int it) {
+      const int db = it & 1;
+      const long e0 = tile_e0(it);
+      const int ne = (int)min((long)E, (long)a.K - e0);
+      double *bU = ring(it);
+      const double *bK = bU + C::S_U;
+      // every compute warp is done with the staging of the previous update
+      consumer_sync(TC);
+      if (warp < 4) {
+        // lane 2j + p of quarter q holds row (node NPQ q + j, operator part p)
+        const int q = warp, p = lane & 1, j = lane >> 1, node = C::NPQ * q + j;
+        const bool on = j < C::NPQ && node < Np;
+        float r[2 * NCOL];
+        const unsigned row = tmem + ((unsigned)(32 * q) << 16) + db * C::D_COLS;
+#pragma unroll
+        for (int c = 0; c < 2 * NCOL; c += 4) tmem_ld4(row + c, r + c);
+        tmem_ld_wait();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&d_free[db]);   // the accumulator is free for tile it + 2
+        // part products of this row, then the partner's half: lane p takes
+        // columns [p H, (p+1) H) (register indices stay compile-time)
+        constexpr int H = NCOL / 2;
+#pragma unroll
+        for (int c = 0; c < H; c++) {
+          const float lo_half = r[c] + r[NCOL + c], hi_half = r[H + c] + r[NCOL + H + c];
+          const float other = __shfl_xor_sync(0xffffffffu, p ? lo_half : hi_half, 1);
+          if (on) sR[(p * H + c) * Np + node] = (double)((p ? hi_half : lo_half) + other);
+        }
+      }
+      consumer_sync(TC);
+      // LSERK update, one flat loop over (variable, element, node): staged
+      // rhs, u and k, coalesced stores
+      const int nep = ne * Np;
+      for (int x = tid; x < NV * nep; x += TC) {
+        const int v = x / nep, g = x - v * nep;
+        const int si = v * E * Np + g;
+        const long gi = v * vs + e0 * Np + g;
+        const double rhs = sR[si];
+        if (a.rhs_only) {
+          a.u_out[gi] = rhs;
+        } else {
+          const double kn = a.rka * bK[si] + dt * rhs;
+          const double un = bU[si] + a.rkb * kn;
+          a.kreg[gi] = kn;
+          a.u_out[gi] = un;
+          if (keep_u) bU[si] = un;
+        }
+      }
+      if (keep_u) {
+        // fused calc_maxv on the new state: per face, max |v|^2 and c^2 over
+        // its nodes (divisions as in face_maxv_kernel, so dt does not depend
+        // on which kernel computed maxv)
+        consumer_sync(TC);
+        const double *bF = bU + C::S_U + C::S_K + C::S_UP + C::S_GEO;
+        for (int x = tid; x < 4 * E; x += TC) {
+          const int f = x / E, e = x - f * E;
+          if (e >= ne) continue;
+          double mv2 = 0.0, mc2 = 0.0;
+          bool bad = false;
+          for (int jj = 0; jj < Nfp; jj++) {
+            const int nd = e * Np + sFm[f * Nfp + jj];
+            const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
+                         u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
+            const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
+            const double v2 = vx * vx + vy * vy + vz * vz;
+            const double pres = (gam - 1) * (u5 - 0.5 * u1 * v2);
+            const double c2 = fabs(gam * pres / u1);
+            mv2 = v2 > mv2 ? v2 : mv2;
+            mc2 = c2 > mc2 ? c2 : mc2;
+            bad |= (v2 != v2) || (c2 != c2);
+          }
+          double mv = sqrt(mv2) + sqrt(mc2);
+          if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+          a.maxv[(e0 + e) * 4 + f] = mv;
+          const unsigned long long bits = dbits(mv * bF[3 * 4 * E + e * 4 + f]);
+          vmax = bits > vmax ? bits : vmax;
+        }
+      }
+      // this warp is done with the ring slot (generic-proxy writes precede
+      // the producer's next bulk copies into it)
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[it % NB]);
+    };
+
     for (int it = 0; ok && it < my_tiles; it++) {
       const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
-      // tile data, its node-0 fluxes, and the previous tile's MMAs done with
-      // this warp's operand image
+      // tile data, its node-0 fluxes, and MMA(t-1) done with the operand images
       bool w = mbar_wait(&full[it % NB], (it / NB) & 1, lim) &&
                mbar_wait(&cen[it % C::NCS], (it / C::NCS) & 1, lim);
-      if (it > 0) w = w && mbar_wait(volw ? bar_v : bar_f, (it - 1) & 1, lim);
-      if (!w) {
+      if (it > 0) w = w && mbar_wait(mma_done, (it - 1) & 1, lim);
+      if (!consumer_all(w, TC)) {
         ok = false;
         break;
       }
-      // the last face warp first computes the node-0 fluxes of the next tile
-      // (its data is normally resident: the ring runs two tiles ahead)
-      if (warp == NF - 1 && it + 1 < my_tiles && !centers(it + 1)) {
-        ok = false;
-        break;
-      }
-      if (volw) {
-        vol_task(it, warp, ne);
-      } else {
-        for (int wt = warp - C::NVW; wt < C::FACE_WT; wt += C::NFW) face_task(it, wt, ne);
+      tc_fence_after();
+      for (int wt = warp; wt < C::NTASK; wt += NC) {
+        if (wt < C::VOL_WT)
+          vol_task(it, wt, ne);
+        else
+          face_task(it, wt - C::VOL_WT, ne);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(volw ? vol_done : face_done);
+      if (lane == 0) mbar_arrive(flux_done);
+      if (it > 0) epilogue(it - 1);
+    }
+    if (ok && my_tiles > 0) {
+      ok = consumer_all(mbar_wait(mma_done, (my_tiles - 1) & 1, lim), TC);
+      if (ok) {
+        tc_fence_after();
+        epilogue(my_tiles - 1);
+      }
     }
   } else if (warp == C::PROD_WARP) {
     // ------------------------------------------------------ producer warp
+    // per ring iteration: the node-0 fluxes of the previous tile (landed by
+    // now: they run ahead of the compute warps), then the copies of this one
+    auto centers_of = [&](int t) -> bool {
+      if (!mbar_wait(&full[t % NB], (t / NB) & 1, lim)) return false;
+      centers(t);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&cen[t % C::NCS]);
+      return true;
+    };
     int it = 0;
     for (; it < my_tiles; it++) {
       const int b = it % NB;
+      if (it > 0 && !centers_of(it - 1)) {
+        ok = false;
+        break;
+      }
       if (it >= NB && !mbar_wait(&empty[b], ((it / NB) - 1) & 1, lim)) {
         ok = false;
         break;
@@ -452,16 +538,17 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NF_, NB_>::THREADS, 1)
       }
       cp_async_arrive_noinc(&full[b]);
     }
+    if (ok && it > 0 && !centers_of(it - 1)) ok = false;
     // the copies of the last NB tiles land before this warp leaves
     for (int j = (it > NB ? it - NB : 0); j < it; j++) mbar_wait(&full[j % NB], (j / NB) & 1);
     asm volatile("cp.async.wait_all;" ::: "memory");
-  } else if (warp == C::MMA_WARP) {
+  } else {
     // ----------------------------------------------------------- MMA warp
     if (lane == 0) {
-      int nv = 0, nf = 0;   // commits issued to bar_v / bar_f
+      int nm = 0;   // commits issued to mma_done
       for (int it = 0; it < my_tiles; it++) {
         const int db = it & 1;
-        bool w = mbar_wait(vol_done, it & 1, lim);
+        bool w = mbar_wait(flux_done, it & 1, lim);
         if (it >= 2) w = w && mbar_wait(&d_free[db], ((it >> 1) - 1) & 1, lim);
         if (!w) {
           ok = false;
@@ -471,125 +558,19 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NF_, NB_>::THREADS, 1)
         const unsigned d = tmem + db * C::D_COLS;
         const unsigned bv = smem_u32(sBv), bf = smem_u32(sBf);
 #pragma unroll 1
-        for (int ks = 0; ks < C::KSV; ks++) {
+        for (int ks = 0; ks < C::KSV; ks++)
           tc_mma_ts(d, tmem + C::A_COL + ks * 8, smem_desc(bv + ks * 256, 128, C::SBO_V),
                     C::IDESC, ks > 0);
-          tc_mma_ts(d, tmem + C::A_COL + ks * 8,
-                    smem_desc(bv + C::BV_PART + ks * 256, 128, C::SBO_V), C::IDESC, 1);
-        }
-        tc_commit(bar_v);
-        nv++;
-        if (!mbar_wait(face_done, it & 1, lim)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
 #pragma unroll 1
-        for (int ks = 0; ks < C::KSF; ks++) {
+        for (int ks = 0; ks < C::KSF; ks++)
           tc_mma_ts(d, tmem + C::A_COL + C::KVA + ks * 8,
                     smem_desc(bf + ks * 256, 128, C::SBO_F), C::IDESC, 1);
-          tc_mma_ts(d, tmem + C::A_COL + C::KVA + ks * 8,
-                    smem_desc(bf + C::BF_PART + ks * 256, 128, C::SBO_F), C::IDESC, 1);
-        }
-        tc_commit(bar_f);
-        tc_commit(&dfull[db]);
-        nf++;
+        tc_commit(mma_done);
+        nm++;
       }
-      // the MMAs issued (and their barrier arrivals) are complete before
+      // the MMAs issued (and their barrier arrival) are complete before
       // tensor and shared memory are released, on expiry too
-      if (nv) mbar_wait(bar_v, (nv - 1) & 1);
-      if (nf) mbar_wait(bar_f, (nf - 1) & 1);
-    }
-  } else {
-    // ------------------------------------------------------ epilogue warps
-    const int q = warp & 3;                          // lane quarter of this warp
-    const int p = lane & 1, j = lane >> 1, node = C::NPQ * q + j;
-    const bool on = j < C::NPQ && node < Np;
-    for (int it = 0; it < my_tiles; it++) {
-      const int db = it & 1;
-      const long e0 = tile_e0(it);
-      const int ne = (int)min((long)E, (long)a.K - e0);
-      double *bU = ring(it);
-      const double *bK = bU + C::S_U;
-      if (!mbar_wait(&dfull[db], (it >> 1) & 1, lim) ||
-          !mbar_wait(&full[it % NB], (it / NB) & 1, lim)) {
-        ok = false;
-        break;
-      }
-      tc_fence_after();
-      // this lane's row (node, part p) for the used columns; the pair's two
-      // lanes each take half of the columns and add the partner's part
-      float r[2 * C::HALF];
-      const unsigned rowaddr = tmem + ((unsigned)(32 * q) << 16) + db * C::D_COLS;
-#pragma unroll
-      for (int c = 0; c < 2 * C::HALF; c += 4) {
-        unsigned v4[4];
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
-                     : "=r"(v4[0]), "=r"(v4[1]), "=r"(v4[2]), "=r"(v4[3])
-                     : "r"(rowaddr + c)
-                     : "memory");
-#pragma unroll
-        for (int i = 0; i < 4; i++) r[c + i] = __uint_as_float(v4[i]);
-      }
-      tmem_ld_wait();
-      // accumulator buffer db is free for tile it + 2
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&d_free[db]);
-#pragma unroll
-      for (int c = 0; c < C::HALF; c++) {
-        const float mine = p ? r[C::HALF + c] : r[c];
-        const float other = __shfl_xor_sync(0xffffffffu, p ? r[c] : r[C::HALF + c], 1);
-        const int col = p * C::HALF + c, v = col / E, e = col - v * E;
-        if (!on || col >= C::NCOL || e >= ne) continue;
-        const double rhs = (double)(mine + other);
-        const long gi = v * vs + (e0 + e) * Np + node;
-        const int si = v * E * Np + e * Np + node;
-        if (a.rhs_only) {
-          a.u_out[gi] = rhs;
-        } else {
-          const double kn = a.rka * bK[si] + dt * rhs;
-          const double un = bU[si] + a.rkb * kn;
-          a.kreg[gi] = kn;
-          a.u_out[gi] = un;
-          if (keep_u) bU[si] = un;
-        }
-      }
-      if (keep_u) {
-        // fused calc_maxv on the new state: per face, max |v|^2 and c^2 over
-        // its nodes (divisions as in face_maxv_kernel, so dt does not depend
-        // on which kernel computed maxv)
-        epi_sync();
-        const double *bF = bU + C::S_U + C::S_K + C::S_UP + C::S_GEO;
-        for (int x = tid - 32 * C::EPI_WARP; x < 4 * E; x += 128) {
-          const int f = x / E, e = x - f * E;
-          if (e >= ne) continue;
-          double mv2 = 0.0, mc2 = 0.0;
-          bool bad = false;
-          for (int jj = 0; jj < Nfp; jj++) {
-            const int nd = e * Np + sFm[f * Nfp + jj];
-            const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
-                         u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
-            const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-            const double v2 = vx * vx + vy * vy + vz * vz;
-            const double pres = (gam - 1) * (u5 - 0.5 * u1 * v2);
-            const double c2 = fabs(gam * pres / u1);
-            mv2 = v2 > mv2 ? v2 : mv2;
-            mc2 = c2 > mc2 ? c2 : mc2;
-            bad |= (v2 != v2) || (c2 != c2);
-          }
-          double mv = sqrt(mv2) + sqrt(mc2);
-          if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
-          a.maxv[(e0 + e) * 4 + f] = mv;
-          const unsigned long long bits = dbits(mv * bF[3 * 4 * E + e * 4 + f]);
-          vmax = bits > vmax ? bits : vmax;
-        }
-      }
-      // the ring slot is free for the producer (generic-proxy writes precede
-      // its next bulk copies)
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[it % NB]);
+      if (nm) mbar_wait(mma_done, (nm - 1) & 1);
     }
   }
   if (!ok) atomicOr(&a.sc->flags, 4);
