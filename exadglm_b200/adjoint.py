@@ -12,7 +12,10 @@ differentiated; finite-difference checks must replay them
 
 Memory: the forward run keeps a checkpoint every ``checkpoint_every`` steps;
 the backward pass recomputes each segment once from its checkpoint, keeping
-its 5 stage inputs per step, and sweeps it in reverse.
+its 5 stage inputs per step, and sweeps it in reverse.  With ``max_bytes``
+the tape instead stays under that many bytes of device memory by binomial
+checkpointing (revolve): fewer checkpoints, more forward steps recomputed,
+the same gradient.
 
 The reference has no adjoint; this module has no counterpart there.
 """
@@ -24,11 +27,12 @@ from .capi import Solver
 
 
 class DGLMStep(torch.autograd.Function):
-    """``DGLMStep.apply(u0, solver, nsteps, checkpoint_every)``: u(T) after
-    ``nsteps`` CFL steps from u0; its backward is the discrete adjoint."""
+    """``DGLMStep.apply(u0, solver, nsteps, checkpoint_every, max_bytes)``:
+    u(T) after ``nsteps`` CFL steps from u0; its backward is the discrete
+    adjoint (max_bytes: None, or a cap on the tape's device memory)."""
 
     @staticmethod
-    def forward(ctx, u0, solver, nsteps, checkpoint_every):
+    def forward(ctx, u0, solver, nsteps, checkpoint_every, max_bytes=None):
         nv = solver.p.nvar
         if u0.dtype != torch.float64 or not u0.is_cuda or tuple(u0.shape) != (
                 nv, solver.p.K * solver.p.Np):
@@ -36,7 +40,10 @@ class DGLMStep(torch.autograd.Function):
         u0c = u0.detach().contiguous()
         torch.cuda.current_stream(u0c.device).synchronize()
         solver.set_state_device([u0c[v].data_ptr() for v in range(nv)])
-        solver.adjoint_record(int(nsteps), int(checkpoint_every))
+        if max_bytes is None:
+            solver.adjoint_record(int(nsteps), int(checkpoint_every))
+        else:
+            solver.adjoint_record_capped(int(nsteps), int(max_bytes))
         uT = torch.empty_like(u0c)
         solver.get_state_device([uT[v].data_ptr() for v in range(nv)])
         solver._tape_id = getattr(solver, "_tape_id", 0) + 1
@@ -55,12 +62,14 @@ class DGLMStep(torch.autograd.Function):
         lam0 = torch.empty_like(g)
         s.adjoint_backward_device([g[v].data_ptr() for v in range(nv)],
                                   [lam0[v].data_ptr() for v in range(nv)])
-        return lam0, None, None, None
+        return lam0, None, None, None, None
 
 
-def evolve(u0: torch.Tensor, solver: Solver, nsteps: int, checkpoint_every: int = 50):
-    """u(T) after nsteps CFL steps from u0, differentiable with respect to u0."""
-    return DGLMStep.apply(u0, solver, nsteps, checkpoint_every)
+def evolve(u0: torch.Tensor, solver: Solver, nsteps: int, checkpoint_every: int = 50,
+           max_bytes: int | None = None):
+    """u(T) after nsteps CFL steps from u0, differentiable with respect to u0;
+    max_bytes caps the tape's device memory (binomial checkpointing)."""
+    return DGLMStep.apply(u0, solver, nsteps, checkpoint_every, max_bytes)
 
 
 def density_misfit(uT: torch.Tensor, rho_target: torch.Tensor) -> torch.Tensor:

@@ -29,6 +29,7 @@ EXPORTS = (
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
     "dglm_set_variant", "dglm_get_variant", "dglm_set_wait_limit", "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
+    "dglm_adjoint_record_capped", "dglm_adjoint_tape_plan", "dglm_adjoint_schedule",
     "dglm_calc_maxv_dt_static", "dglm_adjoint_variant_count", "dglm_adjoint_variant_describe",
     "dglm_adjoint_set_variant", "dglm_batch_create", "dglm_batch_add", "dglm_batch_finalize",
     "dglm_batch_step", "dglm_batch_sync", "dglm_batch_count", "dglm_batch_get_state",
@@ -117,6 +118,11 @@ def lib():
         L.dglm_adjoint_replay.argtypes = [_P]
         L.dglm_adjoint_rhs.argtypes = [_P, _P, _P, _P]
         L.dglm_adjoint_tape_bytes.argtypes = [_P, C.POINTER(C.c_size_t)]
+        L.dglm_adjoint_record_capped.argtypes = [_P, I, C.c_size_t]
+        L.dglm_adjoint_tape_plan.argtypes = [_P, C.POINTER(I), C.POINTER(I),
+                                             C.POINTER(C.c_longlong)]
+        L.dglm_adjoint_schedule.argtypes = [I, I, I, I, _P, I, C.POINTER(I), _P, I, C.POINTER(I),
+                                            C.POINTER(C.c_longlong)]
         L.dglm_adjoint_variant_describe.argtypes = [I, I, I, C.c_char_p, C.c_size_t]
         L.dglm_batch_create.argtypes = [C.POINTER(BatchDesc), C.POINTER(_P)]
         L.dglm_batch_add.argtypes = [_P, I, I, C.POINTER(MeshArrays), _P, _P, C.POINTER(I)]
@@ -174,6 +180,22 @@ def variants(physics, N, precision=None):
     if precision is None:
         return out
     return [(i, d) for i, d in enumerate(out) if variant_precision(d) == precision]
+
+
+def adjoint_schedule(nsteps, leaf, slots, prestored=True):
+    """The binomial checkpointing schedule (host only): (spine, actions,
+    advance_steps); spine[q] = chunk held by slot q after the recording,
+    actions = rows (kind, src, chunk, count, dst), kind 0 advance, 1 reverse."""
+    L = lib()
+    n = (int(nsteps) + int(leaf) - 1) // int(leaf)
+    cap_a = 4 * n * n + 16
+    spine = np.zeros(n + 1, dtype=np.int32)
+    acts = np.zeros((cap_a, 5), dtype=np.int32)
+    ns, na, adv = C.c_int(), C.c_int(), C.c_longlong()
+    check(L.dglm_adjoint_schedule(int(nsteps), int(leaf), int(slots), int(bool(prestored)),
+                                  spine.ctypes.data, len(spine), C.byref(ns), acts.ctypes.data,
+                                  cap_a, C.byref(na), C.byref(adv)))
+    return spine[:ns.value].copy(), acts[:na.value].copy(), adv.value
 
 
 def adjoint_variants(physics, N):
@@ -358,6 +380,19 @@ class Solver:
     def adjoint_record(self, nsteps, checkpoint_every=50):
         """nsteps CFL steps from the current state, recording the tape."""
         check(self.L.dglm_adjoint_record(self.h, int(nsteps), int(checkpoint_every)))
+
+    def adjoint_record_capped(self, nsteps, max_bytes):
+        """nsteps CFL steps from the current state, recording a tape of at
+        most max_bytes of device memory (binomial checkpointing)."""
+        check(self.L.dglm_adjoint_record_capped(self.h, int(nsteps), int(max_bytes)))
+
+    def adjoint_tape_plan(self):
+        """(leaf steps, checkpoint slots, forward steps the next backward
+        pass recomputes) of the recorded tape."""
+        leaf, slots, adv = C.c_int(), C.c_int(), C.c_longlong()
+        check(self.L.dglm_adjoint_tape_plan(self.h, C.byref(leaf), C.byref(slots),
+                                            C.byref(adv)))
+        return leaf.value, slots.value, adv.value
 
     def adjoint_backward(self, lam_T):
         """(du_T/du_0)^T lam_T for the recorded run (numpy in, numpy out)."""

@@ -948,6 +948,17 @@ struct AdjointTape {
   double *store = nullptr;   // cap_store states: stage inputs of one segment
   std::vector<void *> fixed, sized;   // allocations: per mesh / per recording size
   size_t bytes = 0, sized_bytes = 0;
+  // binomial (revolve) recording under a memory cap: chunks of `leaf`
+  // steps, `slots` state checkpoints (slot 0: the initial state), the
+  // checkpoints the recording placed (spine[q] = chunk held by slot q)
+  bool capped = false, spine_valid = false;
+  int leaf = 0, slots = 0, nchunk = 0;
+  long long advance_steps = 0;   // forward steps recomputed by one backward pass
+  std::vector<int> spine;
+  std::vector<int> plan_split;   // split[n][free] of the schedule table
+  int plan_f = 0;                // its free-slot columns - 1
+  double *maxv_tmp = nullptr, *tau_tmp = nullptr;   // wave speeds / tau of a recomputed step
+  DevScalars *sc_tmp = nullptr;
 };
 
 namespace dglm {
@@ -1170,6 +1181,231 @@ cudaError_t frozen_stage(dglm_handle *h, const double *u_in, double *u_out, doub
   return launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, cs);
 }
 
+// ---- binomial checkpointing under a memory cap ------------------------------
+// Binomial checkpointing (Griewank and Walther, "Algorithm 799: revolve",
+// ACM TOMS 26, 2000) over chunks of `leaf` LSERK steps.  A chunk is
+// reversed by recomputing its stage inputs once from the state at its start
+// (into the stage store) and sweeping it backwards; reaching that state from
+// a checkpoint costs forward steps ("advances").  With the state of chunk c0
+// in a slot and `free` further slots, n chunks are reversed by advancing m
+// chunks, storing that state in a free slot, reversing the last n - m chunks
+// with one slot fewer and then the first m with the same slots.  The fewest
+// chunk advances follow from the recursion
+//   cost[1][f] = 0,  cost[n][0] = n (n - 1) / 2,
+//   cost[n][f] = min(cost[n][f-1], min_m  m + cost[n-m][f-1] + cost[m][f]),
+// solved here as a table (the binomial optimum of revolve, computed instead
+// of taken from its closed form).
+struct RevolvePlan {
+  int n = 0, f = 0;
+  std::vector<long long> cost;
+  std::vector<int> split;   // 0: the slot is not used for this (n, f)
+  long long c(int a, int b) const { return cost[(size_t)a * (f + 1) + b]; }
+  int m(int a, int b) const { return split[(size_t)a * (f + 1) + b]; }
+};
+
+void plan_revolve(RevolvePlan &p, int n, int f) {
+  p.n = n;
+  p.f = f;
+  p.cost.assign((size_t)(n + 1) * (f + 1), 0);
+  p.split.assign((size_t)(n + 1) * (f + 1), 0);
+  for (int a = 1; a <= n; a++) {
+    p.cost[(size_t)a * (f + 1)] = (long long)a * (a - 1) / 2;
+    for (int b = 1; b <= f; b++) {
+      long long best = p.c(a, b - 1);
+      int bm = 0;
+      for (int m = 1; m < a; m++) {
+        const long long v = m + p.c(a - m, b - 1) + p.c(m, b);
+        if (v < best) {
+          best = v;
+          bm = m;
+        }
+      }
+      p.cost[(size_t)a * (f + 1) + b] = best;
+      p.split[(size_t)a * (f + 1) + b] = bm;
+    }
+  }
+}
+
+// One action of a backward pass: advance `count` chunks from the state of
+// chunk `chunk` (in slot src) into slot dst (-1: the scratch state), or
+// reverse chunk `chunk` starting from slot src (-1: the scratch state).
+struct RevAction {
+  int kind, src, chunk, count, dst;   // kind 0: advance, 1: reverse a chunk
+};
+
+// checkpoints the recording places: spine[q] = chunk whose start state
+// slot q holds (slot 0: chunk 0), the first path of the schedule
+void revolve_spine(const RevolvePlan &p, int nchunk, int free, std::vector<int> &spine) {
+  spine.assign(1, 0);
+  int c0 = 0, n = nchunk;
+  while (n > 1 && free > 0) {
+    const int m = p.m(n, free);
+    free--;
+    if (m == 0) continue;
+    c0 += m;
+    n -= m;
+    spine.push_back(c0);
+  }
+}
+
+// actions reversing chunks [c0, c0 + n) from the state of c0 in `slot`;
+// pre: the recording already stored this path's checkpoints
+void revolve_actions(const RevolvePlan &p, int c0, int n, int slot, int free, bool pre,
+                     std::vector<RevAction> &out) {
+  if (n == 1) {
+    out.push_back({1, slot, c0, 1, -1});
+    return;
+  }
+  if (free == 0) {
+    for (int j = n - 1; j >= 1; j--) {
+      out.push_back({0, slot, c0, j, -1});
+      out.push_back({1, -1, c0 + j, 1, -1});
+    }
+    out.push_back({1, slot, c0, 1, -1});
+    return;
+  }
+  const int m = p.m(n, free);
+  if (m == 0) {
+    revolve_actions(p, c0, n, slot, free - 1, pre, out);
+    return;
+  }
+  if (!pre) out.push_back({0, slot, c0, m, slot + 1});
+  revolve_actions(p, c0 + m, n - m, slot + 1, free - 1, pre, out);
+  revolve_actions(p, c0, m, slot, free, false, out);
+}
+
+// forward steps of the advances in a list of actions
+long long revolve_advance_steps(const std::vector<RevAction> &acts, int leaf, int nsteps) {
+  long long n = 0;
+  for (const RevAction &a : acts)
+    if (a.kind == 0)
+      n += std::min((long long)(a.chunk + a.count) * leaf, (long long)nsteps) -
+           (long long)a.chunk * leaf;
+  return n;
+}
+
+// Largest chunk count the schedule table is built for (the table costs
+// kMaxChunks^3 / 2 operations once per recording).
+constexpr int kMaxChunks = 256;
+
+// Bytes of a capped recording's sized part for a given leaf and slot count.
+size_t capped_bytes(const dglm_handle *h, int nsteps, int leaf, int slots) {
+  const AdjointTape *t = h->tape;
+  const bool euler = h->d.physics == DGLM_EULER;
+  auto rnd = [](size_t b) { return std::max<size_t>(b, 16); };
+  size_t b = rnd(sizeof(double) * (size_t)slots * t->state);
+  b += rnd(sizeof(double) * (size_t)5 * leaf * t->state);
+  b += rnd(sizeof(double) * (size_t)nsteps);
+  b += rnd(sizeof(double) * (size_t)(euler ? leaf : 1) * 4 * h->Kp);
+  b += 2 * rnd(sizeof(double) * (size_t)4 * h->Kp);
+  b += rnd(sizeof(DevScalars));
+  return b;
+}
+
+// tau of one step from its input state u (Euler), as the forward step
+// computed it: face wave speeds, then the per-face penalty
+cudaError_t tau_from_state(dglm_handle *h, const double *u, double *tau, cudaStream_t s) {
+  AdjointTape *t = h->tape;
+  StageArgs a = stage_args(h, u, nullptr, -1);
+  a.maxv = t->maxv_tmp;
+  a.sc = t->sc_tmp;
+  cudaError_t e = launch_face_maxv(h->d.physics, h->d.N, a, 0, s);
+  if (e == cudaSuccess) e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, t->maxv_tmp, tau, s);
+  h->launches += 2;
+  return e;
+}
+
+// advance: the stages of `count` chunks from the state `src` of chunk c0,
+// the last stage writing `dst`; stage outputs alternate between the first
+// two states of the stage store, tau is recomputed from each step's input
+cudaError_t capped_advance(dglm_handle *h, const double *src, int c0, int count, double *dst,
+                           cudaStream_t s) {
+  AdjointTape *t = h->tape;
+  const bool euler = h->d.physics == DGLM_EULER;
+  const int i0 = c0 * t->leaf, i1 = std::min((c0 + count) * t->leaf, t->nsteps);
+  const int last = 5 * (i1 - i0) - 1;
+  const double *in = src;
+  cudaError_t e = cudaSuccess;
+  int g = 0;
+  for (int i = i0; i < i1 && e == cudaSuccess; i++)
+    for (int k = 0; k < 5 && e == cudaSuccess; k++, g++) {
+      if (k == 0 && euler) e = tau_from_state(h, in, t->tau_tmp, s);
+      double *out = g == last ? dst : t->store + (size_t)(g & 1) * t->state;
+      if (e == cudaSuccess)
+        e = frozen_stage(h, in, out, t->kbuf, k, t->dt[i], euler ? t->tau_tmp : t->tau, s);
+      h->launches++;
+      in = out;
+    }
+  return e;
+}
+
+// reverse one chunk from the state `src` at its start: its stage inputs
+// recomputed into the stage store (tau of each step beside them), then the
+// adjoint stages in reverse order (phi ping-pong index p carried across)
+cudaError_t capped_reverse_chunk(dglm_handle *h, AdjArgs &a, int &p, int c, const double *src,
+                                 cudaStream_t s) {
+  AdjointTape *t = h->tape;
+  const bool euler = h->d.physics == DGLM_EULER;
+  const int s0 = c * t->leaf, s1 = std::min(s0 + t->leaf, t->nsteps);
+  auto slot = [&](int j) -> const double * {
+    return j == 0 ? src : t->store + (size_t)(j - 1) * t->state;
+  };
+  auto tau_i = [&](int i) -> double * {
+    return euler ? t->tau + (size_t)(i - s0) * 4 * h->Kp : t->tau;
+  };
+  cudaError_t e = cudaSuccess;
+  for (int i = s0; i < s1 && e == cudaSuccess; i++)
+    for (int k = 0; k < 5 && e == cudaSuccess; k++) {
+      const int j = 5 * (i - s0) + k;
+      if (i == s1 - 1 && k == 4) break;   // the last stage's output is not needed
+      if (k == 0 && euler) e = tau_from_state(h, slot(j), tau_i(i), s);
+      if (e == cudaSuccess)
+        e = frozen_stage(h, slot(j), const_cast<double *>(slot(j + 1)), t->kbuf, k, t->dt[i],
+                         tau_i(i), s);
+      h->launches++;
+    }
+  for (int i = s1 - 1; i >= s0 && e == cudaSuccess; i--)
+    for (int k = 4; k >= 0 && e == cudaSuccess; k--) {
+      a.update = 1;
+      a.u = slot(5 * (i - s0) + k);
+      a.tau = tau_i(i);
+      a.dt = t->dt[i];
+      a.rka = RKA[k];
+      a.rkb = RKB[k];
+      a.phi_next = (i == 0 && k == 0) ? 0 : 1;
+      a.rkb_next = k > 0 ? RKB[k - 1] : RKB[4];
+      a.phi_in = t->phi[p];
+      a.phi_out = t->phi[p ^ 1];
+      e = t->var.launch(a, s);
+      h->launches++;
+      p ^= 1;
+    }
+  return e;
+}
+
+// the reverse sweep of a capped recording: the binomial schedule's actions
+cudaError_t capped_sweep(dglm_handle *h, AdjArgs &a, int &p, cudaStream_t s) {
+  AdjointTape *t = h->tape;
+  RevolvePlan plan;
+  plan.f = t->plan_f;
+  plan.split = t->plan_split;
+  std::vector<RevAction> acts;
+  revolve_actions(plan, 0, t->nchunk, 0, t->slots - 1, t->spine_valid, acts);
+  double *scratch = t->store + (size_t)(5 * t->leaf - 1) * t->state;
+  auto ck = [&](int q) { return q < 0 ? scratch : t->ckpt + (size_t)q * t->state; };
+  cudaError_t e = cudaSuccess;
+  for (size_t x = 0; x < acts.size() && e == cudaSuccess; x++) {
+    const RevAction &r = acts[x];
+    if (r.kind == 0)
+      e = capped_advance(h, ck(r.src), r.chunk, r.count, ck(r.dst), s);
+    else
+      e = capped_reverse_chunk(h, a, p, r.chunk, ck(r.src), s);
+  }
+  // the sweep overwrote the recording's checkpoints past slot 0
+  t->spine_valid = false;
+  return e;
+}
+
 dglm_status copy_fields(dglm_handle *h, double *dst, const double *const *src, int on_device,
                         const char *what) {
   const long n = (long)h->d.K * h->Np;
@@ -1213,6 +1449,7 @@ dglm_status dglm_adjoint_record(dglm_handle *h, int nsteps, int checkpoint_every
   if (st != DGLM_OK) return st;
   AdjointTape *t = h->tape;
   t->recorded = false;
+  t->capped = false;
   cudaStream_t s = h->stream;
   const double zero = 0.0;
   cudaError_t e = cudaMemcpyAsync(&h->sc->dt_fixed, &zero, sizeof(double),
@@ -1280,8 +1517,12 @@ dglm_status dglm_adjoint_replay(dglm_handle *h) {
   if (!h->state_ready) return set_error(DGLM_ERR_STATE, "dglm_adjoint_replay: set a state first");
   if (!h->tape || !h->tape->recorded)
     return set_error(DGLM_ERR_STATE, "dglm_adjoint_replay: record a forward run first");
-  DeviceGuard g(h->dev);
   AdjointTape *t = h->tape;
+  if (t->capped)
+    return set_error(DGLM_ERR_STATE,
+                     "dglm_adjoint_replay: a capped recording keeps no per-step tau; record "
+                     "with dglm_adjoint_record to replay");
+  DeviceGuard g(h->dev);
   cudaStream_t s = h->stream;
   cudaError_t e = cudaMemsetAsync(h->kreg, 0, sizeof(double) * t->state, s);
   h->launches = 0;
@@ -1317,7 +1558,8 @@ dglm_status dglm_adjoint_backward(dglm_handle *h, const double *const *lam_T,
   a.phi_out = t->phi[p];
   if (e == cudaSuccess) e = t->var.launch(a, s);
   h->launches++;
-  for (int seg = t->nseg - 1; seg >= 0 && e == cudaSuccess; seg--) {
+  if (t->capped && e == cudaSuccess) e = capped_sweep(h, a, p, s);
+  for (int seg = t->capped ? -1 : t->nseg - 1; seg >= 0 && e == cudaSuccess; seg--) {
     const int s0 = seg * t->every, s1 = std::min(s0 + t->every, t->nsteps);
     double *ck = t->ckpt + (size_t)seg * t->state;
     auto slot = [&](int j) -> double * {
@@ -1353,7 +1595,7 @@ dglm_status dglm_adjoint_backward(dglm_handle *h, const double *const *lam_T,
       }
   }
   // the store now holds the first segment: a second sweep recomputes all
-  if (t->nseg > 1) t->last_seg_stored = false;
+  if (!t->capped && t->nseg > 1) t->last_seg_stored = false;
   if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_backward");
   return fetch_fields(h, lam_0, t->lam, on_device, "dglm_adjoint_backward");
 }
@@ -1429,6 +1671,175 @@ dglm_status dglm_adjoint_set_variant(dglm_handle *h, int variant) {
   cudaStreamSynchronize(h->stream);
   free_tape(h);   // operator layout depends on the tile shape; record again
   h->adj_variant = variant;
+  return DGLM_OK;
+}
+
+dglm_status dglm_adjoint_record_capped(dglm_handle *h, int nsteps, size_t max_bytes) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_adjoint_record_capped: NULL handle");
+  if (!h->state_ready)
+    return set_error(DGLM_ERR_STATE, "dglm_adjoint_record_capped: set a state first");
+  if (nsteps <= 0)
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_record_capped: nsteps must be positive");
+  DeviceGuard g(h->dev);
+  dglm_status st = tape_setup(h);
+  if (st != DGLM_OK) return st;
+  AdjointTape *t = h->tape;
+  t->recorded = false;
+  const size_t fixed = t->bytes - t->sized_bytes;
+  const size_t sbytes = sizeof(double) * (size_t)t->state;
+  // the leaf length and slot count with the fewest recomputed steps
+  const int lmin = (nsteps + kMaxChunks - 1) / kMaxChunks;
+  const int nmax = (nsteps + lmin - 1) / lmin;
+  RevolvePlan plan;
+  plan_revolve(plan, nmax, nmax - 1);
+  int best_l = 0, best_free = 0;
+  long long best_cost = -1;
+  for (int L = lmin; L <= nsteps; L++) {
+    const size_t need = fixed + capped_bytes(h, nsteps, L, 1);
+    if (need > max_bytes) break;   // the store grows with L
+    const int n = (nsteps + L - 1) / L;
+    const long long extra = (long long)((max_bytes - need) / sbytes);
+    const int free = (int)std::min<long long>(extra, n - 1);
+    const long long cost = plan.c(n, free) * L;
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best_l = L;
+      best_free = free;
+    }
+  }
+  if (best_cost < 0)
+    return set_error(DGLM_ERR_NOMEM,
+                     "dglm_adjoint_record_capped: the cap is below the minimum tape of " +
+                         std::to_string(fixed + capped_bytes(h, nsteps, lmin, 1)) + " bytes");
+  const int L = best_l, nchunk = (nsteps + L - 1) / L, slots = best_free + 1;
+  const bool euler = h->d.physics == DGLM_EULER;
+  // the sized part, reallocated for this recording
+  cudaStreamSynchronize(h->stream);
+  for (void *p : t->sized) cudaFree(p);
+  t->sized.clear();
+  t->bytes -= t->sized_bytes;
+  t->sized_bytes = 0;
+  t->cap_ckpt = t->cap_steps = t->cap_store = 0;
+  auto chk = [&](dglm_status x) {
+    if (st == DGLM_OK) st = x;
+  };
+  chk(talloc(t, t->sized, &t->ckpt, (size_t)slots * t->state));
+  chk(talloc(t, t->sized, &t->store, (size_t)5 * L * t->state));
+  chk(talloc(t, t->sized, &t->dt_dev, (size_t)nsteps));
+  chk(talloc(t, t->sized, &t->tau, (size_t)(euler ? L : 1) * 4 * h->Kp));
+  chk(talloc(t, t->sized, &t->maxv_tmp, (size_t)4 * h->Kp));
+  chk(talloc(t, t->sized, &t->tau_tmp, (size_t)4 * h->Kp));
+  chk(talloc(t, t->sized, &t->sc_tmp, 1));
+  if (st != DGLM_OK) {
+    for (void *p : t->sized) cudaFree(p);
+    t->sized.clear();
+    t->bytes -= t->sized_bytes;
+    t->sized_bytes = 0;
+    return st;
+  }
+  cudaStream_t s = h->stream;
+  // zero-filled so the padded tail elements of every stored state stay zero
+  cudaError_t e = cudaMemsetAsync(t->ckpt, 0, sbytes * slots, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->store, 0, sbytes * 5 * L, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(t->tau, 0, sizeof(double) * (euler ? L : 1) * 4 * h->Kp, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->tau_tmp, 0, sizeof(double) * 4 * h->Kp, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->sc_tmp, 0, sizeof(DevScalars), s);
+  // advection: the penalty is fixed at set-state time
+  if (e == cudaSuccess && !euler)
+    e = cudaMemcpyAsync(t->tau, h->tau, sizeof(double) * 4 * h->Kp, cudaMemcpyDeviceToDevice, s);
+  const double zero = 0.0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&h->sc->dt_fixed, &zero, sizeof(double), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record_capped");
+  revolve_spine(plan, nchunk, slots - 1, t->spine);
+  h->launches = 0;
+  size_t q = 0;
+  for (int i = 0; i < nsteps; i++) {
+    if (q < t->spine.size() && i == t->spine[q] * L) {
+      e = cudaMemcpyAsync(t->ckpt + q * t->state, h->u[h->cur], sbytes,
+                          cudaMemcpyDeviceToDevice, s);
+      q++;
+      if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record_capped");
+    }
+    st = run_steps(h, 1);
+    if (st != DGLM_OK) return st;
+    e = cudaMemcpyAsync(t->dt_dev + i, &h->sc->dt, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record_capped");
+  }
+  t->dt.assign(nsteps, 0.0);
+  e = cudaMemcpyAsync(t->dt.data(), t->dt_dev, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_check(e, "dglm_adjoint_record_capped");
+  for (double d : t->dt)
+    if (!std::isfinite(d) || d < 0)
+      return set_error(DGLM_ERR_NONFINITE, "dglm_adjoint_record_capped: non-finite dt recorded");
+  t->nsteps = nsteps;
+  t->every = 0;
+  t->nseg = 0;
+  t->last_seg_stored = false;
+  t->leaf = L;
+  t->slots = slots;
+  t->nchunk = nchunk;
+  t->plan_f = plan.f;
+  t->plan_split = plan.split;
+  std::vector<RevAction> acts;
+  revolve_actions(plan, 0, nchunk, 0, slots - 1, true, acts);
+  t->advance_steps = revolve_advance_steps(acts, L, nsteps);
+  t->capped = true;
+  t->spine_valid = true;
+  t->recorded = true;
+  return DGLM_OK;
+}
+
+dglm_status dglm_adjoint_tape_plan(dglm_handle *h, int *leaf, int *slots,
+                                   long long *advance_steps) {
+  if (!h || !leaf || !slots || !advance_steps)
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_tape_plan: NULL argument");
+  if (!h->tape || !h->tape->recorded)
+    return set_error(DGLM_ERR_STATE, "dglm_adjoint_tape_plan: record a forward run first");
+  const AdjointTape *t = h->tape;
+  *leaf = t->capped ? t->leaf : t->every;
+  *slots = t->capped ? t->slots : t->nseg;
+  *advance_steps = t->capped ? t->advance_steps : 0;
+  return DGLM_OK;
+}
+
+dglm_status dglm_adjoint_schedule(int nsteps, int leaf, int slots, int prestored, int *spine,
+                                  int max_spine, int *n_spine, int *actions, int max_actions,
+                                  int *n_actions, long long *advance_steps) {
+  if (!n_spine || !n_actions || !advance_steps || (max_spine > 0 && !spine) ||
+      (max_actions > 0 && !actions))
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_schedule: NULL argument");
+  if (nsteps <= 0 || leaf <= 0 || slots <= 0)
+    return set_error(DGLM_ERR_INVALID,
+                     "dglm_adjoint_schedule: nsteps, leaf and slots must be positive");
+  const int n = (nsteps + leaf - 1) / leaf;
+  if (n > 4 * kMaxChunks)
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_schedule: more than " +
+                                           std::to_string(4 * kMaxChunks) + " chunks");
+  const int free = std::min(slots - 1, n - 1);
+  RevolvePlan plan;
+  plan_revolve(plan, n, free);
+  std::vector<int> sp;
+  revolve_spine(plan, n, free, sp);
+  std::vector<RevAction> acts;
+  revolve_actions(plan, 0, n, 0, free, prestored != 0, acts);
+  *n_spine = (int)sp.size();
+  *n_actions = (int)acts.size();
+  *advance_steps = revolve_advance_steps(acts, leaf, nsteps);
+  if ((int)sp.size() > max_spine || (int)acts.size() > max_actions)
+    return set_error(DGLM_ERR_INVALID, "dglm_adjoint_schedule: output arrays too short");
+  for (size_t q = 0; q < sp.size(); q++) spine[q] = sp[q];
+  for (size_t x = 0; x < acts.size(); x++) {
+    int *r = actions + 5 * x;
+    r[0] = acts[x].kind;
+    r[1] = acts[x].src;
+    r[2] = acts[x].chunk;
+    r[3] = acts[x].count;
+    r[4] = acts[x].dst;
+  }
   return DGLM_OK;
 }
 

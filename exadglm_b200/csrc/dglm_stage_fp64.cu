@@ -58,6 +58,26 @@ __device__ __forceinline__ void euler_flux_fast(double g, const double q[5], dou
   W[0] = q[3]; W[1] = q[1] * vz; W[2] = q[2] * vz; W[3] = q[3] * vz + p; W[4] = H * vz;
 }
 
+// Centring of split-precision operands: subtracts the flux of the element's
+// node-0 state (q0[v] = u0[v * vstride]) from a node's flux.  A flux that is
+// constant over an element has zero DG right-hand side (the weak volume term
+// equals the surface term on straight-sided tetrahedra), so the contraction
+// of centred fluxes is the right-hand side, and the split parts carry only
+// the within-element variation (smaller, and with it their rounding).
+__device__ __forceinline__ void centre_node0(double g, const double *u0, int vstride,
+                                             double F[5], double G[5], double W[5]) {
+  double q0[5], F0[5], G0[5], W0[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) q0[v] = u0[v * vstride];
+  euler_flux_fast(g, q0, F0, G0, W0);
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    F[v] -= F0[v];
+    G[v] -= G0[v];
+    W[v] -= W0[v];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // configuration
 // ---------------------------------------------------------------------------
@@ -177,7 +197,8 @@ __device__ __forceinline__ void contract_dmma(const double *__restrict__ Afrag, 
 // pre-split on the host into fragments [kstep][mtile][part][lane] (4 x 32
 // bits per lane, one coalesced 512-byte load); B = the FP64 fluxes in
 // shared memory, split in registers; NPROD16 part products per k-step into
-// FP32 accumulators that are folded into FP64 every SL16 k-steps.
+// FP32 accumulators that are folded into FP64 every SL16 k-steps.  Euler
+// fluxes are centred (centre_node0) before they are stored for the split.
 //   m16n8k8 TF32:  a0=A[g][t] a1=A[g+8][t] a2=A[g][t+4] a3=A[g+8][t+4],
 //                  b0=B[t][g] b1=B[t+4][g]
 //   m16n8k16 BF16: a0=A[g][2t..2t+1] a1=A[g+8][2t..] a2=A[g][2t+8..] a3=A[g+8][2t+8..],
@@ -381,6 +402,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 #pragma unroll
       for (int v = 0; v < 5; v++) q[v] = sU[(v * Np + i) * EP + e];
       euler_flux_fast(a.gamma, q, F, Gf, W);
+      if constexpr (M16) centre_node0(a.gamma, sU + e, Np * EP, F, Gf, W);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const int col = v * E + e;
@@ -456,6 +478,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
         qb[v] = 0.5 * (qm[v] + __ldg(a.u_in + v * vs + idxP));
       }
       euler_flux_fast(a.gamma, qb, F, Gf, W);
+      if constexpr (M16) centre_node0(a.gamma, sU + e, Np * EP, F, Gf, W);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];

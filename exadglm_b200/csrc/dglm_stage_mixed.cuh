@@ -12,6 +12,9 @@
 // the product is taken in three passes, hi*hi + hi*lo + lo*hi, accumulating
 // in FP32.  Fluxes, the LSERK state and update, metrics and face data stay
 // FP64; only the contraction operands and its accumulator are reduced.
+// Euler fluxes are centred before the split (centre_node0: the element's
+// node-0 flux subtracted, which leaves the right-hand side unchanged), so
+// the split parts carry only the within-element variation.
 //
 // Per tile: flux phase writes the volume operand -> one thread issues the
 // volume MMAs and commits to an mbarrier -> once they have read the operand
@@ -353,6 +356,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
 #pragma unroll
         for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
         euler_flux_fast(a.gamma, q, F, Gf, W);
+        centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const int m = v * E + e;
@@ -401,6 +405,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
           qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
         }
         euler_flux_fast(a.gamma, qb, F, Gf, W);
+        centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];

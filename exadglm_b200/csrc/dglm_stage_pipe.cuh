@@ -410,6 +410,7 @@ __global__ void __launch_bounds__(
 #pragma unroll
         for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
         euler_flux_fast(a.gamma, q, F, Gf, W);
+        if constexpr (C::M16) centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const int col = v * E + e, r0 = i, r1 = Np + i, r2 = 2 * Np + i;
@@ -451,6 +452,7 @@ __global__ void __launch_bounds__(
           qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
         }
         euler_flux_fast(a.gamma, qb, F, Gf, W);
+        if constexpr (C::M16) centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];

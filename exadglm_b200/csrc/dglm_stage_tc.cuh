@@ -12,20 +12,23 @@
 //   B = the tile's fluxes in shared memory, split x = hi + lo; row
 //       n = p NCOL + v E + e holds part p of (variable v, element e), so one
 //       MMA per k-step multiplies both parts (rows past 2 NCOL stay zero);
+//       two image sets, so that the fluxes of tile t+1 are written while the
+//       MMAs of tile t read theirs;
 //   D = FP32 accumulators in tensor memory, double-buffered across tiles:
 //       column n of lane (i, p') holds A_p' . B_p of column n mod NCOL.
 // The right-hand side of (v, e) at node i is the sum of the four part
 // products D[(i,0)][c] + D[(i,0)][NCOL + c] + D[(i,1)][c] + D[(i,1)][NCOL + c].
 //
 // Centring.  Before the split every flux value of an element has that
-// element's flux at node 0 subtracted: fluxR/S/T - metric . F(u_0) and
-// fluxLM - Fscale_f n_f . F(u_0).  A constant flux has zero DG right-hand
-// side (the weak volume term equals the surface term for constant data on
-// straight-sided tetrahedra, to FP64 rounding), so the contraction of the
-// centred fluxes IS the right-hand side, while the values that reach the
-// tensor cores are the within-element variations: an order of magnitude
-// smaller than the fluxes for resolved solutions, and with them the TF32
-// representation and FP32 accumulation errors.
+// element's flux at node 0 subtracted: fluxR/S/T = metric . (F(u_i) - F(u_0))
+// and fluxLM = Fscale_f (n_f . (F(u*) - F(u_0)) - tau (u* - u-)).  A constant
+// flux has zero DG right-hand side (the weak volume term equals the surface
+// term for constant data on straight-sided tetrahedra, to FP64 rounding), so
+// the contraction of the centred fluxes IS the right-hand side, while the
+// values that reach the tensor cores are the within-element variations: an
+// order of magnitude smaller than the fluxes for resolved solutions, and with
+// them the TF32 representation and FP32 accumulation errors.  Each flux lane
+// evaluates F(u_0) of its own element beside its node's flux.
 //
 // K order.  Volume columns are node-group major, k = (i/4)*12 + d*4 + i%4
 // (d = r, s, t); face columns follow at KVA + f NFPP + j.  A warp task covers
@@ -33,23 +36,23 @@
 // 8-row x 16-byte core matrix.
 //
 // Warps: NC compute warps, one producer warp, one MMA warp.
-//   producer    per tile, into a ring of NB buffers: bulk copies of u, the RK
-//               register k, metrics and face data (one copy per lane),
-//               cp.async gathers of the neighbour traces u[vmapP]; before
-//               each refill, the node-0 fluxes of the previous tile.
-//   MMA         lane 0: once the compute warps have written the operand
-//               images of tile t (flux_done) and the accumulator D[t%2] is
-//               free (d_free), the volume and face MMAs, committed to
-//               mma_done.
-//   compute     per tile t: volume and face flux tasks of t, after MMA(t-1)
-//               has read the images; then the
-//               epilogue of t-1: warps 0..3 read D[(t-1)%2] (one lane quarter
-//               each), add the parts into the rhs staging, and all compute
-//               warps do the LSERK update from the staged u and k with
+//   producer    per tile, into a ring of NB buffers: bulk copies of u,
+//               metrics and face data (one copy per lane), an L2 prefetch of
+//               the tile's RK register rows, cp.async gathers of the
+//               neighbour traces u[vmapP].
+//   MMA         lane 0: once the compute warps have written operand image
+//               set t%2 (flux_done[t%2]) and accumulator D[t%2] is free
+//               (d_free[t%2]), the volume and face MMAs of tile t, committed
+//               to mma_done[t%2].
+//   compute     per tile t: volume and face flux tasks of t into image set
+//               t%2, then the epilogue of t-1: loads of t-1's RK register
+//               values, the wait for MMA(t-1); warps 0..3 read D[(t-1)%2]
+//               (one lane quarter each) and add the parts into the rhs
+//               staging; all compute warps do the LSERK update with
 //               coalesced stores.
-// The tensor cores work on tile t while the compute warps finish t-1.
-// Every wait is bounded; on expiry a warp sets flag bit 2, waits (with the
-// default bound) for the MMAs and copies it issued, and leaves.
+// The tensor cores work on tile t while the compute warps finish t-1 and
+// start t+1.  Every wait is bounded; on expiry a warp sets flag bit 2, waits
+// (with the default bound) for the MMAs and copies it issued, and leaves.
 #pragma once
 
 template <int PHYS, int N, int E_, int NC_, int NB_>
@@ -67,23 +70,19 @@ struct TCfg {
   static constexpr int KT = KVA + KFA, KSV = KVA / 8, KSF = KFA / 8;
   static constexpr int SBO_V = KVA / 4 * 128, SBO_F = KFA / 4 * 128;
   static constexpr int BV_BYTES = MN / 8 * SBO_V, BF_BYTES = MN / 8 * SBO_F;
+  static constexpr int B_BYTES = BV_BYTES + BF_BYTES;    // one operand image set
   // tensor memory: D0, D1, then the operator
   static constexpr int D_COLS = MN, A_COL = 2 * MN;
   static constexpr int TMEM_COLS = 512;
-  // tile ring buffer (doubles): u [v][e][i], k [v][e][i], neighbour traces
-  // [v][e][UPS], metrics [9][e], face data [nx ny nz fs tau][e][f]
+  // tile ring buffer (doubles): u [v][e][i], neighbour traces [v][e][UPS],
+  // metrics [9][e], face data [nx ny nz fs tau][e][f]
   static constexpr int UPS = NFF % 8 == 4 ? NFF : NFF + 4;
-  static constexpr int S_U = NV * E * Np, S_K = NV * E * Np, S_UP = NV * E * UPS;
+  static constexpr int S_U = NV * E * Np, S_UP = NV * E * UPS;
   static constexpr int S_GEO = 9 * E, S_FACE = 20 * E;
-  static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE;
-  static constexpr unsigned TX = 8u * (S_U + S_K + S_GEO + S_FACE);
-  static constexpr int NCOPY = 2 * NV + 9 + 5;           // bulk copies per tile
-  // node-0 flux terms per element: 3 volume directions + 4 faces, per
-  // variable; three slots (the producer writes tile t+1's, or t+2's, while
-  // the compute warps read tile t's)
-  static constexpr int NCEN = 7, NCS = 3;
-  static constexpr int S_C = E * NV * NCEN;
-  // rhs staging [v][e][i] for the update
+  static constexpr int S_BUF = S_U + S_UP + S_GEO + S_FACE;
+  static constexpr unsigned TX = 8u * (S_U + S_GEO + S_FACE);
+  static constexpr int NCOPY = NV + 9 + 5 + NV;          // bulk copies + k prefetches per tile
+  // rhs staging [v][e][i] (FP32: the sum of the four part products)
   static constexpr int S_R = NV * E * Np;
   // warp tasks per tile: volume (8 elements x one node group of 4), face
   // (8 elements x 4 nodes of one face)
@@ -92,15 +91,14 @@ struct TCfg {
   static constexpr int NTASK = VOL_WT + FACE_WT;
   static constexpr int PROD_WARP = NC, MMA_WARP = NC + 1, NWARPS = NC + 2;
   static constexpr int THREADS = 32 * NWARPS, TC = 32 * NC;
+  static constexpr int KPT = (NV * E * Np + TC - 1) / TC;   // update values per compute thread
   static constexpr int GPL = (E * NFF + 31) / 32;        // gathers per producer lane
-  static constexpr size_t OFF_BV = 0, OFF_BF = BV_BYTES;
-  static constexpr size_t OFF_RING = OFF_BF + (size_t)BF_BYTES;
-  static constexpr size_t OFF_C = OFF_RING + 8 * (size_t)NB * S_BUF;
-  static constexpr size_t OFF_R = OFF_C + 8 * NCS * (size_t)S_C;
-  static constexpr size_t OFF_BAR = OFF_R + 8 * (size_t)S_R;
-  // barriers: full[NB], empty[NB], cen[NCS], flux_done, mma_done, d_free[2];
+  static constexpr size_t OFF_RING = 2 * (size_t)B_BYTES;
+  static constexpr size_t OFF_R = OFF_RING + 8 * (size_t)NB * S_BUF;
+  static constexpr size_t OFF_BAR = OFF_R + (4 * (size_t)S_R + 15) / 16 * 16;
+  // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2];
   // then the tensor-memory address, Fmask, maxima
-  static constexpr int NBARS = 2 * NB + NCS + 4;
+  static constexpr int NBARS = 2 * NB + 6;
   static constexpr size_t SMEM = OFF_BAR + 8 * (NBARS + 1) + 4 * NFF + 8 * 32 + 64;
   // instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N, M = 128
   static constexpr unsigned IDESC =
@@ -110,13 +108,10 @@ struct TCfg {
   static_assert(2 * NPQ <= 32, "both operator parts of a quarter's nodes fit its 32 lanes");
   static_assert(2 * D_COLS + KT <= TMEM_COLS, "accumulators and operator fit tensor memory");
   static_assert(NC >= 4, "compute warps 0..3 cover the four tensor-memory lane quarters");
-  static_assert(E <= 32, "one lane per element computes the node-0 fluxes");
   static_assert(NCOPY <= 32, "one producer lane per bulk copy");
   static_assert(NCOL <= 64 && NCOL % 2 == 0,
                 "an epilogue lane holds both parts of its row's columns, split in halves");
-  // NB >= 3: the node-0 fluxes of tile t+1 are computed during tile t, while
-  // the slot of tile t-1 may still be held by its epilogue
-  static_assert(NB >= 3 && NB <= 4, "ring of 3..4 tile buffers");
+  static_assert(NB >= 2 && NB <= 4, "ring of 2..4 tile buffers");
   static_assert((E * Np * 8) % 16 == 0, "16-byte bulk copies");
   static_assert(THREADS <= 1024 && NWARPS <= 32, "block size");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
@@ -158,6 +153,10 @@ __device__ __forceinline__ void split_tf32_pair(double x, unsigned &hi, unsigned
   hi = __float_as_uint(f) & 0xffffe000u;
   lo = __float_as_uint(f - __uint_as_float(hi));
 }
+// bulk prefetch of [src, src + bytes) into L2 (16-byte aligned, multiple of 16)
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 
 template <int PHYS, int N, int E_, int NC_, int NB_>
 __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
@@ -166,15 +165,11 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, NB = C::NB,
                 NC = C::NC, TC = C::TC, NCOL = C::NCOL;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  unsigned char *sBv = smem_raw + C::OFF_BV;
-  unsigned char *sBf = smem_raw + C::OFF_BF;
   double *sRing = reinterpret_cast<double *>(smem_raw + C::OFF_RING);
-  double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
-  double *sR = reinterpret_cast<double *>(smem_raw + C::OFF_R);
+  float *sR = reinterpret_cast<float *>(smem_raw + C::OFF_R);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
-  unsigned long long *full = bars, *empty = bars + NB, *cen = bars + 2 * NB,
-                     *flux_done = cen + C::NCS, *mma_done = flux_done + 1,
-                     *d_free = flux_done + 2;
+  unsigned long long *full = bars, *empty = bars + NB, *flux_done = bars + 2 * NB,
+                     *mma_done = flux_done + 2, *d_free = flux_done + 4;
   unsigned *sTmem = reinterpret_cast<unsigned *>(bars + C::NBARS);
   int *sFm = reinterpret_cast<int *>(bars + C::NBARS + 1);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
@@ -191,10 +186,11 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       mbar_init(&full[b], 1 + 32);   // the byte-count arrive + each producer lane's gathers
       mbar_init(&empty[b], NC);
     }
-    for (int c = 0; c < C::NCS; c++) mbar_init(&cen[c], 1);
-    mbar_init(flux_done, NC);
-    mbar_init(mma_done, 1);
-    for (int b = 0; b < 2; b++) mbar_init(&d_free[b], 4);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&flux_done[b], NC);
+      mbar_init(&mma_done[b], 1);
+      mbar_init(&d_free[b], 4);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NFF; i += C::THREADS) sFm[i] = a.Fmask[i];
@@ -232,57 +228,21 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
   unsigned long long vmax = 0ull;
   bool ok = true;
 
-  // node-0 fluxes of ring iteration `it` (lane e < E of the producer warp):
-  // the volume terms metric_d . F(u_0) and the face terms Fscale_f n_f .
-  // F(u_0), into centre slot it % NCS
-  auto centers = [&](int it) {
-    const int e = lane;
-    if (e >= E) return;
-    const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
-    const double *bU = ring(it), *bG = bU + C::S_U + C::S_K + C::S_UP, *bF = bG + C::S_GEO;
-    double *c = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN;
-    if (e < ne) {
-      double q[5], F[5], G[5], W[5];
-#pragma unroll
-      for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
-      euler_flux_fast(gam, q, F, G, W);
-      double m[9];
-#pragma unroll
-      for (int i = 0; i < 9; i++) m[i] = bG[i * E + e];
-      double nf[4][4];
-#pragma unroll
-      for (int f = 0; f < 4; f++)
-#pragma unroll
-        for (int x = 0; x < 4; x++) nf[f][x] = bF[x * 4 * E + e * 4 + f];
-#pragma unroll
-      for (int v = 0; v < 5; v++) {
-#pragma unroll
-        for (int d = 0; d < 3; d++)
-          c[v * C::NCEN + d] = m[3 * d] * F[v] + m[3 * d + 1] * G[v] + m[3 * d + 2] * W[v];
-#pragma unroll
-        for (int f = 0; f < 4; f++)
-          c[v * C::NCEN + 3 + f] =
-              (nf[f][0] * F[v] + nf[f][1] * G[v] + nf[f][2] * W[v]) * nf[f][3];
-      }
-    } else {
-#pragma unroll
-      for (int x = 0; x < NV * C::NCEN; x++) c[x] = 0.0;
-    }
-  };
-
   if (warp < NC) {
     // ------------------------------------------------------- compute warps
     // volume fluxes of ring iteration `it`, task wt: 8 elements x nodes
-    // 4g .. 4g+3, centred and split into the operand image
-    auto vol_task = [&](int it, int wt, int ne) {
+    // 4g .. 4g+3, centred and split into operand image sBv
+    auto vol_task = [&](int it, int wt, int ne, unsigned char *sBv) {
       const int eb = wt / C::NG, g = wt - eb * C::NG;
       const int e = eb * 8 + (lane & 7), i = 4 * g + (lane >> 3);
       const bool okn = e < ne && i < Np;
-      const double *bU = ring(it), *bG = bU + C::S_U + C::S_K + C::S_UP;
+      const double *bU = ring(it), *bG = bU + C::S_U + C::S_UP;
       unsigned hv[5][3], lv[5][3];
       if (okn) {
-        const double *cn = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN;
-        double q[5], F[5], G[5], W[5];
+        double q[5], F[5], G[5], W[5], F0[5], G0[5], W0[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
+        euler_flux_fast(gam, q, F0, G0, W0);
 #pragma unroll
         for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
         euler_flux_fast(gam, q, F, G, W);
@@ -290,14 +250,13 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
 #pragma unroll
         for (int x = 0; x < 9; x++) m[x] = bG[x * E + e];
 #pragma unroll
-        for (int v = 0; v < 5; v++)
+        for (int v = 0; v < 5; v++) {
+          const double dF = F[v] - F0[v], dG = G[v] - G0[v], dW = W[v] - W0[v];
 #pragma unroll
           for (int d = 0; d < 3; d++)
-            // the node-0 term enters the first FMA of the metric combination
-            split_tf32_pair(fma(m[3 * d + 2], W[v],
-                                fma(m[3 * d + 1], G[v], fma(m[3 * d], F[v],
-                                                            -cn[v * C::NCEN + d]))),
+            split_tf32_pair(fma(m[3 * d + 2], dW, fma(m[3 * d + 1], dG, m[3 * d] * dF)),
                             hv[v][d], lv[v][d]);
+        }
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++)
@@ -316,12 +275,12 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
     };
 
     // face fluxes of ring iteration `it`, task wt: each lane one face node
-    // of 8 elements x 4 nodes of one face, neighbour traces staged
-    auto face_task = [&](int it, int wt, int ne) {
+    // of 8 elements x 4 nodes of one face, neighbour traces staged; image sBf
+    auto face_task = [&](int it, int wt, int ne, unsigned char *sBf) {
       const int eb = wt / (4 * C::NJB), f = (wt / C::NJB) & 3, jb = wt % C::NJB;
       const int e = eb * 8 + (lane & 7), j = jb * 4 + (lane >> 3);
       const bool okn = e < ne && j < Nfp;
-      const double *bU = ring(it), *bUP = bU + C::S_U + C::S_K;
+      const double *bU = ring(it), *bUP = bU + C::S_U;
       const double *bF = bUP + C::S_UP + C::S_GEO;
       unsigned hv[5], lv[5];
       if (okn) {
@@ -329,8 +288,10 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         const double nx = bF[0 * 4 * E + e * 4 + f], ny = bF[1 * 4 * E + e * 4 + f],
                      nz = bF[2 * 4 * E + e * 4 + f], fs = bF[3 * 4 * E + e * 4 + f],
                      tau = bF[4 * 4 * E + e * 4 + f];
-        const double *cn = sC0 + (it % C::NCS) * C::S_C + e * NV * C::NCEN + 3 + f;
-        double qm[5], qb[5], F[5], G[5], W[5];
+        double q0[5], qm[5], qb[5], F[5], G[5], W[5], F0[5], G0[5], W0[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q0[v] = bU[v * E * Np + e * Np];
+        euler_flux_fast(gam, q0, F0, G0, W0);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           qm[v] = bU[v * E * Np + e * Np + nodeM];
@@ -339,8 +300,8 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         euler_flux_fast(gam, qb, F, G, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          const double nd = fma(nz, W[v], fma(ny, G[v], nx * F[v]));
-          split_tf32_pair(fma(nd - tau * (qb[v] - qm[v]), fs, -cn[v * C::NCEN]), hv[v], lv[v]);
+          const double nd = fma(nz, W[v] - W0[v], fma(ny, G[v] - G0[v], nx * (F[v] - F0[v])));
+          split_tf32_pair((nd - tau * (qb[v] - qm[v])) * fs, hv[v], lv[v]);
         }
       } else {
 #pragma unroll
@@ -356,15 +317,30 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       }
     };
 
-    // epilogue of ring iteration `it` from accumulator buffer it % 2
-    auto epilogue = [&](int it) {
+    // epilogue of ring iteration `it` from accumulator buffer it % 2; false
+    // when the wait for its MMAs expired (on every compute warp alike)
+    auto epilogue = [&](int it) -> bool {
       const int db = it & 1;
       const long e0 = tile_e0(it);
       const int ne = (int)min((long)E, (long)a.K - e0);
+      const int nep = ne * Np;
       double *bU = ring(it);
-      const double *bK = bU + C::S_U;
-      // every compute warp is done with the staging of the previous update
-      consumer_sync(TC);
+      // this thread's RK register values (prefetched into L2 with the tile),
+      // loaded while the MMAs finish
+      double kr[C::KPT];
+#pragma unroll
+      for (int r = 0; r < C::KPT; r++) {
+        const int x = tid + r * TC;
+        kr[r] = 0.0;
+        if (!a.rhs_only && x < NV * nep) {
+          const int v = x / nep, g = x - v * nep;
+          kr[r] = a.kreg[v * vs + e0 * Np + g];
+        }
+      }
+      // MMA(it) done; every compute warp is done with the staging of the
+      // previous update
+      if (!consumer_all(mbar_wait(&mma_done[db], (it >> 1) & 1, lim), TC)) return false;
+      tc_fence_after();
       if (warp < 4) {
         // lane 2j + p of quarter q holds row (node NPQ q + j, operator part p)
         const int q = warp, p = lane & 1, j = lane >> 1, node = C::NPQ * q + j;
@@ -384,26 +360,29 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         for (int c = 0; c < H; c++) {
           const float lo_half = r[c] + r[NCOL + c], hi_half = r[H + c] + r[NCOL + H + c];
           const float other = __shfl_xor_sync(0xffffffffu, p ? lo_half : hi_half, 1);
-          if (on) sR[(p * H + c) * Np + node] = (double)((p ? hi_half : lo_half) + other);
+          if (on) sR[(p * H + c) * Np + node] = (p ? hi_half : lo_half) + other;
         }
       }
       consumer_sync(TC);
-      // LSERK update, one flat loop over (variable, element, node): staged
-      // rhs, u and k, coalesced stores
-      const int nep = ne * Np;
-      for (int x = tid; x < NV * nep; x += TC) {
-        const int v = x / nep, g = x - v * nep;
-        const int si = v * E * Np + g;
-        const long gi = v * vs + e0 * Np + g;
-        const double rhs = sR[si];
-        if (a.rhs_only) {
-          a.u_out[gi] = rhs;
-        } else {
-          const double kn = a.rka * bK[si] + dt * rhs;
-          const double un = bU[si] + a.rkb * kn;
-          a.kreg[gi] = kn;
-          a.u_out[gi] = un;
-          if (keep_u) bU[si] = un;
+      // LSERK update over (variable, element, node): staged rhs, u and the
+      // RK register values, coalesced stores
+#pragma unroll
+      for (int r = 0; r < C::KPT; r++) {
+        const int x = tid + r * TC;
+        if (x < NV * nep) {
+          const int v = x / nep, g = x - v * nep;
+          const int si = v * E * Np + g;
+          const long gi = v * vs + e0 * Np + g;
+          const double rhs = (double)sR[si];
+          if (a.rhs_only) {
+            a.u_out[gi] = rhs;
+          } else {
+            const double kn = a.rka * kr[r] + dt * rhs;
+            const double un = bU[si] + a.rkb * kn;
+            a.kreg[gi] = kn;
+            a.u_out[gi] = un;
+            if (keep_u) bU[si] = un;
+          }
         }
       }
       if (keep_u) {
@@ -411,7 +390,7 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         // its nodes (divisions as in face_maxv_kernel, so dt does not depend
         // on which kernel computed maxv)
         consumer_sync(TC);
-        const double *bF = bU + C::S_U + C::S_K + C::S_UP + C::S_GEO;
+        const double *bF = bU + C::S_U + C::S_UP + C::S_GEO;
         for (int x = tid; x < 4 * E; x += TC) {
           const int f = x / E, e = x - f * E;
           if (e >= ne) continue;
@@ -441,82 +420,63 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[it % NB]);
+      return true;
     };
 
     for (int it = 0; ok && it < my_tiles; it++) {
       const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
-      // tile data, its node-0 fluxes, and MMA(t-1) done with the operand images
-      bool w = mbar_wait(&full[it % NB], (it / NB) & 1, lim) &&
-               mbar_wait(&cen[it % C::NCS], (it / C::NCS) & 1, lim);
-      if (it > 0) w = w && mbar_wait(mma_done, (it - 1) & 1, lim);
-      if (!consumer_all(w, TC)) {
+      // the tile's data; image set it % 2 was last read by MMA(it - 2),
+      // whose completion every compute warp saw in epilogue(it - 2)
+      if (!consumer_all(mbar_wait(&full[it % NB], (it / NB) & 1, lim), TC)) {
         ok = false;
         break;
       }
-      tc_fence_after();
+      unsigned char *sBv = smem_raw + (it & 1) * C::B_BYTES, *sBf = sBv + C::BV_BYTES;
       for (int wt = warp; wt < C::NTASK; wt += NC) {
         if (wt < C::VOL_WT)
-          vol_task(it, wt, ne);
+          vol_task(it, wt, ne, sBv);
         else
-          face_task(it, wt - C::VOL_WT, ne);
+          face_task(it, wt - C::VOL_WT, ne, sBf);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(flux_done);
-      if (it > 0) epilogue(it - 1);
-    }
-    if (ok && my_tiles > 0) {
-      ok = consumer_all(mbar_wait(mma_done, (my_tiles - 1) & 1, lim), TC);
-      if (ok) {
-        tc_fence_after();
-        epilogue(my_tiles - 1);
-      }
-    }
-  } else if (warp == C::PROD_WARP) {
-    // ------------------------------------------------------ producer warp
-    // per ring iteration: the node-0 fluxes of the previous tile (landed by
-    // now: they run ahead of the compute warps), then the copies of this one
-    auto centers_of = [&](int t) -> bool {
-      if (!mbar_wait(&full[t % NB], (t / NB) & 1, lim)) return false;
-      centers(t);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&cen[t % C::NCS]);
-      return true;
-    };
-    int it = 0;
-    for (; it < my_tiles; it++) {
-      const int b = it % NB;
-      if (it > 0 && !centers_of(it - 1)) {
+      if (lane == 0) mbar_arrive(&flux_done[it & 1]);
+      if (it > 0 && !epilogue(it - 1)) {
         ok = false;
         break;
       }
+    }
+    if (ok && my_tiles > 0 && !epilogue(my_tiles - 1)) ok = false;
+  } else if (warp == C::PROD_WARP) {
+    // ------------------------------------------------------ producer warp
+    int it = 0;
+    for (; it < my_tiles; it++) {
+      const int b = it % NB;
       if (it >= NB && !mbar_wait(&empty[b], ((it / NB) - 1) & 1, lim)) {
         ok = false;
         break;
       }
       const long e0 = tile_e0(it);
       const int ne = (int)min((long)E, (long)a.K - e0);
-      double *bU = ring(it), *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
-      double *bF = bG + C::S_GEO;
+      double *bU = ring(it), *bUP = bU + C::S_U, *bG = bUP + C::S_UP, *bF = bG + C::S_GEO;
       // bulk copies, one per lane, after lane 0 has posted the byte count
       if (lane == 0) mbar_arrive_expect_tx(&full[b], C::TX);
       __syncwarp();
       const int x = lane;
       if (x < NV) {
         bulk_g2s(bU + x * E * Np, a.u_in + x * vs + e0 * Np, 8u * E * Np, &full[b]);
-      } else if (x < 2 * NV) {
-        const int v = x - NV;
-        bulk_g2s(bK + v * E * Np, a.kreg + v * vs + e0 * Np, 8u * E * Np, &full[b]);
-      } else if (x < 2 * NV + 9) {
-        const int m = x - 2 * NV;
+      } else if (x < NV + 9) {
+        const int m = x - NV;
         bulk_g2s(bG + m * E, a.geo + m * a.gstride + e0, 8u * E, &full[b]);
-      } else if (x < 2 * NV + 12) {
-        const int q = x - 2 * NV - 9;
+      } else if (x < NV + 12) {
+        const int q = x - NV - 9;
         bulk_g2s(bF + q * 4 * E, a.nrm + q * 4 * a.gstride + 4 * e0, 32u * E, &full[b]);
-      } else if (x == 2 * NV + 12) {
+      } else if (x == NV + 12) {
         bulk_g2s(bF + 3 * 4 * E, a.fscale + 4 * e0, 32u * E, &full[b]);
-      } else if (x == 2 * NV + 13) {
+      } else if (x == NV + 13) {
         bulk_g2s(bF + 4 * 4 * E, a.tau + 4 * e0, 32u * E, &full[b]);
+      } else if (x < NV + 14 + NV && !a.rhs_only) {
+        bulk_prefetch_l2(a.kreg + (x - NV - 14) * vs + e0 * Np, 8u * E * Np);
       }
       // neighbour traces u+ = u[vmapP] into [v][e][UPS]: this lane's vmapP
       // entries are loaded before its gathers are issued
@@ -538,25 +498,24 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       }
       cp_async_arrive_noinc(&full[b]);
     }
-    if (ok && it > 0 && !centers_of(it - 1)) ok = false;
     // the copies of the last NB tiles land before this warp leaves
     for (int j = (it > NB ? it - NB : 0); j < it; j++) mbar_wait(&full[j % NB], (j / NB) & 1);
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else {
     // ----------------------------------------------------------- MMA warp
     if (lane == 0) {
-      int nm = 0;   // commits issued to mma_done
+      int nm = 0;   // tiles whose MMAs were issued and committed
       for (int it = 0; it < my_tiles; it++) {
-        const int db = it & 1;
-        bool w = mbar_wait(flux_done, it & 1, lim);
-        if (it >= 2) w = w && mbar_wait(&d_free[db], ((it >> 1) - 1) & 1, lim);
+        const int b = it & 1;
+        bool w = mbar_wait(&flux_done[b], (it >> 1) & 1, lim);
+        if (it >= 2) w = w && mbar_wait(&d_free[b], ((it >> 1) - 1) & 1, lim);
         if (!w) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const unsigned d = tmem + db * C::D_COLS;
-        const unsigned bv = smem_u32(sBv), bf = smem_u32(sBf);
+        const unsigned d = tmem + b * C::D_COLS;
+        const unsigned bv = smem_u32(smem_raw + b * C::B_BYTES), bf = bv + C::BV_BYTES;
 #pragma unroll 1
         for (int ks = 0; ks < C::KSV; ks++)
           tc_mma_ts(d, tmem + C::A_COL + ks * 8, smem_desc(bv + ks * 256, 128, C::SBO_V),
@@ -565,12 +524,12 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         for (int ks = 0; ks < C::KSF; ks++)
           tc_mma_ts(d, tmem + C::A_COL + C::KVA + ks * 8,
                     smem_desc(bf + ks * 256, 128, C::SBO_F), C::IDESC, 1);
-        tc_commit(mma_done);
+        tc_commit(&mma_done[b]);
         nm++;
       }
-      // the MMAs issued (and their barrier arrival) are complete before
+      // the MMAs issued (and their barrier arrivals) are complete before
       // tensor and shared memory are released, on expiry too
-      if (nm) mbar_wait(mma_done, (nm - 1) & 1);
+      for (int t = (nm > 2 ? nm - 2 : 0); t < nm; t++) mbar_wait(&mma_done[t & 1], (t >> 1) & 1);
     }
   }
   if (!ok) atomicOr(&a.sc->flags, 4);

@@ -276,6 +276,35 @@ dglm_status dglm_adjoint_replay(dglm_handle *h);
 dglm_status dglm_adjoint_rhs(dglm_handle *h, const double *const *u, const double *const *mu,
                              double *const *out);
 dglm_status dglm_adjoint_tape_bytes(dglm_handle *h, size_t *bytes);
+/* dglm_adjoint_record_capped: as dglm_adjoint_record, with the tape held
+ * under max_bytes of device memory (the whole tape, as dglm_adjoint_tape_bytes
+ * reports it) by binomial checkpointing (revolve, Griewank and Walther 2000):
+ * the run is cut into chunks of `leaf` steps, `slots` state checkpoints are
+ * kept, and the backward pass recomputes each chunk's stage inputs once plus
+ * the fewest forward steps the slots allow.  The recording picks leaf and
+ * slots for the least recomputation under the cap and places the first
+ * checkpoints of the schedule while it runs.  The gradient equals that of a
+ * dglm_adjoint_record recording (tau is recomputed from the recomputed
+ * states, bit for bit as the forward run computed it).  DGLM_ERR_NOMEM when
+ * max_bytes is below the minimum (one checkpoint and one step's stage
+ * inputs); dglm_adjoint_replay is not available for capped recordings.
+ * dglm_adjoint_tape_plan: leaf, slots and the forward steps the next
+ * backward pass recomputes (fixed-interval recordings: checkpoint_every,
+ * segments, 0).
+ * dglm_adjoint_schedule: the schedule itself, for nsteps, leaf and slots
+ * (host only, no device): spine[q] = chunk whose start state slot q holds
+ * after the recording (slot 0: chunk 0); actions as 5 ints each, (0, src,
+ * chunk, count, dst) = advance count chunks from the state of `chunk` in
+ * slot src into slot dst (-1: a scratch state), (1, src, chunk, 1, -1) =
+ * reverse `chunk` from its start state in slot src; prestored: whether the
+ * spine checkpoints are in place (the first backward pass after a
+ * recording). */
+dglm_status dglm_adjoint_record_capped(dglm_handle *h, int nsteps, size_t max_bytes);
+dglm_status dglm_adjoint_tape_plan(dglm_handle *h, int *leaf, int *slots,
+                                   long long *advance_steps);
+dglm_status dglm_adjoint_schedule(int nsteps, int leaf, int slots, int prestored, int *spine,
+                                  int max_spine, int *n_spine, int *actions, int max_actions,
+                                  int *n_actions, long long *advance_steps);
 /* Tile shapes of the adjoint stage kernel for (physics, N); selecting one
  * drops the tape (record again). */
 int dglm_adjoint_variant_count(int physics, int N);
