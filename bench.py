@@ -64,6 +64,10 @@ def parse():
                     help="hexahedra per axis of the adjoint workload (K = 6 n^3)")
     ap.add_argument("--adjoint-steps", type=int, default=500)
     ap.add_argument("--adjoint-every", type=int, default=50, help="checkpoint spacing")
+    ap.add_argument("--adjoint-caps-gib", default="2,8",
+                    help="tape caps (GiB) of the capped (binomial checkpointing) adjoint runs")
+    ap.add_argument("--adjoint-large-cap-gib", type=float, default=16.0,
+                    help="tape cap of the capped adjoint at the headline size (0: skip)")
     ap.add_argument("--batch-count", type=int, default=256, help="instances of the batch workload")
     ap.add_argument("--precision-n", type=int, default=48,
                     help="hexahedra per axis of the N=6 precision study (K = 6 n^3)")
@@ -457,6 +461,60 @@ def adjoint_section(a, stream):
         "grad_norm": float(torch.linalg.norm(grad).item()),
         "tape_bytes": s.adjoint_tape_bytes(),
     }
+    # binomial checkpointing under a cap: same gradient, fewer bytes, the
+    # recomputed forward steps on top of the backward pass
+    g_fixed = grad.clone()
+    capped = []
+    for cap_gib in [float(c) for c in a.adjoint_caps_gib.split(",") if c.strip()]:
+        cap = int(cap_gib * 2**30)
+        s.set_state(pa.u0)
+        rec_c = timed(lambda: s.adjoint_record_capped(T, cap))
+        leaf, slots, adv = s.adjoint_tape_plan()
+        bwd_c = timed(lambda: s.adjoint_backward_device(lp, gp))
+        capped.append({
+            "cap_bytes": cap, "tape_bytes": s.adjoint_tape_bytes(), "leaf_steps": leaf,
+            "slots": slots, "advance_steps": adv, "record_ms_per_step": rec_c / T,
+            "bwd_ms_per_step": bwd_c / T, "ratio_bwd_over_fwd": bwd_c / fwd,
+            "grad_rel_l2_vs_fixed": float(torch.linalg.norm(grad - g_fixed) /
+                                          torch.linalg.norm(g_fixed))})
+    out["capped"] = capped
+    s.close()
+    if a.adjoint_large_cap_gib > 0:
+        out["capped_headline_size"] = adjoint_large(a, stream, timed)
+    return out
+
+
+def adjoint_large(a, stream, timed):
+    """Capped adjoint at the headline size: Euler N=4, K = 6 n^3 (--n), 200
+    steps, J = 1/2 ||rho(T)||^2, tape capped at --adjoint-large-cap-gib."""
+    import torch
+    from exadglm_b200 import problem as P
+    from exadglm_b200.capi import Solver
+    p = P.euler_sine(n=a.n, N=4, cfl=0.4)
+    T, cap = 200, int(a.adjoint_large_cap_gib * 2**30)
+    s = Solver(p)
+    s.set_stream(stream.cuda_stream)
+    s.step(3)
+    s.sync()
+    s.set_state(p.u0)
+    fwd = timed(lambda: s.step(T))
+    s.set_state(p.u0)
+    rec = timed(lambda: s.adjoint_record_capped(T, cap))
+    leaf, slots, adv = s.adjoint_tape_plan()
+    nv, n = p.nvar, p.K * p.Np
+    uT = s.get_state()
+    lam = torch.zeros((nv, n), dtype=torch.float64, device="cuda")
+    lam[0] = torch.from_numpy(uT[0]).cuda()
+    grad = torch.empty_like(lam)
+    torch.cuda.synchronize()
+    bwd = timed(lambda: s.adjoint_backward_device([lam[v].data_ptr() for v in range(nv)],
+                                                  [grad[v].data_ptr() for v in range(nv)]))
+    out = {"workload": f"euler_sine N=4 K={p.K} (n={a.n}) CFL 0.4, J = 1/2||rho(T)||^2, "
+                       f"T = {T} steps", "cap_bytes": cap,
+           "tape_bytes": s.adjoint_tape_bytes(), "leaf_steps": leaf, "slots": slots,
+           "advance_steps": adv, "fwd_ms_per_step": fwd / T, "record_ms_per_step": rec / T,
+           "bwd_ms_per_step": bwd / T, "ratio_bwd_over_fwd": bwd / fwd,
+           "grad_norm": float(torch.linalg.norm(grad).item())}
     s.close()
     return out
 

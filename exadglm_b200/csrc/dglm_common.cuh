@@ -33,6 +33,10 @@ struct DevScalars {
   int flags;                      // bit 0: non-finite dt / wave speed; bit 1: non-finite state
 };
 
+// Doubles per element of the element record: rx ry rz sx sy sz tx ty tz,
+// nx[4], ny[4], nz[4], Fscale[4] (faces 0..3), one pad (16-byte multiple).
+constexpr int kRecord = 26;
+
 // Arguments of the fused stage kernels.  Field arrays are one allocation
 // with `vs` doubles between variables.
 struct StageArgs {
@@ -40,6 +44,7 @@ struct StageArgs {
   const double *geo;     // rx,ry,rz,sx,sy,sz,tx,ty,tz, each K doubles
   const double *fscale;  // K*4
   const double *nrm;     // nx, ny, nz, each K*4
+  const double *erec;    // per-element record [K][kRecord] or null (see kRecord)
   const double *tau;     // K*4
   const int *vmapP;      // K*4*Nfp
   const int *Fmask;      // 4*Nfp

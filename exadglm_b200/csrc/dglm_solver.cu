@@ -62,6 +62,7 @@ StageArgs dglm::stage_args(dglm_handle *h, const double *u_in, double *u_out, in
   a.geo = h->geo;
   a.fscale = h->fscale;
   a.nrm = h->nrm;
+  a.erec = h->erec;
   a.tau = h->tau;
   a.vmapP = h->vmapP;
   a.Fmask = h->Fmask;
@@ -438,6 +439,8 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   chk(dalloc(h, &h->geo, (size_t)9 * K));
   chk(dalloc(h, &h->fscale, (size_t)4 * K));
   chk(dalloc(h, &h->nrm, (size_t)12 * K));
+  if (d.physics == DGLM_EULER && d.precision == DGLM_PREC_TF32X3)
+    chk(dalloc(h, &h->erec, (size_t)kRecord * K));
   chk(dalloc(h, &h->tau, (size_t)4 * K));
   chk(dalloc(h, &h->maxv, (size_t)4 * K));
   // padded to whole tiles: the tensor-core kernel bulk-copies vmapP per tile
@@ -572,6 +575,20 @@ dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *m) {
   cudaError_t e = cudaMemcpy(h->geo, geo.data(), sizeof(double) * geo.size(), H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->nrm, nrm.data(), sizeof(double) * nrm.size(), H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->fscale, m->Fscale, sizeof(double) * 4 * K, H2D);
+  if (e == cudaSuccess && h->erec) {
+    std::vector<double> rec((size_t)kRecord * Kp, 0.0);
+    for (long k = 0; k < K; k++) {
+      double *r = &rec[(size_t)k * kRecord];
+      for (int q = 0; q < 9; q++) r[q] = g9[q][k];
+      for (int f = 0; f < 4; f++) {
+        r[9 + f] = m->nx[4 * k + f];
+        r[13 + f] = m->ny[4 * k + f];
+        r[17 + f] = m->nz[4 * k + f];
+        r[21 + f] = m->Fscale[4 * k + f];
+      }
+    }
+    e = cudaMemcpy(h->erec, rec.data(), sizeof(double) * rec.size(), H2D);
+  }
   if (e == cudaSuccess) e = cudaMemcpy(h->vmapP, m->vmapP, sizeof(int) * K * NFF, H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->vmapF, m->vmapF, sizeof(int) * 4 * K, H2D);
   if (e == cudaSuccess) e = cudaMemcpy(h->Fmask, m->Fmask, sizeof(int) * NFF, H2D);

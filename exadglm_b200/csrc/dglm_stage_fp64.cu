@@ -36,6 +36,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
 #include <vector>
 
 #include "dglm_common.cuh"

@@ -27,8 +27,10 @@
 // the contraction of the centred fluxes IS the right-hand side, while the
 // values that reach the tensor cores are the within-element variations: an
 // order of magnitude smaller than the fluxes for resolved solutions, and with
-// them the TF32 representation and FP32 accumulation errors.  Each flux lane
-// evaluates F(u_0) of its own element beside its node's flux.
+// them the TF32 representation and FP32 accumulation errors.  The node-0
+// terms metric_d . F(u_0) and Fscale_f n_f . F(u_0) of a tile are formed once
+// per element (by the MMA warp, one tile ahead) and subtracted in the first
+// FMA of each flux value.
 //
 // K order.  Volume columns are node-group major, k = (i/4)*12 + d*4 + i%4
 // (d = r, s, t); face columns follow at KVA + f NFPP + j.  A warp task covers
@@ -36,19 +38,20 @@
 // 8-row x 16-byte core matrix.
 //
 // Warps: NC compute warps, one producer warp, one MMA warp.
-//   producer    per tile, into a ring of NB buffers: bulk copies of u,
-//               metrics and face data (one copy per lane), an L2 prefetch of
-//               the tile's RK register rows, cp.async gathers of the
-//               neighbour traces u[vmapP].
-//   MMA         lane 0: once the compute warps have written operand image
-//               set t%2 (flux_done[t%2]) and accumulator D[t%2] is free
-//               (d_free[t%2]), the volume and face MMAs of tile t, committed
-//               to mma_done[t%2].
-//   compute     per tile t: volume and face flux tasks of t into image set
-//               t%2, then the epilogue of t-1: loads of t-1's RK register
-//               values, the wait for MMA(t-1); warps 0..3 read D[(t-1)%2]
-//               (one lane quarter each) and add the parts into the rhs
-//               staging; all compute warps do the LSERK update with
+//   producer    per tile, into a ring of NB buffers: bulk copies of u (one
+//               per variable), of the element records (metrics, normals,
+//               Fscale) and of tau, one copy per lane; cp.async gathers of
+//               the neighbour traces u[vmapP].
+//   MMA         once the compute warps have written operand image set t%2
+//               (flux_done[t%2]): all lanes form the node-0 terms of tile t+1
+//               (cen[(t+1)%2]); then lane 0, once accumulator D[t%2] is free
+//               (d_free[t%2]), issues the volume and face MMAs of tile t,
+//               committed to mma_done[t%2].
+//   compute     per tile t: loads of tile t-1's RK register values, the
+//               volume and face flux tasks of t into image set t%2, then the
+//               epilogue of t-1: the wait for MMA(t-1); warps 0..3 read
+//               D[(t-1)%2] (one lane quarter each) and add the parts into the
+//               rhs staging; all compute warps do the LSERK update with
 //               coalesced stores.
 // The tensor cores work on tile t while the compute warps finish t-1 and
 // start t+1.  Every wait is bounded; on expiry a warp sets flag bit 2, waits
@@ -75,13 +78,15 @@ struct TCfg {
   static constexpr int D_COLS = MN, A_COL = 2 * MN;
   static constexpr int TMEM_COLS = 512;
   // tile ring buffer (doubles): u [v][e][i], neighbour traces [v][e][UPS],
-  // metrics [9][e], face data [nx ny nz fs tau][e][f]
+  // element records [e][kRecord], tau [e][f]
   static constexpr int UPS = NFF % 8 == 4 ? NFF : NFF + 4;
   static constexpr int S_U = NV * E * Np, S_UP = NV * E * UPS;
-  static constexpr int S_GEO = 9 * E, S_FACE = 20 * E;
-  static constexpr int S_BUF = S_U + S_UP + S_GEO + S_FACE;
-  static constexpr unsigned TX = 8u * (S_U + S_GEO + S_FACE);
-  static constexpr int NCOPY = NV + 9 + 5 + NV;          // bulk copies + k prefetches per tile
+  static constexpr int S_REC = kRecord * E, S_TAU = 4 * E;
+  static constexpr int S_BUF = S_U + S_UP + S_REC + S_TAU;
+  static constexpr unsigned TX = 8u * (S_U + S_REC + S_TAU);
+  static constexpr int NCOPY = NV + 2;                   // bulk copies per tile
+  // node-0 terms [e][v][NCEN] (3 volume directions, 4 faces), two slots
+  static constexpr int NCEN = 7, S_C = E * NV * NCEN;
   // rhs staging [v][e][i] (FP32: the sum of the four part products)
   static constexpr int S_R = NV * E * Np;
   // warp tasks per tile: volume (8 elements x one node group of 4), face
@@ -95,10 +100,11 @@ struct TCfg {
   static constexpr int GPL = (E * NFF + 31) / 32;        // gathers per producer lane
   static constexpr size_t OFF_RING = 2 * (size_t)B_BYTES;
   static constexpr size_t OFF_R = OFF_RING + 8 * (size_t)NB * S_BUF;
-  static constexpr size_t OFF_BAR = OFF_R + (4 * (size_t)S_R + 15) / 16 * 16;
-  // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2];
-  // then the tensor-memory address, Fmask, maxima
-  static constexpr int NBARS = 2 * NB + 6;
+  static constexpr size_t OFF_C = OFF_R + (4 * (size_t)S_R + 15) / 16 * 16;
+  static constexpr size_t OFF_BAR = OFF_C + 8 * 2 * (size_t)S_C;
+  // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2],
+  // cen[2]; then the tensor-memory address, Fmask, maxima
+  static constexpr int NBARS = 2 * NB + 8;
   static constexpr size_t SMEM = OFF_BAR + 8 * (NBARS + 1) + 4 * NFF + 8 * 32 + 64;
   // instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N, M = 128
   static constexpr unsigned IDESC =
@@ -109,6 +115,7 @@ struct TCfg {
   static_assert(2 * D_COLS + KT <= TMEM_COLS, "accumulators and operator fit tensor memory");
   static_assert(NC >= 4, "compute warps 0..3 cover the four tensor-memory lane quarters");
   static_assert(NCOPY <= 32, "one producer lane per bulk copy");
+  static_assert(4 * E <= 32, "the MMA warp forms node-0 terms with 4 lanes per element");
   static_assert(NCOL <= 64 && NCOL % 2 == 0,
                 "an epilogue lane holds both parts of its row's columns, split in halves");
   static_assert(NB >= 2 && NB <= 4, "ring of 2..4 tile buffers");
@@ -153,10 +160,6 @@ __device__ __forceinline__ void split_tf32_pair(double x, unsigned &hi, unsigned
   hi = __float_as_uint(f) & 0xffffe000u;
   lo = __float_as_uint(f - __uint_as_float(hi));
 }
-// bulk prefetch of [src, src + bytes) into L2 (16-byte aligned, multiple of 16)
-__device__ __forceinline__ void bulk_prefetch_l2(const void *src, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
 
 template <int PHYS, int N, int E_, int NC_, int NB_>
 __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
@@ -167,9 +170,10 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   double *sRing = reinterpret_cast<double *>(smem_raw + C::OFF_RING);
   float *sR = reinterpret_cast<float *>(smem_raw + C::OFF_R);
+  double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
   unsigned long long *full = bars, *empty = bars + NB, *flux_done = bars + 2 * NB,
-                     *mma_done = flux_done + 2, *d_free = flux_done + 4;
+                     *mma_done = flux_done + 2, *d_free = flux_done + 4, *cen = flux_done + 6;
   unsigned *sTmem = reinterpret_cast<unsigned *>(bars + C::NBARS);
   int *sFm = reinterpret_cast<int *>(bars + C::NBARS + 1);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
@@ -190,6 +194,7 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       mbar_init(&flux_done[b], NC);
       mbar_init(&mma_done[b], 1);
       mbar_init(&d_free[b], 4);
+      mbar_init(&cen[b], 1);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -236,27 +241,26 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       const int eb = wt / C::NG, g = wt - eb * C::NG;
       const int e = eb * 8 + (lane & 7), i = 4 * g + (lane >> 3);
       const bool okn = e < ne && i < Np;
-      const double *bU = ring(it), *bG = bU + C::S_U + C::S_UP;
+      const double *bU = ring(it), *bR = bU + C::S_U + C::S_UP + e * kRecord;
       unsigned hv[5][3], lv[5][3];
       if (okn) {
-        double q[5], F[5], G[5], W[5], F0[5], G0[5], W0[5];
-#pragma unroll
-        for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
-        euler_flux_fast(gam, q, F0, G0, W0);
+        const double *cn = sC0 + (it & 1) * C::S_C + e * NV * C::NCEN;
+        double q[5], F[5], G[5], W[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
         euler_flux_fast(gam, q, F, G, W);
         double m[9];
 #pragma unroll
-        for (int x = 0; x < 9; x++) m[x] = bG[x * E + e];
+        for (int x = 0; x < 9; x++) m[x] = bR[x];
 #pragma unroll
-        for (int v = 0; v < 5; v++) {
-          const double dF = F[v] - F0[v], dG = G[v] - G0[v], dW = W[v] - W0[v];
+        for (int v = 0; v < 5; v++)
 #pragma unroll
           for (int d = 0; d < 3; d++)
-            split_tf32_pair(fma(m[3 * d + 2], dW, fma(m[3 * d + 1], dG, m[3 * d] * dF)),
+            // the node-0 term enters the first FMA of the metric combination
+            split_tf32_pair(fma(m[3 * d + 2], W[v],
+                                fma(m[3 * d + 1], G[v], fma(m[3 * d], F[v],
+                                                            -cn[v * C::NCEN + d]))),
                             hv[v][d], lv[v][d]);
-        }
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++)
@@ -281,17 +285,14 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       const int e = eb * 8 + (lane & 7), j = jb * 4 + (lane >> 3);
       const bool okn = e < ne && j < Nfp;
       const double *bU = ring(it), *bUP = bU + C::S_U;
-      const double *bF = bUP + C::S_UP + C::S_GEO;
+      const double *bR = bUP + C::S_UP + e * kRecord, *bT = bUP + C::S_UP + C::S_REC;
       unsigned hv[5], lv[5];
       if (okn) {
         const int fj = f * Nfp + j, nodeM = sFm[fj];
-        const double nx = bF[0 * 4 * E + e * 4 + f], ny = bF[1 * 4 * E + e * 4 + f],
-                     nz = bF[2 * 4 * E + e * 4 + f], fs = bF[3 * 4 * E + e * 4 + f],
-                     tau = bF[4 * 4 * E + e * 4 + f];
-        double q0[5], qm[5], qb[5], F[5], G[5], W[5], F0[5], G0[5], W0[5];
-#pragma unroll
-        for (int v = 0; v < 5; v++) q0[v] = bU[v * E * Np + e * Np];
-        euler_flux_fast(gam, q0, F0, G0, W0);
+        const double nx = bR[9 + f], ny = bR[13 + f], nz = bR[17 + f], fs = bR[21 + f],
+                     tau = bT[e * 4 + f];
+        const double *cn = sC0 + (it & 1) * C::S_C + e * NV * C::NCEN + 3 + f;
+        double qm[5], qb[5], F[5], G[5], W[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           qm[v] = bU[v * E * Np + e * Np + nodeM];
@@ -300,8 +301,8 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         euler_flux_fast(gam, qb, F, G, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          const double nd = fma(nz, W[v] - W0[v], fma(ny, G[v] - G0[v], nx * (F[v] - F0[v])));
-          split_tf32_pair((nd - tau * (qb[v] - qm[v])) * fs, hv[v], lv[v]);
+          const double nd = fma(nz, W[v], fma(ny, G[v], nx * F[v]));
+          split_tf32_pair(fma(nd - tau * (qb[v] - qm[v]), fs, -cn[v * C::NCEN]), hv[v], lv[v]);
         }
       } else {
 #pragma unroll
@@ -317,26 +318,39 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       }
     };
 
-    // epilogue of ring iteration `it` from accumulator buffer it % 2; false
-    // when the wait for its MMAs expired (on every compute warp alike)
+    // this thread's RK register values of ring iteration `it` (update order:
+    // x = tid + r TC over (variable, element node)); the element count is a
+    // literal for full tiles, so the index divisions are multiplications
+    double kr[C::KPT];
+    auto load_k = [&](int it) {
+      const long e0 = tile_e0(it);
+      const int ne = (int)min((long)E, (long)a.K - e0);
+      auto body = [&](auto nepc) {
+        const int nep = nepc;
+#pragma unroll
+        for (int r = 0; r < C::KPT; r++) {
+          const int x = tid + r * TC;
+          kr[r] = 0.0;
+          if (!a.rhs_only && x < NV * nep) {
+            const int v = x / nep, g = x - v * nep;
+            kr[r] = a.kreg[v * vs + e0 * Np + g];
+          }
+        }
+      };
+      if (ne == E)
+        body(std::integral_constant<int, E * Np>{});
+      else
+        body(ne * Np);
+    };
+
+    // epilogue of ring iteration `it` from accumulator buffer it % 2, with
+    // its RK register values in kr; false when the wait for its MMAs expired
+    // (on every compute warp alike)
     auto epilogue = [&](int it) -> bool {
       const int db = it & 1;
       const long e0 = tile_e0(it);
       const int ne = (int)min((long)E, (long)a.K - e0);
-      const int nep = ne * Np;
       double *bU = ring(it);
-      // this thread's RK register values (prefetched into L2 with the tile),
-      // loaded while the MMAs finish
-      double kr[C::KPT];
-#pragma unroll
-      for (int r = 0; r < C::KPT; r++) {
-        const int x = tid + r * TC;
-        kr[r] = 0.0;
-        if (!a.rhs_only && x < NV * nep) {
-          const int v = x / nep, g = x - v * nep;
-          kr[r] = a.kreg[v * vs + e0 * Np + g];
-        }
-      }
       // MMA(it) done; every compute warp is done with the staging of the
       // previous update
       if (!consumer_all(mbar_wait(&mma_done[db], (it >> 1) & 1, lim), TC)) return false;
@@ -364,33 +378,40 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         }
       }
       consumer_sync(TC);
-      // LSERK update over (variable, element, node): staged rhs, u and the
+      // LSERK update over (variable, element node): staged rhs, u and the
       // RK register values, coalesced stores
+      auto update = [&](auto nepc) {
+        const int nep = nepc;
 #pragma unroll
-      for (int r = 0; r < C::KPT; r++) {
-        const int x = tid + r * TC;
-        if (x < NV * nep) {
-          const int v = x / nep, g = x - v * nep;
-          const int si = v * E * Np + g;
-          const long gi = v * vs + e0 * Np + g;
-          const double rhs = (double)sR[si];
-          if (a.rhs_only) {
-            a.u_out[gi] = rhs;
-          } else {
-            const double kn = a.rka * kr[r] + dt * rhs;
-            const double un = bU[si] + a.rkb * kn;
-            a.kreg[gi] = kn;
-            a.u_out[gi] = un;
-            if (keep_u) bU[si] = un;
+        for (int r = 0; r < C::KPT; r++) {
+          const int x = tid + r * TC;
+          if (x < NV * nep) {
+            const int v = x / nep, g = x - v * nep;
+            const int si = v * E * Np + g;
+            const long gi = v * vs + e0 * Np + g;
+            const double rhs = (double)sR[si];
+            if (a.rhs_only) {
+              a.u_out[gi] = rhs;
+            } else {
+              const double kn = a.rka * kr[r] + dt * rhs;
+              const double un = bU[si] + a.rkb * kn;
+              a.kreg[gi] = kn;
+              a.u_out[gi] = un;
+              if (keep_u) bU[si] = un;
+            }
           }
         }
-      }
+      };
+      if (ne == E)
+        update(std::integral_constant<int, E * Np>{});
+      else
+        update(ne * Np);
       if (keep_u) {
         // fused calc_maxv on the new state: per face, max |v|^2 and c^2 over
         // its nodes (divisions as in face_maxv_kernel, so dt does not depend
         // on which kernel computed maxv)
         consumer_sync(TC);
-        const double *bF = bU + C::S_U + C::S_UP + C::S_GEO;
+        const double *bR = bU + C::S_U + C::S_UP;
         for (int x = tid; x < 4 * E; x += TC) {
           const int f = x / E, e = x - f * E;
           if (e >= ne) continue;
@@ -411,7 +432,7 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
           double mv = sqrt(mv2) + sqrt(mc2);
           if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
           a.maxv[(e0 + e) * 4 + f] = mv;
-          const unsigned long long bits = dbits(mv * bF[3 * 4 * E + e * 4 + f]);
+          const unsigned long long bits = dbits(mv * bR[e * kRecord + 21 + f]);
           vmax = bits > vmax ? bits : vmax;
         }
       }
@@ -425,12 +446,17 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
 
     for (int it = 0; ok && it < my_tiles; it++) {
       const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
-      // the tile's data; image set it % 2 was last read by MMA(it - 2),
-      // whose completion every compute warp saw in epilogue(it - 2)
-      if (!consumer_all(mbar_wait(&full[it % NB], (it / NB) & 1, lim), TC)) {
+      // the tile's data and its node-0 terms; image set it % 2 was last read
+      // by MMA(it - 2), whose completion every compute warp saw in
+      // epilogue(it - 2)
+      const bool w = mbar_wait(&full[it % NB], (it / NB) & 1, lim) &&
+                     mbar_wait(&cen[it & 1], (it >> 1) & 1, lim);
+      if (!consumer_all(w, TC)) {
         ok = false;
         break;
       }
+      // the previous tile's RK register values, in flight during the tasks
+      if (it > 0) load_k(it - 1);
       unsigned char *sBv = smem_raw + (it & 1) * C::B_BYTES, *sBf = sBv + C::BV_BYTES;
       for (int wt = warp; wt < C::NTASK; wt += NC) {
         if (wt < C::VOL_WT)
@@ -446,7 +472,10 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         break;
       }
     }
-    if (ok && my_tiles > 0 && !epilogue(my_tiles - 1)) ok = false;
+    if (ok && my_tiles > 0) {
+      load_k(my_tiles - 1);
+      if (!epilogue(my_tiles - 1)) ok = false;
+    }
   } else if (warp == C::PROD_WARP) {
     // ------------------------------------------------------ producer warp
     int it = 0;
@@ -458,26 +487,16 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       }
       const long e0 = tile_e0(it);
       const int ne = (int)min((long)E, (long)a.K - e0);
-      double *bU = ring(it), *bUP = bU + C::S_U, *bG = bUP + C::S_UP, *bF = bG + C::S_GEO;
+      double *bU = ring(it), *bUP = bU + C::S_U, *bR = bUP + C::S_UP, *bT = bR + C::S_REC;
       // bulk copies, one per lane, after lane 0 has posted the byte count
       if (lane == 0) mbar_arrive_expect_tx(&full[b], C::TX);
       __syncwarp();
-      const int x = lane;
-      if (x < NV) {
-        bulk_g2s(bU + x * E * Np, a.u_in + x * vs + e0 * Np, 8u * E * Np, &full[b]);
-      } else if (x < NV + 9) {
-        const int m = x - NV;
-        bulk_g2s(bG + m * E, a.geo + m * a.gstride + e0, 8u * E, &full[b]);
-      } else if (x < NV + 12) {
-        const int q = x - NV - 9;
-        bulk_g2s(bF + q * 4 * E, a.nrm + q * 4 * a.gstride + 4 * e0, 32u * E, &full[b]);
-      } else if (x == NV + 12) {
-        bulk_g2s(bF + 3 * 4 * E, a.fscale + 4 * e0, 32u * E, &full[b]);
-      } else if (x == NV + 13) {
-        bulk_g2s(bF + 4 * 4 * E, a.tau + 4 * e0, 32u * E, &full[b]);
-      } else if (x < NV + 14 + NV && !a.rhs_only) {
-        bulk_prefetch_l2(a.kreg + (x - NV - 14) * vs + e0 * Np, 8u * E * Np);
-      }
+      if (lane < NV)
+        bulk_g2s(bU + lane * E * Np, a.u_in + lane * vs + e0 * Np, 8u * E * Np, &full[b]);
+      else if (lane == NV)
+        bulk_g2s(bR, a.erec + e0 * kRecord, 8u * C::S_REC, &full[b]);
+      else if (lane == NV + 1)
+        bulk_g2s(bT, a.tau + 4 * e0, 8u * C::S_TAU, &full[b]);
       // neighbour traces u+ = u[vmapP] into [v][e][UPS]: this lane's vmapP
       // entries are loaded before its gathers are issued
       int vmr[C::GPL];
@@ -503,16 +522,65 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
     asm volatile("cp.async.wait_all;" ::: "memory");
   } else {
     // ----------------------------------------------------------- MMA warp
-    if (lane == 0) {
-      int nm = 0;   // tiles whose MMAs were issued and committed
-      for (int it = 0; it < my_tiles; it++) {
-        const int b = it & 1;
-        bool w = mbar_wait(&flux_done[b], (it >> 1) & 1, lim);
-        if (it >= 2) w = w && mbar_wait(&d_free[b], ((it >> 1) - 1) & 1, lim);
-        if (!w) {
-          ok = false;
-          break;
+    // node-0 terms of ring iteration t into centre slot t & 1: lane
+    // 4e + r evaluates F(u_0) of element e, then r = 0 the three volume
+    // terms, r = 1..3 the face terms of faces r - 1 and (r = 3) 3
+    auto centers = [&](int t) {
+      const int e = lane >> 2, r = lane & 3;
+      const int ne = (int)min((long)E, (long)a.K - tile_e0(t));
+      const double *bU = ring(t), *bR = bU + C::S_U + C::S_UP + e * kRecord;
+      double *c = sC0 + (t & 1) * C::S_C + e * NV * C::NCEN;
+      if (e >= E) return;
+      if (e >= ne) {
+        if (r == 0)
+#pragma unroll
+          for (int x = 0; x < NV * C::NCEN; x++) c[x] = 0.0;
+        return;
+      }
+      double q[5], F[5], G[5], W[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
+      euler_flux_fast(gam, q, F, G, W);
+      if (r == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const double mx = bR[3 * d], my = bR[3 * d + 1], mz = bR[3 * d + 2];
+#pragma unroll
+          for (int v = 0; v < 5; v++) c[v * C::NCEN + d] = mx * F[v] + my * G[v] + mz * W[v];
         }
+      } else {
+        const int nf = r == 3 ? 2 : 1;   // r = 1: face 0, r = 2: face 1, r = 3: faces 2, 3
+#pragma unroll
+        for (int h = 0; h < nf; h++) {
+          const int f = r - 1 + h;
+          const double nx = bR[9 + f], ny = bR[13 + f], nz = bR[17 + f], fs = bR[21 + f];
+#pragma unroll
+          for (int v = 0; v < 5; v++)
+            c[v * C::NCEN + 3 + f] = (nx * F[v] + ny * G[v] + nz * W[v]) * fs;
+        }
+      }
+    };
+    // the terms of tile t once its data has landed; false on expiry
+    auto centers_of = [&](int t) -> bool {
+      const bool w = mbar_wait(&full[t % NB], (t / NB) & 1, lim);
+      if (w) centers(t);
+      __syncwarp();
+      if (lane == 0 && w) mbar_arrive(&cen[t & 1]);
+      return __all_sync(0xffffffffu, w);
+    };
+    int nm = 0;   // tiles whose MMAs were issued and committed
+    if (my_tiles > 0 && !centers_of(0)) ok = false;
+    for (int it = 0; ok && it < my_tiles; it++) {
+      const int b = it & 1;
+      bool w = mbar_wait(&flux_done[b], (it >> 1) & 1, lim);
+      // the next tile's node-0 terms while the tensor cores are idle
+      if (__all_sync(0xffffffffu, w) && it + 1 < my_tiles) w = centers_of(it + 1);
+      if (w && it >= 2) w = mbar_wait(&d_free[b], ((it >> 1) - 1) & 1, lim);
+      if (!__all_sync(0xffffffffu, w)) {
+        ok = false;
+        break;
+      }
+      if (lane == 0) {
         tc_fence_after();
         const unsigned d = tmem + b * C::D_COLS;
         const unsigned bv = smem_u32(smem_raw + b * C::B_BYTES), bf = bv + C::BV_BYTES;
@@ -525,12 +593,14 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
           tc_mma_ts(d, tmem + C::A_COL + C::KVA + ks * 8,
                     smem_desc(bf + ks * 256, 128, C::SBO_F), C::IDESC, 1);
         tc_commit(&mma_done[b]);
-        nm++;
       }
-      // the MMAs issued (and their barrier arrivals) are complete before
-      // tensor and shared memory are released, on expiry too
-      for (int t = (nm > 2 ? nm - 2 : 0); t < nm; t++) mbar_wait(&mma_done[t & 1], (t >> 1) & 1);
+      __syncwarp();
+      nm++;
     }
+    // the MMAs issued (and their barrier arrivals) are complete before
+    // tensor and shared memory are released, on expiry too
+    if (lane == 0)
+      for (int t = (nm > 2 ? nm - 2 : 0); t < nm; t++) mbar_wait(&mma_done[t & 1], (t >> 1) & 1);
   }
   if (!ok) atomicOr(&a.sc->flags, 4);
   if (keep_u) {
