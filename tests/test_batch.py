@@ -80,3 +80,31 @@ def test_batch_clips_each_instance_to_tmax():
         assert t2 == pytest.approx(0.02, abs=1e-15) and t1 == t2 and n1 == n2
         s.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_batch_config4_instances_match_single_solvers():
+    """The first 16 instances of the 256-instance ensemble workload (seed 0:
+    n in 4..24, N in 2..6, the full size distribution) batched, against one
+    single-mesh solver per instance, 10 steps."""
+    probs = P.batch_instances(count=16, seed=0)
+    assert max(p.K for p in probs) > 6 * 12 ** 3 and len({p.N for p in probs}) >= 4
+    b = capi.BatchSolver(probs)
+    nsteps = 10
+    b.step(nsteps)
+    b.sync()
+    worst = 0.0
+    for i, p in enumerate(probs):
+        s = capi.Solver(p)
+        s.step(nsteps)
+        s.sync()
+        e = rel(b.get_state(i), s.get_state().ravel())
+        t1, dt1, n1 = s.time()
+        t2, dt2, n2 = b.time(i)
+        s.close()
+        worst = max(worst, e)
+        assert e <= 1e-13, (i, p.N, p.K, e)
+        assert n1 == n2 == nsteps and t1 == t2 and dt1 == dt2, (i, t1, t2)
+    print(f"16 config-4 instances (K {min(p.K for p in probs)}..{max(p.K for p in probs)}): "
+          f"worst rel L2 vs single solvers {worst:.2e}")
+    b.close()
