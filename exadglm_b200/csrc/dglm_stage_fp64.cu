@@ -59,23 +59,38 @@ __device__ __forceinline__ void euler_flux_fast(double g, const double q[5], dou
   W[0] = q[3]; W[1] = q[1] * vz; W[2] = q[2] * vz; W[3] = q[3] * vz + p; W[4] = H * vz;
 }
 
-// Centring of split-precision operands: subtracts the flux of the element's
-// node-0 state (q0[v] = u0[v * vstride]) from a node's flux.  A flux that is
-// constant over an element has zero DG right-hand side (the weak volume term
-// equals the surface term on straight-sided tetrahedra), so the contraction
-// of centred fluxes is the right-hand side, and the split parts carry only
-// the within-element variation (smaller, and with it their rounding).
-__device__ __forceinline__ void centre_node0(double g, const double *u0, int vstride,
-                                             double F[5], double G[5], double W[5]) {
-  double q0[5], F0[5], G0[5], W0[5];
+// Centring of split-precision operands.  A flux that is constant over an
+// element has zero DG right-hand side (the weak volume term equals the
+// surface term on straight-sided tetrahedra), so subtracting each element's
+// node-0 flux from all its flux values leaves the contraction's result
+// unchanged, while the split parts carry only the within-element variation
+// (smaller, and with it their rounding).  node0_fluxes writes F, G, W of the
+// node-0 state of elements e = t, t + nt, ... < E to cen[e * 15 + (0..4,
+// 5..9, 10..14)], reading variable v of element e at u[e * estride + v * vstride];
+// centre_sub subtracts them from a node's flux.
+constexpr int kCen = 15;
+__device__ __forceinline__ void node0_fluxes(double g, const double *u, int estride,
+                                             int vstride, int E, int t, int nt, double *cen) {
+  for (int e = t; e < E; e += nt) {
+    double q[5], F[5], G[5], W[5];
 #pragma unroll
-  for (int v = 0; v < 5; v++) q0[v] = u0[v * vstride];
-  euler_flux_fast(g, q0, F0, G0, W0);
+    for (int v = 0; v < 5; v++) q[v] = u[e * estride + v * vstride];
+    euler_flux_fast(g, q, F, G, W);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      cen[e * kCen + v] = F[v];
+      cen[e * kCen + 5 + v] = G[v];
+      cen[e * kCen + 10 + v] = W[v];
+    }
+  }
+}
+__device__ __forceinline__ void centre_sub(const double *c, double F[5], double G[5],
+                                           double W[5]) {
 #pragma unroll
   for (int v = 0; v < 5; v++) {
-    F[v] -= F0[v];
-    G[v] -= G0[v];
-    W[v] -= W0[v];
+    F[v] -= c[v];
+    G[v] -= c[5 + v];
+    W[v] -= c[10 + v];
   }
 }
 
@@ -124,8 +139,9 @@ struct Cfg {
   static constexpr int S_B = BROWS * BLD;
   static constexpr int S_GEO = 9 * E;
   static constexpr int S_FACE = 5 * 4 * E;                     // nx ny nz fs tau
+  static constexpr int S_CEN = (MODE == MODE_MMA16 && PHYS == EUL) ? kCen * E : 0;
   static constexpr int VMLD = NFF + 1;                         // vmapP row stride (ints)
-  static constexpr size_t SMEM = sizeof(double) * (S_U + S_B + S_GEO + S_FACE) +
+  static constexpr size_t SMEM = sizeof(double) * (S_U + S_B + S_GEO + S_FACE + S_CEN) +
                                  sizeof(int) * ((size_t)E * VMLD + NFF);
   static_assert(NCOL % CPT_ == 0, "columns must split evenly");
   static_assert(S_B >= NV * Np * EP, "epilogue reuses B for the rhs");
@@ -199,7 +215,8 @@ __device__ __forceinline__ void contract_dmma(const double *__restrict__ Afrag, 
 // bits per lane, one coalesced 512-byte load); B = the FP64 fluxes in
 // shared memory, split in registers; NPROD16 part products per k-step into
 // FP32 accumulators that are folded into FP64 every SL16 k-steps.  Euler
-// fluxes are centred (centre_node0) before they are stored for the split.
+// fluxes are centred (node0_fluxes, centre_sub) before they are stored for
+// the split.
 //   m16n8k8 TF32:  a0=A[g][t] a1=A[g+8][t] a2=A[g][t+4] a3=A[g+8][t+4],
 //                  b0=B[t][g] b1=B[t+4][g]
 //   m16n8k16 BF16: a0=A[g][2t..2t+1] a1=A[g+8][2t..] a2=A[g][2t+8..] a3=A[g+8][2t+8..],
@@ -354,7 +371,8 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
   double *sB = sU + C::S_U;             // [k][BLD], col = v*E + e
   double *sGeo = sB + C::S_B;           // [9][E]
   double *sFace = sGeo + C::S_GEO;      // [5][4][E]: nx ny nz fs tau
-  int *sVm = reinterpret_cast<int *>(sFace + C::S_FACE);   // [E][VMLD]
+  double *sCen = sFace + C::S_FACE;    // [E][15]: node-0 fluxes (split modes, Euler)
+  int *sVm = reinterpret_cast<int *>(sCen + C::S_CEN);     // [E][VMLD]
   int *sFm = sVm + E * C::VMLD;         // [NFF]
 
   const int tid = threadIdx.x;
@@ -391,6 +409,10 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
     sVm[e * C::VMLD + fj] = g < ne * NFF ? __ldg(a.vmapP + e0 * NFF + g) : 0;
   }
   __syncthreads();
+  if constexpr (M16 && PHYS == EUL) {
+    node0_fluxes(a.gamma, sU, 1, Np * EP, E, tid, T, sCen);
+    __syncthreads();
+  }
 
   // 1. volume fluxes -> B rows [0, 3Np)
   for (int it = tid; it < E * Np; it += T) {
@@ -403,7 +425,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 #pragma unroll
       for (int v = 0; v < 5; v++) q[v] = sU[(v * Np + i) * EP + e];
       euler_flux_fast(a.gamma, q, F, Gf, W);
-      if constexpr (M16) centre_node0(a.gamma, sU + e, Np * EP, F, Gf, W);
+      if constexpr (M16) centre_sub(sCen + e * kCen, F, Gf, W);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const int col = v * E + e;
@@ -479,7 +501,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
         qb[v] = 0.5 * (qm[v] + __ldg(a.u_in + v * vs + idxP));
       }
       euler_flux_fast(a.gamma, qb, F, Gf, W);
-      if constexpr (M16) centre_node0(a.gamma, sU + e, Np * EP, F, Gf, W);
+      if constexpr (M16) centre_sub(sCen + e * kCen, F, Gf, W);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];

@@ -12,9 +12,9 @@
 // the product is taken in three passes, hi*hi + hi*lo + lo*hi, accumulating
 // in FP32.  Fluxes, the LSERK state and update, metrics and face data stay
 // FP64; only the contraction operands and its accumulator are reduced.
-// Euler fluxes are centred before the split (centre_node0: the element's
-// node-0 flux subtracted, which leaves the right-hand side unchanged), so
-// the split parts carry only the within-element variation.
+// Euler fluxes are centred before the split (each element's node-0 flux,
+// formed once per tile by node0_fluxes, subtracted; the right-hand side is
+// unchanged), so the split parts carry only the within-element variation.
 //
 // Per tile: flux phase writes the volume operand -> one thread issues the
 // volume MMAs and commits to an mbarrier -> once they have read the operand
@@ -172,7 +172,10 @@ struct MCfg {
   static constexpr int S_VEL = PHYS == EUL ? 0 : 3 * E * Np;
   static constexpr int S_BUF = S_U + S_K + S_UP + S_GEO + S_FACE + S_VEL;
   static constexpr int S_R = NV * Np * EP;
-  static constexpr size_t FP64_BYTES = sizeof(double) * (2 * (size_t)S_BUF + S_R) + 1024;
+  // + barriers, tensor-memory address, Fmask, maxima, node-0 fluxes [E][15] (Euler)
+  static constexpr int S_CEN = PHYS == EUL ? kCen * E : 0;
+  static constexpr size_t FP64_BYTES =
+      sizeof(double) * (2 * (size_t)S_BUF + S_R + S_CEN) + 1024;
   // separate volume and lift operands let the face phase overlap the volume
   // MMAs; used where they fit next to the rest
   static constexpr bool SEPL =
@@ -263,6 +266,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
   unsigned *sTmem = reinterpret_cast<unsigned *>(bars + 6);
   int *sFm = reinterpret_cast<int *>(bars + 8);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
+  double *sCen = reinterpret_cast<double *>(sMax + 32);   // [E][15] node-0 fluxes
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long vs = a.vs;
@@ -344,6 +348,11 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
     double *B = sBuf0 + b * C::S_BUF;
     double *bU = B, *bK = bU + C::S_U, *bUP = bK + C::S_K, *bG = bUP + C::S_UP;
     double *bF = bG + C::S_GEO, *bV = bF + C::S_FACE;
+    if (PHYS == EUL) {
+      // the previous tile's face fluxes, the last readers, are past a barrier
+      node0_fluxes(a.gamma, bU, Np, E * Np, E, tid, TC, sCen);
+      consumer_sync(TC);
+    }
 
     // 1. volume fluxes -> operand rows m = v*E + e, k = d*Np + i
     for (int itm = tid; itm < E * Np; itm += TC) {
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
 #pragma unroll
         for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
         euler_flux_fast(a.gamma, q, F, Gf, W);
-        centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
+        centre_sub(sCen + e * kCen, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const int m = v * E + e;
@@ -405,7 +414,7 @@ __global__ void __launch_bounds__(MCfg<PHYS, N, E_, PREC, NWC_, PW_>::THREADS, 1
           qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
         }
         euler_flux_fast(a.gamma, qb, F, Gf, W);
-        centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
+        centre_sub(sCen + e * kCen, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];

@@ -198,7 +198,10 @@ struct PCfg {
   static constexpr int S_B = BROWS * BLD > KSP * S_R ? BROWS * BLD : KSP * S_R;
   // barriers: full[NB], empty[NB], the operator-image barrier, padding
   static constexpr int NBAR = 2 * NB + 2 > 8 ? 2 * NB + 2 : 8;
-  static constexpr int S_MISC = NBAR + NFF / 2 + 1 + 32 * NG + 8;  // barriers, Fmask, reduction
+  // node-0 fluxes of a tile's elements, per consumer group (split modes, Euler)
+  static constexpr int S_CEN = (M16 && PHYS == EUL) ? kCen * E : 0;
+  static constexpr int S_MISC = NBAR + NFF / 2 + 1 + 32 * NG + 8 + NG * S_CEN;  // barriers,
+                                                          // Fmask, reduction, node-0 fluxes
   static constexpr size_t SMEM =
       sizeof(double) * ((size_t)S_AF + NB * S_BUF + NG * S_B + S_MISC);
   // bytes the producer's bulk copies deliver per tile
@@ -352,6 +355,7 @@ __global__ void __launch_bounds__(
   const int warp = twarp - grp * C::NWC, tid = ttid - grp * TC;
   const int bar_sync = 1 + 2 * grp, bar_and = 2 + 2 * grp;
   double *sB = sB0 + grp * C::S_B;
+  double *sCen = reinterpret_cast<double *>(sMax + 32 * C::NG) + grp * C::S_CEN;
   auto consumer_sync = [&](int n) { group_sync(bar_sync, n); };
   auto consumer_all = [&](bool v, int n) { return group_all(v, bar_and, n); };
   double acc[C::M16 ? 1 : C::WM][C::M16 ? 1 : C::WN][2];
@@ -410,7 +414,7 @@ __global__ void __launch_bounds__(
 #pragma unroll
         for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
         euler_flux_fast(a.gamma, q, F, Gf, W);
-        if constexpr (C::M16) centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
+        if constexpr (C::M16) centre_sub(sCen + e * kCen, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const int col = v * E + e, r0 = i, r1 = Np + i, r2 = 2 * Np + i;
@@ -452,7 +456,7 @@ __global__ void __launch_bounds__(
           qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
         }
         euler_flux_fast(a.gamma, qb, F, Gf, W);
-        if constexpr (C::M16) centre_node0(a.gamma, bU + e * Np, E * Np, F, Gf, W);
+        if constexpr (C::M16) centre_sub(sCen + e * kCen, F, Gf, W);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           const double nd = nx * F[v] + ny * Gf[v] + nz * W[v];
@@ -616,6 +620,11 @@ __global__ void __launch_bounds__(
     const long e0 = (long)t * E;
     const int ne = (int)min((long)E, (long)a.K - e0);
     double *B = buf(b);
+    if constexpr (C::M16 && PHYS == EUL) {
+      // the previous tile's face fluxes, the last readers, are past a barrier
+      node0_fluxes(a.gamma, B, Np, E * Np, E, tid, TC, sCen);
+      consumer_sync(TC);
+    }
     vol_flux(B);
 
     // 2. volume contraction (FUSE: part of the one pass after the face fluxes)
