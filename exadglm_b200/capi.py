@@ -160,9 +160,12 @@ def variant_precision(desc):
     for prec in ("tf32x3", "bf16x3", "bf16x6"):
         if desc.startswith(("tcgen05-" + prec, "mma16-" + prec, "pipe-mma16-" + prec)):
             return prec
-    # split TF32 with all four part products (the tensor-memory operator kernel)
+    # split TF32 / BF16 with all four part products (the tensor-memory
+    # operator kernels)
     if desc.startswith("tc-tmem-tf32"):
         return "tf32x3"
+    if desc.startswith("tc-tmem-bf16"):
+        return "bf16x3"
     return "fp64"
 
 

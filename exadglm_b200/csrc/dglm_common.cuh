@@ -143,7 +143,8 @@ dglm_status set_error(dglm_status s, const std::string &msg);
 dglm_status cuda_check(cudaError_t e, const char *what);
 
 // contraction engines of the fused stage kernel
-enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3, MODE_MMA16 = 4, MODE_TC = 5 };
+enum { MODE_SIMT = 0, MODE_DMMA = 1, MODE_PIPE = 2, MODE_MIXED = 3, MODE_MMA16 = 4, MODE_TC = 5,
+       MODE_TCB = 6 };
 
 // One compiled tile shape of the fused stage kernel.
 struct StageVariantInfo {
@@ -160,7 +161,7 @@ struct StageVariantInfo {
   int prec;      // dglm_precision of the contraction (0 FP64, 1 TF32x3, 2 BF16x3)
   int npad;      // MIXED: MMA N (output nodes, padded); TC: output nodes per lane quarter
   int kva, kfa;  // MIXED, TC: volume / lift K extents of the operand images
-  int bimg;      // MIXED: bytes of the operator image (hi then lo); TC: tensor-memory image
+  int bimg;      // MIXED: bytes of the operator image (hi then lo); TC, TCB: tensor-memory image
   int groups;    // PIPE: consumer groups taking alternate tiles (1 or 2)
   int kstep;     // MMA16: K per mma.sync (8 TF32, 16 BF16)
   int persistent;  // 1: one CTA per SM walking the tiles (TMA-fed pipeline)

@@ -26,7 +26,7 @@ struct dglm_handle {
   double *AT = nullptr, *geo = nullptr, *fscale = nullptr, *nrm = nullptr;
   double *tau = nullptr, *maxv = nullptr, *vel = nullptr;
   int *vmapP = nullptr, *vmapF = nullptr, *Fmask = nullptr;
-  // per-element record [Kp][kRecord] (TF32x3 Euler handles): the 9 metrics,
+  // per-element record [Kp][kRecord] (TF32x3 and BF16x3 Euler handles): the 9 metrics,
   // nx, ny, nz and Fscale of the 4 faces, one pad double; one bulk copy per
   // tile in the tensor-memory kernel
   double *erec = nullptr;

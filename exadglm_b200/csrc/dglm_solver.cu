@@ -90,7 +90,8 @@ namespace {
 // Doubles of the device operator copy for a variant's layout.
 size_t op_doubles(const StageVariantInfo &v, int Np, int NFF) {
   if (v.mode == MODE_SIMT) return (size_t)(3 * Np + NFF) * v.IP;
-  if (v.mode == MODE_MIXED || v.mode == MODE_TC) return ((size_t)v.bimg + 7) / 8;
+  if (v.mode == MODE_MIXED || v.mode == MODE_TC || v.mode == MODE_TCB)
+    return ((size_t)v.bimg + 7) / 8;
   if (v.mode == MODE_MMA16) {
     const int parts = v.prec == DGLM_PREC_BF16X6 ? 3 : 2;
     return (size_t)(v.KVP / v.kstep + v.KFP / v.kstep) * v.MT * parts * 64;   // 512 B each
@@ -264,11 +265,42 @@ std::vector<uint32_t> tc_image(const dglm_handle *h, const StageVariantInfo &v) 
   return img;
 }
 
+// Tensor-memory image of the split-BF16 operator (stage_tcb_kernel): 128
+// lanes (lane i = operator row i) x KT 32-bit columns; columns [0, KT/2)
+// hold the BF16 hi parts, [KT/2, KT) the lo parts, two K values per column
+// (the lower K in the low half), K in the kernel's order (volume k = (i/4)*12
+// + d*4 + i%4 over kva columns, then face f node j at kva + f*nfpp + j).
+std::vector<uint32_t> tcb_image(const dglm_handle *h, const StageVariantInfo &v) {
+  const int Np = h->Np, Nfp = h->Nfp, KA = 3 * Np + h->NFF;
+  const int KT = v.kva + v.kfa, half = KT / 2, nfpp = v.kfa / 4, ng = (Np + 3) / 4;
+  std::vector<uint32_t> img((size_t)128 * KT, 0u);
+  for (int k = 0; k < KT; k++) {
+    int col = -1;
+    if (k < v.kva) {
+      const int g = k / 12, d = (k % 12) / 4, i = g * 4 + k % 4;
+      if (g < ng && i < Np) col = d * Np + i;
+    } else {
+      const int f = (k - v.kva) / nfpp, j = (k - v.kva) % nfpp;
+      if (j < Nfp) col = 3 * Np + f * Nfp + j;
+    }
+    if (col < 0) continue;
+    const int c = k / 2, sh = (k & 1) * 16;
+    for (int i = 0; i < Np; i++) {
+      const double x = h->Ahost[(size_t)i * KA + col];
+      const uint16_t hi = bf16_rne((float)x);
+      const uint16_t lo = bf16_rne((float)(x - (double)f32_of((uint32_t)hi << 16)));
+      img[(size_t)i * KT + c] |= (uint32_t)hi << sh;
+      img[(size_t)i * KT + half + c] |= (uint32_t)lo << sh;
+    }
+  }
+  return img;
+}
+
 dglm_status upload_operator_layout(dglm_handle *h) {
   const int Np = h->Np, NFF = h->NFF, KA = 3 * Np + NFF, KV = 3 * Np;
   const StageVariantInfo &v = h->vinfo;
-  if (v.mode == MODE_TC) {
-    std::vector<uint32_t> img = tc_image(h, v);
+  if (v.mode == MODE_TC || v.mode == MODE_TCB) {
+    std::vector<uint32_t> img = v.mode == MODE_TC ? tc_image(h, v) : tcb_image(h, v);
     return cuda_check(cudaMemcpy(h->AT, img.data(), img.size() * 4, cudaMemcpyHostToDevice),
                       "operator upload");
   }
@@ -439,7 +471,8 @@ dglm_status dglm_create(const dglm_desc *desc, dglm_handle **out) {
   chk(dalloc(h, &h->geo, (size_t)9 * K));
   chk(dalloc(h, &h->fscale, (size_t)4 * K));
   chk(dalloc(h, &h->nrm, (size_t)12 * K));
-  if (d.physics == DGLM_EULER && d.precision == DGLM_PREC_TF32X3)
+  if (d.physics == DGLM_EULER &&
+      (d.precision == DGLM_PREC_TF32X3 || d.precision == DGLM_PREC_BF16X3))
     chk(dalloc(h, &h->erec, (size_t)kRecord * K));
   chk(dalloc(h, &h->tau, (size_t)4 * K));
   chk(dalloc(h, &h->maxv, (size_t)4 * K));
@@ -971,6 +1004,9 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
   else if (v.mode == MODE_TC)
     snprintf(buf, len, "tc-tmem-tf32x4 E=%d compute=%d threads=%d smem=%zu ring=%d", v.E,
              v.producers, v.threads, v.smem, v.ring);
+  else if (v.mode == MODE_TCB)
+    snprintf(buf, len, "tc-tmem-bf16x4 E=%d compute=%d threads=%d smem=%zu ring=%d buffers=%d",
+             v.E, v.producers, v.threads, v.smem, v.ring, v.npad);
   else if (v.mode == MODE_MIXED) {
     const int n = snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
                            v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"

@@ -657,6 +657,7 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 #include "dglm_stage_pipe.cuh"
 #include "dglm_stage_mixed.cuh"
 #include "dglm_stage_tc.cuh"
+#include "dglm_stage_tcb.cuh"
 
 // Standalone calc_maxv (initial state, advection velocity): maxv per face and
 // a device-wide max of maxv*Fscale into sc->acc[slot].
@@ -875,6 +876,38 @@ static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <int PHYS, int N, int E, int NF, int NB, bool DB>
+static cudaError_t launch_tcb(const StageArgs &a, cudaStream_t s) {
+  using C = TBCfg<PHYS, N, E, NF, NB, DB>;
+  auto k = stage_tcb_kernel<PHYS, N, E, NF, NB, DB>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)C::SMEM);
+  if (e != cudaSuccess) return e;
+  const int ntiles = (a.K + E - 1) / E;
+  const int grid = ntiles < sm_count() ? ntiles : sm_count();
+  k<<<grid, C::THREADS, C::SMEM, s>>>(a, ntiles);
+  return cudaGetLastError();
+}
+
+template <int PHYS, int N, int E, int NF, int NB, bool DB>
+static Variant make_tcb() {
+  using C = TBCfg<PHYS, N, E, NF, NB, DB>;
+  StageVariantInfo i{};
+  i.mode = MODE_TCB;
+  i.E = E;
+  i.threads = C::THREADS;
+  i.smem = C::SMEM;
+  i.prec = DGLM_PREC_BF16X3;
+  i.npad = DB ? 2 : 1;   // operand image sets and accumulators
+  i.kva = C::KVA;
+  i.kfa = C::KFA;
+  i.bimg = 128 * C::KT * 4;
+  i.ring = NB;
+  i.producers = NF;      // compute warps
+  i.persistent = 1;
+  return Variant{i, &launch_tcb<PHYS, N, E, NF, NB, DB>};
+}
+
 template <int PHYS, int N, int E, int NF, int NB>
 static Variant make_tc() {
   using C = TCfg<PHYS, N, E, NF, NB>;
@@ -961,6 +994,8 @@ static const std::vector<Variant> &variants();
 #define V_MXP(P, NN, E, PREC, W, PW) make_mixed<P, NN, E, PREC, W, PW>()
 // split-TF32 with the operator in tensor memory: E elements, NF compute warps, NB ring slots
 #define V_TC(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB>()
+// split-BF16 with the operator in tensor memory: DB = double-buffered images and accumulators
+#define V_TCB(P, NN, E, NF, NB, DB) make_tcb<P, NN, E, NF, NB, DB>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -992,7 +1027,8 @@ DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),
               V_PM16G(EUL, 5, 8, 1, 2, 1, 2), V_PIPEFW(EUL, 5, 8, 5, 1, false, 1, 2),
-              V_PIPEFW(EUL, 5, 8, 5, 1, false, 2, 2), V_PIPEFW(EUL, 5, 8, 5, 2, false, 3, 2))
+              V_PIPEFW(EUL, 5, 8, 5, 1, false, 2, 2), V_PIPEFW(EUL, 5, 8, 5, 2, false, 3, 2),
+              V_TCB(EUL, 5, 8, 14, 2, true))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEG(EUL, 6, 8, 1, false, 2, 2), V_PIPEG(EUL, 6, 8, 1, false, 2, 1),
               V_PM16G(EUL, 6, 8, 1, 2, 1, 2), V_PM16G(EUL, 6, 8, 1, 2, 2, 2),
@@ -1001,7 +1037,7 @@ DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEGW(EUL, 6, 8, 5, 1, 1, 2), V_PIPEGW(EUL, 6, 8, 5, 1, 2, 2),
               V_PIPEGW(EUL, 6, 8, 5, 2, 2, 2), V_PIPEGW(EUL, 6, 8, 5, 2, 3, 2),
               V_PIPEGW(EUL, 6, 8, 5, 3, 2, 2), V_PIPEGW(EUL, 6, 8, 5, 3, 3, 2),
-              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 1))
+              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 1), V_TCB(EUL, 6, 8, 14, 2, false))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 // N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB
 DGLM_VARIANTS(EUL, 8, V_SIMT(EUL, 8, 4, 8, 5), V_SIMT(EUL, 8, 4, 6, 5))
