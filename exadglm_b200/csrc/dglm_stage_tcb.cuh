@@ -56,7 +56,7 @@ struct TBCfg {
   static constexpr unsigned TX = 8u * (S_U + S_REC + S_TAU);
   static constexpr int NCOPY = NV + 2;
   static constexpr int NCEN = 7, S_C = E * NV * NCEN;
-  static constexpr int S_R = NV * E * Np;
+  static constexpr int S_R = NV * E * Np;   // rhs (and new state) staging [v][e][i], doubles
   static constexpr int NEB = E / 8, NJB = NFPP / 4;
   static constexpr int VOL_WT = NEB * NG, FACE_WT = NEB * 4 * NJB;
   static constexpr int NTASK = VOL_WT + FACE_WT;
@@ -66,7 +66,7 @@ struct TBCfg {
   static constexpr int GPL = (E * NFF + 31) / 32;
   static constexpr size_t OFF_RING = NBUF * (size_t)B_BYTES;
   static constexpr size_t OFF_R = OFF_RING + 8 * (size_t)NB * S_BUF;
-  static constexpr size_t OFF_C = OFF_R + (4 * (size_t)S_R + 15) / 16 * 16;
+  static constexpr size_t OFF_C = OFF_R + 8 * (size_t)S_R;
   static constexpr size_t OFF_BAR = OFF_C + 8 * 2 * (size_t)S_C;
   // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2],
   // cen[2] (index 0 only for the single-buffered ones)
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
                 NC = C::NC, TC = C::TC, NCOL = C::NCOL, NBUF = C::NBUF;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   double *sRing = reinterpret_cast<double *>(smem_raw + C::OFF_RING);
-  float *sR = reinterpret_cast<float *>(smem_raw + C::OFF_R);
+  double *sR = reinterpret_cast<double *>(smem_raw + C::OFF_R);
   double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
   unsigned long long *full = bars, *empty = bars + NB, *flux_done = bars + 2 * NB,
@@ -263,49 +263,58 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       }
     };
 
-    // epilogue of ring iteration `it` (MMA(it) complete and seen by every
-    // compute warp): this thread's RK register values are requested first;
-    // warps q < NQ read lane quarter q of D (node 32 q + lane) and add the
-    // two parts; then the LSERK update.  The element count is a literal for
-    // full tiles, so the index divisions become multiplications.
-    auto epilogue = [&](int it) {
-      const int db = bsel(it);
+    // D of ring iteration `it` (its MMAs complete) into the rhs staging:
+    // warps NC-4 .. NC-1 read lane quarter warp % 4 (node 32 q + lane) and
+    // add the two parts; the accumulator is then free for the next MMAs
+    auto read_d = [&](int it) {
+      const int q = warp & 3;
+      if (warp < NC - 4 || q >= C::NQ) return;
+      const int db = bsel(it), node = 32 * q + lane;
+      float r[2 * NCOL];
+      const unsigned row = tmem + ((unsigned)(32 * q) << 16) + db * C::D_COLS;
+#pragma unroll
+      for (int c = 0; c < 2 * NCOL; c += 4) tmem_ld4(row + c, r + c);
+      tmem_ld_wait();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&d_free[db]);
+      if (node < Np)
+#pragma unroll
+        for (int c = 0; c < NCOL; c++) sR[c * Np + node] = (double)(r[c] + r[NCOL + c]);
+    };
+    // this thread's RK register and state values of ring iteration `it` (the
+    // ring slot is released once the flux tasks are done, so the update reads
+    // u from global memory, an L2 hit); the element count is a literal for
+    // full tiles, so the index divisions become multiplications
+    double kr[C::KPT], ur[C::KPT];
+    auto load_ku = [&](int it) {
       const long e0 = tile_e0(it);
       const int ne = (int)min((long)E, (long)a.K - e0);
-      double *bU = ring(it);
-      double kr[C::KPT];
-      auto load_k = [&](auto nepc) {
+      auto body = [&](auto nepc) {
         const int nep = nepc;
 #pragma unroll
         for (int r = 0; r < C::KPT; r++) {
           const int x = tid + r * TC;
-          kr[r] = 0.0;
+          kr[r] = ur[r] = 0.0;
           if (!a.rhs_only && x < NV * nep) {
             const int v = x / nep, g = x - v * nep;
             kr[r] = a.kreg[v * vs + e0 * Np + g];
+            ur[r] = a.u_in[v * vs + e0 * Np + g];
           }
         }
       };
       if (ne == E)
-        load_k(std::integral_constant<int, E * Np>{});
+        body(std::integral_constant<int, E * Np>{});
       else
-        load_k(ne * Np);
-      if (warp < C::NQ) {
-        const int node = 32 * warp + lane;
-        float r[2 * NCOL];
-        const unsigned row = tmem + ((unsigned)(32 * warp) << 16) + db * C::D_COLS;
-#pragma unroll
-        for (int c = 0; c < 2 * NCOL; c += 4) tmem_ld4(row + c, r + c);
-        tmem_ld_wait();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&d_free[db]);
-        if (node < Np)
-#pragma unroll
-          for (int c = 0; c < NCOL; c++) sR[c * Np + node] = r[c] + r[NCOL + c];
-      }
-      consumer_sync(TC);
-      auto update = [&](auto nepc) {
+        body(ne * Np);
+    };
+    // LSERK update of ring iteration `it` from the staged rhs (complete:
+    // after a barrier behind read_d); on the last stage the new state goes
+    // to the staging for the fused wave speed
+    auto update = [&](int it) {
+      const long e0 = tile_e0(it);
+      const int ne = (int)min((long)E, (long)a.K - e0);
+      auto body = [&](auto nepc) {
         const int nep = nepc;
 #pragma unroll
         for (int r = 0; r < C::KPT; r++) {
@@ -314,27 +323,27 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
             const int v = x / nep, g = x - v * nep;
             const int si = v * E * Np + g;
             const long gi = v * vs + e0 * Np + g;
-            const double rhs = (double)sR[si];
+            const double rhs = sR[si];
             if (a.rhs_only) {
               a.u_out[gi] = rhs;
             } else {
               const double kn = a.rka * kr[r] + dt * rhs;
-              const double un = bU[si] + a.rkb * kn;
+              const double un = ur[r] + a.rkb * kn;
               a.kreg[gi] = kn;
               a.u_out[gi] = un;
-              if (keep_u) bU[si] = un;
+              if (keep_u) sR[si] = un;
             }
           }
         }
       };
       if (ne == E)
-        update(std::integral_constant<int, E * Np>{});
+        body(std::integral_constant<int, E * Np>{});
       else
-        update(ne * Np);
+        body(ne * Np);
       if (keep_u) {
-        // fused calc_maxv on the new state (divisions as in face_maxv_kernel)
+        // fused calc_maxv on the new state (divisions as in face_maxv_kernel);
+        // metrics and Fscale from the element records in global memory
         consumer_sync(TC);
-        const double *bR = bU + C::S_U + C::S_UP;
         for (int x = tid; x < 4 * E; x += TC) {
           const int f = x / E, e = x - f * E;
           if (e >= ne) continue;
@@ -342,8 +351,8 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
           bool bad = false;
           for (int jj = 0; jj < Nfp; jj++) {
             const int nd = e * Np + sFm[f * Nfp + jj];
-            const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
-                         u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
+            const double u1 = sR[nd], u2 = sR[E * Np + nd], u3 = sR[2 * E * Np + nd],
+                         u4 = sR[3 * E * Np + nd], u5 = sR[4 * E * Np + nd];
             const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
             const double v2 = vx * vx + vy * vy + vz * vz;
             const double pres = (gam - 1) * (u5 - 0.5 * u1 * v2);
@@ -355,22 +364,18 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
           double mv = sqrt(mv2) + sqrt(mc2);
           if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
           a.maxv[(e0 + e) * 4 + f] = mv;
-          const unsigned long long bits = dbits(mv * bR[e * kRecord + 21 + f]);
+          const unsigned long long bits = dbits(mv * __ldg(a.erec + (e0 + e) * kRecord + 21 + f));
           vmax = bits > vmax ? bits : vmax;
         }
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[it % NB]);
-      // the next rewrite of the rhs staging comes after the next iteration's
-      // first barrier
     };
 
     for (int it = 0; ok && it < my_tiles; it++) {
       const int ne = (int)min((long)E, (long)a.K - tile_e0(it));
-      // the tile's data and node-0 terms; with one image set also MMA(it - 1)
-      // done with it (with two, the set's last reader MMA(it - 2) was seen
-      // done in epilogue(it - 2))
+      // the tile's data and node-0 terms; with one image set and accumulator
+      // also MMA(it - 1) done, whose D is read back before the tasks so the
+      // MMAs of this tile can start as soon as its operand is written (with
+      // two, the set's last reader MMA(it - 2) was seen done in iteration it - 1)
       bool w = mbar_wait(&full[it % NB], (it / NB) & 1, lim) &&
                mbar_wait(&cen[it & 1], (it >> 1) & 1, lim);
       if (!DBUF_ && it > 0) w = w && mbar_wait(&mma_done[0], (it - 1) & 1, lim);
@@ -379,6 +384,7 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
         break;
       }
       tc_fence_after();
+      if (!DBUF_ && it > 0) read_d(it - 1);
       unsigned char *sBv = smem_raw + bsel(it) * C::B_BYTES, *sBf = sBv + C::BV_BYTES;
       for (int wt = warp; wt < C::NTASK; wt += NC) {
         if (wt < C::VOL_WT)
@@ -386,25 +392,36 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
         else
           face_task(it, wt - C::VOL_WT, ne, sBf);
       }
+      // operand written; the ring slot is no longer read by this warp
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(&flux_done[bsel(it)]);
+      if (lane == 0) {
+        mbar_arrive(&flux_done[bsel(it)]);
+        mbar_arrive(&empty[it % NB]);
+      }
       if (it > 0) {
+        load_ku(it - 1);
         if (DBUF_) {
           if (!consumer_all(mbar_wait(&mma_done[bsel(it - 1)], bphase(it - 1), lim), TC)) {
             ok = false;
             break;
           }
           tc_fence_after();
+          read_d(it - 1);
         }
-        epilogue(it - 1);
+        consumer_sync(TC);
+        update(it - 1);
       }
     }
     if (ok && my_tiles > 0) {
-      ok = consumer_all(mbar_wait(&mma_done[bsel(my_tiles - 1)], bphase(my_tiles - 1), lim), TC);
+      const int last = my_tiles - 1;
+      load_ku(last);
+      ok = consumer_all(mbar_wait(&mma_done[bsel(last)], bphase(last), lim), TC);
       if (ok) {
         tc_fence_after();
-        epilogue(my_tiles - 1);
+        read_d(last);
+        consumer_sync(TC);
+        update(last);
       }
     }
   } else if (warp == C::PROD_WARP) {
@@ -495,8 +512,7 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
     for (int it = 0; ok && it < my_tiles; it++) {
       const int b = bsel(it);
       bool w = mbar_wait(&flux_done[b], bphase(it), lim);
-      if (__all_sync(0xffffffffu, w) && it + 1 < my_tiles) w = centers_of(it + 1);
-      // the accumulator: read back by epilogue(it - NBUF)
+      // the accumulator: read back by read_d(it - NBUF)
       if (w && it >= NBUF) w = mbar_wait(&d_free[b], bphase(it - NBUF), lim);
       if (!__all_sync(0xffffffffu, w)) {
         ok = false;
@@ -523,6 +539,11 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       }
       __syncwarp();
       nm++;
+      // the next tile's node-0 terms while the tensor cores work
+      if (it + 1 < my_tiles && !centers_of(it + 1)) {
+        ok = false;
+        break;
+      }
     }
     // the MMAs issued (and their barrier arrivals) are complete before
     // tensor and shared memory are released, on expiry too
