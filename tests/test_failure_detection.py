@@ -99,14 +99,15 @@ def _rel(a, b):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,kind", [("fp64", "pipe-dmma"), ("tf32x3", "tc-tmem")])
-def test_bounded_waits_report_expiry(precision, kind):
+@pytest.mark.parametrize("precision,kind,N", [("fp64", "pipe-dmma", 4), ("tf32x3", "tc-tmem", 4),
+                                             ("bf16x3", "tc-tmem-bf16", 6)])
+def test_bounded_waits_report_expiry(precision, kind, N):
     """Waits bounded to one cycle expire; the step reports DGLM_ERR_CUDA and
     the solver recovers once the bound is restored and a state is set."""
-    prob = P.euler_sine(n=6, N=4, noise=1e-3, seed=4)       # 1,296 tets: 81 tiles of 16
+    prob = P.euler_sine(n=6, N=N, noise=1e-3, seed=4)       # 1,296 tets: 162 tiles of 8
     ref, _, _, _ = oracle.Oracle(prob).run(3)
-    var = [v for v, d in capi.variants("euler", 4, precision) if d.startswith(kind)][0]
-    tol = 1e-12 if precision == "fp64" else 1e-6
+    var = [v for v, d in capi.variants("euler", N, precision) if d.startswith(kind)][0]
+    tol = 1e-12 if precision == "fp64" else 1e-6 if precision == "tf32x3" else 1e-5
     s = capi.Solver(prob, precision=precision, variant=var)
     s.set_wait_limit(1)
     s.step(1)

@@ -4,8 +4,8 @@ state (the precision pattern's bar: <= 1e-6 after 200 steps).
 
 * Euler N=4 on 32^3 x 6 = 196,608 tets, CFL 0.4: TF32x3 (the handle's
   default variant and every tensor-memory variant) <= 5e-7.
-* Euler N=6 on 48^3 x 6 = 663,552 tets, CFL 0.4: TF32x3 and BF16x6
-  (default variants) <= 1e-6.
+* Euler N=6 on 48^3 x 6 = 663,552 tets, CFL 0.4: TF32x3, BF16x6 and BF16x3
+  (default variants, and the BF16 tensor-memory kernel) <= 1e-6.
 
 The split operands are centred on each element's node-0 flux, which leaves
 the right-hand side unchanged and shrinks the values the tensor cores see."""
@@ -48,8 +48,10 @@ def test_euler_n4_196608_tets():
 def test_euler_n6_663552_tets():
     prob = P.euler_sine(n=48, N=6, cfl=0.4)
     ref, _ = run(prob, "fp64")
-    for prec in ("tf32x3", "bf16x6"):
-        u, desc = run(prob, prec)
+    cases = [("tf32x3", None), ("bf16x6", None), ("bf16x3", None)] + \
+        [("bf16x3", v) for v, d in variants("euler", 6, "bf16x3") if d.startswith("tc-")]
+    for prec, var in cases:
+        u, desc = run(prob, prec, var)
         err = rel(u, ref)
         per_field = [rel(u[v], ref[v]) for v in range(prob.nvar)]
         print(f"N=6 K={prob.K} {prec} {desc}: {STEPS}-step rel L2 {err:.3e}, per field "
