@@ -300,6 +300,7 @@ def mixed_section(a, p, stream, fp64_ms_per_step):
     """Mixed-precision stage kernels on the same workload: throughput, speed-up
     over the FP64 path and relative L2 against FP64 after --accuracy-steps."""
     import numpy as np
+    import torch
     from exadglm_b200.capi import Solver, variants
     S = a.accuracy_steps
     ref = Solver(p, precision="fp64")
@@ -328,8 +329,11 @@ def mixed_section(a, p, stream, fp64_ms_per_step):
         ms = e0.elapsed_time(e1) / a.steps
         stage_ms = stage_alone_ms(s, stream)
         s.set_state(p.u0)
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
         s.step(S)
         s.sync()
+        clk = clocks.stop()
         um = s.get_state()
         per_field = [float(np.linalg.norm(um[v] - u64[v]) / np.linalg.norm(u64[v]))
                      for v in range(p.nvar)]
@@ -342,6 +346,7 @@ def mixed_section(a, p, stream, fp64_ms_per_step):
             "rel_l2_per_field": per_field,
             "kernel": variants("euler", p.N)[s.variant()],
             "roofline": hbm_roofline(p, stage_ms, variants("euler", p.N)[s.variant()]),
+            "clocks_during_accuracy_run": clk,
         }
         s.close()
     return out
@@ -582,6 +587,7 @@ def precision_section(a, stream):
     of each mixed mode from the same state; relative L2 against FP64 per field,
     and ms per step of each."""
     import numpy as np
+    import torch
     from exadglm_b200 import problem as P
     from exadglm_b200.capi import Solver, variants
     p6 = P.euler_sine(n=a.precision_n, N=6, cfl=0.4)
@@ -595,15 +601,18 @@ def precision_section(a, stream):
         s.sync()
         s.set_state(p6.u0)
         e0, e1 = _events(stream)
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
         e0.record(stream)
         s.step(S)
         e1.record(stream)
         e1.synchronize()
         s.sync()
+        clk = clocks.stop()
         u = s.get_state()
         ms = e0.elapsed_time(e1) / S
         row = {"ms_per_step": ms, "kernel": variants("euler", 6)[s.variant()],
-               "value": dof_stages_per_step(p6) / (ms * 1e-3), "unit": UNIT}
+               "value": dof_stages_per_step(p6) / (ms * 1e-3), "unit": UNIT, "clocks": clk}
         if ref is None:
             ref = u
         else:

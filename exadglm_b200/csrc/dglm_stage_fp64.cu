@@ -1022,7 +1022,7 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
               V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2),
-              V_TC(EUL, 4, 8, 14, 3))
+              V_TC(EUL, 4, 8, 14, 3), V_TCB(EUL, 4, 8, 14, 2, true))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),
