@@ -344,28 +344,39 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
         // fused calc_maxv on the new state (divisions as in face_maxv_kernel);
         // metrics and Fscale from the element records in global memory
         consumer_sync(TC);
-        for (int x = tid; x < 4 * E; x += TC) {
-          const int f = x / E, e = x - f * E;
-          if (e >= ne) continue;
-          double mv2 = 0.0, mc2 = 0.0;
-          bool bad = false;
-          for (int jj = 0; jj < Nfp; jj++) {
-            const int nd = e * Np + sFm[f * Nfp + jj];
+        // one lane per face node, LPF lanes per face, maxima by shuffles
+        constexpr int LPF = Nfp <= 16 ? 16 : 32, FPW = 32 / LPF;
+        const int jn = lane % LPF;
+        for (int f0 = warp * FPW; f0 < 4 * E; f0 += NC * FPW) {
+          const int fx = f0 + lane / LPF, f = fx / E, e = fx - f * E;
+          const bool on = fx < 4 * E && e < ne;
+          double v2 = 0.0, c2 = 0.0;
+          int bad = 0;
+          if (on && jn < Nfp) {
+            const int nd = e * Np + sFm[f * Nfp + jn];
             const double u1 = sR[nd], u2 = sR[E * Np + nd], u3 = sR[2 * E * Np + nd],
                          u4 = sR[3 * E * Np + nd], u5 = sR[4 * E * Np + nd];
             const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-            const double v2 = vx * vx + vy * vy + vz * vz;
+            v2 = vx * vx + vy * vy + vz * vz;
             const double pres = (gam - 1) * (u5 - 0.5 * u1 * v2);
-            const double c2 = fabs(gam * pres / u1);
-            mv2 = v2 > mv2 ? v2 : mv2;
-            mc2 = c2 > mc2 ? c2 : mc2;
-            bad |= (v2 != v2) || (c2 != c2);
+            c2 = fabs(gam * pres / u1);
+            bad = (v2 != v2) || (c2 != c2);
           }
-          double mv = sqrt(mv2) + sqrt(mc2);
-          if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
-          a.maxv[(e0 + e) * 4 + f] = mv;
-          const unsigned long long bits = dbits(mv * __ldg(a.erec + (e0 + e) * kRecord + 21 + f));
-          vmax = bits > vmax ? bits : vmax;
+#pragma unroll
+          for (int o = LPF / 2; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, v2, o);
+            const double oc = __shfl_xor_sync(0xffffffffu, c2, o);
+            v2 = ov > v2 ? ov : v2;
+            c2 = oc > c2 ? oc : c2;
+            bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+          }
+          if (on && jn == 0) {
+            double mv = sqrt(v2) + sqrt(c2);
+            if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+            a.maxv[(e0 + e) * 4 + f] = mv;
+            const unsigned long long bits = dbits(mv * __ldg(a.erec + (e0 + e) * kRecord + 21 + f));
+            vmax = bits > vmax ? bits : vmax;
+          }
         }
       }
     };
