@@ -343,6 +343,20 @@ dglm_status upload_operator_layout(dglm_handle *h) {
                     "operator upload");
 }
 
+// Whether the step's wave-speed maximum runs as its own kernel after the
+// fifth stage (the tensor-memory stage kernels: inside them it costs more
+// than the standalone face_maxv_kernel, whose result is the same bit for bit).
+bool separate_maxv(const dglm_handle *h) {
+  return h->d.physics == DGLM_EULER &&
+         (h->vinfo.mode == MODE_TC || h->vinfo.mode == MODE_TCB);
+}
+
+// Kernel launches of one step: step_begin, tau (Euler), five stages, the
+// separate wave-speed maximum where it applies, step_end.
+int step_launches(const dglm_handle *h) {
+  return (h->d.physics == DGLM_ADVECTION ? 7 : 8) + (separate_maxv(h) ? 1 : 0);
+}
+
 }  // namespace
 
 // One LSERK step whose stage k reads in[k] and writes out[k] (for the
@@ -354,10 +368,14 @@ dglm_status dglm::issue_step_ptrs(dglm_handle *h, const double *const *in, doubl
   cudaError_t e = launch_step_begin(h->d.N, h->d.cfl, h->d.tmax, frozen, h->sc, h->dt_hist, s);
   if (e == cudaSuccess && !frozen)
     e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv, h->tau, s);
+  const bool sep = separate_maxv(h);
   for (int st = 0; st < 5 && e == cudaSuccess; st++) {
     StageArgs a = stage_args(h, in[st], out[st], st);
+    if (sep) a.last_stage = 0;
     e = launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, s);
   }
+  if (e == cudaSuccess && sep)
+    e = launch_face_maxv(h->d.physics, h->d.N, stage_args(h, out[4], nullptr, -1), -1, s);
   if (e == cudaSuccess) e = launch_step_end(h->sc, s);
   return cuda_check(e, "step launch");
 }
@@ -370,11 +388,17 @@ dglm_status issue_step(dglm_handle *h, int cur, cudaStream_t s) {
   cudaError_t e = launch_step_begin(h->d.N, h->d.cfl, h->d.tmax, frozen, h->sc, h->dt_hist, s);
   if (e == cudaSuccess && !frozen)
     e = launch_tau(h->d.K, h->d.tau_scale, h->vmapF, h->maxv, h->tau, s);
+  const bool sep = separate_maxv(h);
   for (int st = 0; st < 5 && e == cudaSuccess; st++) {
     const int in = (cur + st) & 1;
     StageArgs a = stage_args(h, h->u[in], h->u[in ^ 1], st);
+    if (sep) a.last_stage = 0;
     e = launch_stage_fp64(h->d.physics, h->d.N, h->variant, a, s);
   }
+  // after five stages the new state is in u[cur ^ 1]
+  if (e == cudaSuccess && sep)
+    e = launch_face_maxv(h->d.physics, h->d.N, stage_args(h, h->u[cur ^ 1], nullptr, -1), -1,
+                         s);
   if (e == cudaSuccess) e = launch_step_end(h->sc, s);
   return cuda_check(e, "step launch");
 }
@@ -841,14 +865,14 @@ dglm_status dglm::run_steps(dglm_handle *h, int nsteps) {
       if (!ok) {
         dglm_status s2 = issue_step(h, c, h->stream);
         if (s2 != DGLM_OK) return s2;
-        h->launches += h->d.physics == DGLM_ADVECTION ? 7 : 8;
+        h->launches += step_launches(h);
         h->cur ^= 1;
         continue;
       }
     }
     cudaError_t e = cudaGraphLaunch(h->graph[c], h->stream);
     if (e != cudaSuccess) return cuda_check(e, "dglm_step: graph launch");
-    h->launches += h->d.physics == DGLM_ADVECTION ? 7 : 8;
+    h->launches += step_launches(h);
     h->cur ^= 1;
   }
   return DGLM_OK;

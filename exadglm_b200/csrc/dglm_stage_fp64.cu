@@ -659,44 +659,65 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 #include "dglm_stage_tc.cuh"
 #include "dglm_stage_tcb.cuh"
 
-// Standalone calc_maxv (initial state, advection velocity): maxv per face and
-// a device-wide max of maxv*Fscale into sc->acc[slot].
+// Standalone calc_maxv (initial state, advection velocity, and the end of a
+// step for the stage kernels that do not fuse it): maxv per face and a
+// device-wide max of maxv*Fscale into sc->acc[slot] (slot < 0: the slot the
+// fused copy would use, acc[parity ^ 1]).  One lane per face node, LPF lanes
+// per face, the face maxima by shuffles (max is exact, so the result does not
+// depend on the order); divisions as in the reference's calc_maxv.
 template <int PHYS, int N>
 __global__ void face_maxv_kernel(const StageArgs a, int slot) {
   constexpr int Np = np_of(N), Nfp = nfp_of(N);
+  constexpr int LPF = Nfp <= 16 ? 16 : 32, FPW = 32 / LPF;
   __shared__ unsigned long long sMax[32];
   unsigned long long local = 0ull;
   const long nF = 4L * a.K;
-  for (long gf = blockIdx.x * (long)blockDim.x + threadIdx.x; gf < nF;
-       gf += (long)gridDim.x * blockDim.x) {
-    const long e = gf / 4;
-    const int f = (int)(gf % 4);
-    double mv2 = 0.0, mc2 = 0.0;
-    bool bad = false;
-    for (int j = 0; j < Nfp; j++) {
+  const int lane = threadIdx.x & 31, jn = lane % LPF;
+  const long warps = (long)gridDim.x * (blockDim.x >> 5);
+  // warp-uniform loop over groups of FPW faces
+  for (long w = blockIdx.x * (long)(blockDim.x >> 5) + (threadIdx.x >> 5); w * FPW < nF;
+       w += warps) {
+    const long gf = w * FPW + lane / LPF;
+    const bool on = gf < nF;
+    double v2 = 0.0, c2 = 0.0;
+    int bad = 0;
+    // nodes jn, jn + LPF, ... of the face (one of them below order 7)
+    for (int j = jn; on && j < Nfp; j += LPF) {
+      const long e = gf / 4;
+      const int f = (int)(gf % 4);
       const long nd = e * Np + a.Fmask[f * Nfp + j];
+      double w2, d2 = 0.0;
       if (PHYS == EUL) {
         const double u1 = a.u_in[nd], u2 = a.u_in[a.vs + nd], u3 = a.u_in[2 * a.vs + nd],
                      u4 = a.u_in[3 * a.vs + nd], u5 = a.u_in[4 * a.vs + nd];
         const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-        const double v2 = vx * vx + vy * vy + vz * vz;
-        mv2 = v2 > mv2 ? v2 : mv2;
-        const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-        const double c2 = fabs(a.gamma * pres / u1);
-        mc2 = c2 > mc2 ? c2 : mc2;
-        bad |= (v2 != v2) || (c2 != c2);
+        w2 = vx * vx + vy * vy + vz * vz;
+        const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * w2);
+        d2 = fabs(a.gamma * pres / u1);
+        bad |= (w2 != w2) || (d2 != d2);
       } else {
         const double vx = a.vel[nd], vy = a.vel[a.vs + nd], vz = a.vel[2 * a.vs + nd];
-        const double v2 = vx * vx + vy * vy + vz * vz;
-        mv2 = v2 > mv2 ? v2 : mv2;
-        bad |= (v2 != v2);
+        w2 = vx * vx + vy * vy + vz * vz;
+        bad |= (w2 != w2);
       }
+      v2 = w2 > v2 ? w2 : v2;
+      c2 = d2 > c2 ? d2 : c2;
     }
-    double mv = (PHYS == EUL) ? sqrt(mv2) + sqrt(mc2) : sqrt(mv2);
-    if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
-    a.maxv[gf] = mv;
-    const unsigned long long b = dbits(mv * a.fscale[gf]);
-    local = b > local ? b : local;
+#pragma unroll
+    for (int o = LPF / 2; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, v2, o);
+      const double oc = __shfl_xor_sync(0xffffffffu, c2, o);
+      v2 = ov > v2 ? ov : v2;
+      c2 = oc > c2 ? oc : c2;
+      bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if (on && jn == 0) {
+      double mv = (PHYS == EUL) ? sqrt(v2) + sqrt(c2) : sqrt(v2);
+      if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+      a.maxv[gf] = mv;
+      const unsigned long long b = dbits(mv * a.fscale[gf]);
+      local = b > local ? b : local;
+    }
   }
   local = warp_max_bits(local);
   if ((threadIdx.x & 31) == 0) sMax[threadIdx.x >> 5] = local;
@@ -704,7 +725,7 @@ __global__ void face_maxv_kernel(const StageArgs a, int slot) {
   if (threadIdx.x < 32) {
     unsigned long long v = threadIdx.x < (blockDim.x + 31) / 32 ? sMax[threadIdx.x] : 0ull;
     v = warp_max_bits(v);
-    if (threadIdx.x == 0) atomicMax(&a.sc->acc[slot], v);
+    if (threadIdx.x == 0) atomicMax(&a.sc->acc[slot >= 0 ? slot : a.sc->parity ^ 1], v);
   }
 }
 
@@ -1097,8 +1118,9 @@ cudaError_t launch_stage_fp64(int physics, int N, int variant, const StageArgs &
 
 template <int PHYS, int N>
 static cudaError_t launch_maxv_one(const StageArgs &a, int slot, cudaStream_t s) {
-  const long nF = 4L * a.K;
-  int blocks = (int)((nF + 255) / 256);
+  // 8 warps per block, FPW faces per warp
+  const long nF = 4L * a.K, fpb = 8L * (nfp_of(N) <= 16 ? 2 : 1);
+  int blocks = (int)((nF + fpb - 1) / fpb);
   if (blocks > 148 * 16) blocks = 148 * 16;
   face_maxv_kernel<PHYS, N><<<blocks, 256, 0, s>>>(a, slot);
   return cudaGetLastError();
