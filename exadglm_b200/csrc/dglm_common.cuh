@@ -107,6 +107,21 @@ __device__ __forceinline__ unsigned long long warp_max_bits(unsigned long long b
   return b;
 }
 
+// |v|^2 and the squared sound speed of one node's state, for the wave-speed
+// maxima of the solver's steps (the fused copies in the stage kernels and the
+// standalone face_maxv_kernel share it, so dt does not depend on which kernel
+// computed maxv and a restarted run repeats the original bit for bit).  One
+// division by rho, as a reciprocal; the per-kernel calc_maxv entry points
+// below keep the reference's three divisions.
+__device__ __forceinline__ void node_speeds(double gamma, double u1, double u2, double u3,
+                                            double u4, double u5, double &v2, double &c2) {
+  const double ir = 1.0 / u1;
+  const double vx = u2 * ir, vy = u3 * ir, vz = u4 * ir;
+  v2 = vx * vx + vy * vy + vz * vz;
+  const double pres = (gamma - 1) * (u5 - 0.5 * u1 * v2);
+  c2 = fabs(gamma * pres * ir);
+}
+
 // calc_maxv of face fi of element e (euler_nopad_dglm.cu:7-76,
 // advec_nopad_dglm.cu:7-62): the largest |v| over the face nodes plus, for
 // Euler, the largest sound speed, with the reference's divisions by rho.

@@ -344,12 +344,9 @@ dglm_status upload_operator_layout(dglm_handle *h) {
 }
 
 // Whether the step's wave-speed maximum runs as its own kernel after the
-// fifth stage (the tensor-memory stage kernels: inside them it costs more
-// than the standalone face_maxv_kernel, whose result is the same bit for bit).
-bool separate_maxv(const dglm_handle *h) {
-  return h->d.physics == DGLM_EULER &&
-         (h->vinfo.mode == MODE_TC || h->vinfo.mode == MODE_TCB);
-}
+// fifth stage (Euler): inside the persistent stage kernels it costs more than
+// the standalone face_maxv_kernel, whose result is the same bit for bit.
+bool separate_maxv(const dglm_handle *h) { return h->d.physics == DGLM_EULER; }
 
 // Kernel launches of one step: step_begin, tau (Euler), five stages, the
 // separate wave-speed maximum where it applies, step_end.

@@ -627,13 +627,9 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
       const double u1 = sU[(0 * Np + nd) * EP + e], u2 = sU[(1 * Np + nd) * EP + e],
                    u3 = sU[(2 * Np + nd) * EP + e], u4 = sU[(3 * Np + nd) * EP + e],
                    u5 = sU[(4 * Np + nd) * EP + e];
-      // divisions as in face_maxv_kernel, so dt does not depend on which
-      // kernel computed maxv (a restarted run repeats the original bit for bit)
-      const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-      const double v2 = vx * vx + vy * vy + vz * vz;
+      double v2, c2;
+      node_speeds(a.gamma, u1, u2, u3, u4, u5, v2, c2);   // as in face_maxv_kernel
       mv2 = v2 > mv2 ? v2 : mv2;
-      const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-      const double c2 = fabs(a.gamma * pres / u1);
       mc2 = c2 > mc2 ? c2 : mc2;
       bad |= (v2 != v2) || (c2 != c2);
     }
@@ -662,68 +658,88 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 // Standalone calc_maxv (initial state, advection velocity, and the end of a
 // step for the stage kernels that do not fuse it): maxv per face and a
 // device-wide max of maxv*Fscale into sc->acc[slot] (slot < 0: the slot the
-// fused copy would use, acc[parity ^ 1]).  One lane per face node, LPF lanes
-// per face, the face maxima by shuffles (max is exact, so the result does not
-// depend on the order); divisions as in the reference's calc_maxv.
+// fused copy would use, acc[parity ^ 1]).  One warp per element: its nodes'
+// |v|^2 and c^2 (node_speeds) from coalesced loads into shared memory, then
+// LPF lanes per face take the face maxima by
+// shuffles (max is exact, so the result does not depend on the order).
 template <int PHYS, int N>
-__global__ void face_maxv_kernel(const StageArgs a, int slot) {
-  constexpr int Np = np_of(N), Nfp = nfp_of(N);
-  constexpr int LPF = Nfp <= 16 ? 16 : 32, FPW = 32 / LPF;
-  __shared__ unsigned long long sMax[32];
-  unsigned long long local = 0ull;
-  const long nF = 4L * a.K;
-  const int lane = threadIdx.x & 31, jn = lane % LPF;
-  const long warps = (long)gridDim.x * (blockDim.x >> 5);
-  // warp-uniform loop over groups of FPW faces
-  for (long w = blockIdx.x * (long)(blockDim.x >> 5) + (threadIdx.x >> 5); w * FPW < nF;
-       w += warps) {
-    const long gf = w * FPW + lane / LPF;
-    const bool on = gf < nF;
-    double v2 = 0.0, c2 = 0.0;
-    int bad = 0;
-    // nodes jn, jn + LPF, ... of the face (one of them below order 7)
-    for (int j = jn; on && j < Nfp; j += LPF) {
-      const long e = gf / 4;
-      const int f = (int)(gf % 4);
-      const long nd = e * Np + a.Fmask[f * Nfp + j];
-      double w2, d2 = 0.0;
-      if (PHYS == EUL) {
-        const double u1 = a.u_in[nd], u2 = a.u_in[a.vs + nd], u3 = a.u_in[2 * a.vs + nd],
-                     u4 = a.u_in[3 * a.vs + nd], u5 = a.u_in[4 * a.vs + nd];
-        const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-        w2 = vx * vx + vy * vy + vz * vz;
-        const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * w2);
-        d2 = fabs(a.gamma * pres / u1);
-        bad |= (w2 != w2) || (d2 != d2);
-      } else {
-        const double vx = a.vel[nd], vy = a.vel[a.vs + nd], vz = a.vel[2 * a.vs + nd];
-        w2 = vx * vx + vy * vy + vz * vz;
-        bad |= (w2 != w2);
-      }
-      v2 = w2 > v2 ? w2 : v2;
-      c2 = d2 > c2 ? d2 : c2;
-    }
+__global__ void __launch_bounds__(256) face_maxv_kernel(const StageArgs a, int slot) {
+  constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
+  constexpr int LPF = Nfp <= 16 ? 16 : 32, FPW = 32 / LPF, WPB = 8;
+  __shared__ double sV[WPB][Np], sC[WPB][Np];
+  __shared__ int sFm[NFF];
+  __shared__ unsigned long long sMax[WPB];
+  for (int i = threadIdx.x; i < NFF; i += blockDim.x) sFm[i] = a.Fmask[i];
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, jn = lane % LPF;
+  // node values of this warp's next element, requested one element ahead
+  constexpr int NI = (Np + 31) / 32, NQ = PHYS == EUL ? 5 : 3;
+  const double *src = PHYS == EUL ? a.u_in : a.vel;
+  double q[NI][NQ];
+  auto fetch = [&](long e) {
 #pragma unroll
-    for (int o = LPF / 2; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, v2, o);
-      const double oc = __shfl_xor_sync(0xffffffffu, c2, o);
-      v2 = ov > v2 ? ov : v2;
-      c2 = oc > c2 ? oc : c2;
-      bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    for (int r = 0; r < NI; r++) {
+      const int i = lane + 32 * r;
+#pragma unroll
+      for (int v = 0; v < NQ; v++)
+        q[r][v] = (e < a.K && i < Np) ? src[v * a.vs + e * Np + i] : 1.0;
     }
-    if (on && jn == 0) {
-      double mv = (PHYS == EUL) ? sqrt(v2) + sqrt(c2) : sqrt(v2);
-      if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
-      a.maxv[gf] = mv;
-      const unsigned long long b = dbits(mv * a.fscale[gf]);
-      local = b > local ? b : local;
+  };
+  unsigned long long local = 0ull;
+  const long stride = (long)gridDim.x * WPB;
+  fetch(blockIdx.x * (long)WPB + w);
+  for (long e = blockIdx.x * (long)WPB + w; e < a.K; e += stride) {
+#pragma unroll
+    for (int r = 0; r < NI; r++) {
+      const int i = lane + 32 * r;
+      double v2, c2 = 0.0;
+      if (PHYS == EUL)
+        node_speeds(a.gamma, q[r][0], q[r][1], q[r][2], q[r][3], q[r][4], v2, c2);
+      else
+        v2 = q[r][0] * q[r][0] + q[r][1] * q[r][1] + q[r][2] * q[r][2];
+      if (i < Np) {
+        sV[w][i] = v2;
+        sC[w][i] = c2;
+      }
     }
+    fetch(e + stride);
+    __syncwarp();
+#pragma unroll
+    for (int f0 = 0; f0 < 4; f0 += FPW) {
+      const int f = f0 + lane / LPF;
+      double v2 = 0.0, c2 = 0.0;
+      int bad = 0;
+      for (int j = jn; j < Nfp; j += LPF) {
+        const int nd = sFm[f * Nfp + j];
+        const double w2 = sV[w][nd], d2 = sC[w][nd];
+        bad |= (w2 != w2) || (d2 != d2);
+        v2 = w2 > v2 ? w2 : v2;
+        c2 = d2 > c2 ? d2 : c2;
+      }
+#pragma unroll
+      for (int o = LPF / 2; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v2, o);
+        const double oc = __shfl_xor_sync(0xffffffffu, c2, o);
+        v2 = ov > v2 ? ov : v2;
+        c2 = oc > c2 ? oc : c2;
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+      }
+      if (jn == 0) {
+        const long gf = e * 4 + f;
+        double mv = (PHYS == EUL) ? sqrt(v2) + sqrt(c2) : sqrt(v2);
+        if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+        a.maxv[gf] = mv;
+        const unsigned long long b = dbits(mv * a.fscale[gf]);
+        local = b > local ? b : local;
+      }
+    }
+    __syncwarp();
   }
   local = warp_max_bits(local);
-  if ((threadIdx.x & 31) == 0) sMax[threadIdx.x >> 5] = local;
+  if (lane == 0) sMax[w] = local;
   __syncthreads();
   if (threadIdx.x < 32) {
-    unsigned long long v = threadIdx.x < (blockDim.x + 31) / 32 ? sMax[threadIdx.x] : 0ull;
+    unsigned long long v = threadIdx.x < WPB ? sMax[threadIdx.x] : 0ull;
     v = warp_max_bits(v);
     if (threadIdx.x == 0) atomicMax(&a.sc->acc[slot >= 0 ? slot : a.sc->parity ^ 1], v);
   }
@@ -1118,10 +1134,9 @@ cudaError_t launch_stage_fp64(int physics, int N, int variant, const StageArgs &
 
 template <int PHYS, int N>
 static cudaError_t launch_maxv_one(const StageArgs &a, int slot, cudaStream_t s) {
-  // 8 warps per block, FPW faces per warp
-  const long nF = 4L * a.K, fpb = 8L * (nfp_of(N) <= 16 ? 2 : 1);
-  int blocks = (int)((nF + fpb - 1) / fpb);
-  if (blocks > 148 * 16) blocks = 148 * 16;
+  // 8 warps per block, one element per warp at a time
+  int blocks = (int)((a.K + 7) / 8);
+  if (blocks > 148 * 8) blocks = 148 * 8;
   face_maxv_kernel<PHYS, N><<<blocks, 256, 0, s>>>(a, slot);
   return cudaGetLastError();
 }

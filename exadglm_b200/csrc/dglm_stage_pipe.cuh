@@ -580,12 +580,9 @@ __global__ void __launch_bounds__(
           const int nd = e * Np + sFm[f * Nfp + j];
           const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
                        u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
-          // divisions as in face_maxv_kernel, so dt does not depend on which
-          // kernel computed maxv (a restarted run repeats the original bit for bit)
-          const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-          v2 = vx * vx + vy * vy + vz * vz;
-          const double pres = (a.gamma - 1) * (u5 - 0.5 * u1 * v2);
-          c2 = fabs(a.gamma * pres / u1);
+          // as in face_maxv_kernel, so dt does not depend on which kernel
+          // computed maxv (a restarted run repeats the original bit for bit)
+          node_speeds(a.gamma, u1, u2, u3, u4, u5, v2, c2);
         }
         sW[2 * it] = v2;
         sW[2 * it + 1] = c2;

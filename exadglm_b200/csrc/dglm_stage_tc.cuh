@@ -408,8 +408,8 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
         update(ne * Np);
       if (keep_u) {
         // fused calc_maxv on the new state: per face, max |v|^2 and c^2 over
-        // its nodes (divisions as in face_maxv_kernel, so dt does not depend
-        // on which kernel computed maxv)
+        // its nodes (node_speeds, as in face_maxv_kernel, so dt does not
+        // depend on which kernel computed maxv)
         consumer_sync(TC);
         const double *bR = bU + C::S_U + C::S_UP;
         // one lane per face node, LPF lanes per face, maxima by shuffles
@@ -424,10 +424,7 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
             const int nd = e * Np + sFm[f * Nfp + jn];
             const double u1 = bU[nd], u2 = bU[E * Np + nd], u3 = bU[2 * E * Np + nd],
                          u4 = bU[3 * E * Np + nd], u5 = bU[4 * E * Np + nd];
-            const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-            v2 = vx * vx + vy * vy + vz * vz;
-            const double pres = (gam - 1) * (u5 - 0.5 * u1 * v2);
-            c2 = fabs(gam * pres / u1);
+            node_speeds(gam, u1, u2, u3, u4, u5, v2, c2);
             bad = (v2 != v2) || (c2 != c2);
           }
 #pragma unroll

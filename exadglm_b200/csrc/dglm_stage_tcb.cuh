@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       else
         body(ne * Np);
       if (keep_u) {
-        // fused calc_maxv on the new state (divisions as in face_maxv_kernel);
+        // fused calc_maxv on the new state (node_speeds, as in face_maxv_kernel);
         // metrics and Fscale from the element records in global memory
         consumer_sync(TC);
         // one lane per face node, LPF lanes per face, maxima by shuffles
@@ -356,10 +356,7 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
             const int nd = e * Np + sFm[f * Nfp + jn];
             const double u1 = sR[nd], u2 = sR[E * Np + nd], u3 = sR[2 * E * Np + nd],
                          u4 = sR[3 * E * Np + nd], u5 = sR[4 * E * Np + nd];
-            const double vx = u2 / u1, vy = u3 / u1, vz = u4 / u1;
-            v2 = vx * vx + vy * vy + vz * vz;
-            const double pres = (gam - 1) * (u5 - 0.5 * u1 * v2);
-            c2 = fabs(gam * pres / u1);
+            node_speeds(gam, u1, u2, u3, u4, u5, v2, c2);
             bad = (v2 != v2) || (c2 != c2);
           }
 #pragma unroll

@@ -61,8 +61,9 @@ def test_ensemble_pinned_overlap_and_reuse():
         assert bad == -1
         for i in range(len(states)):
             np.testing.assert_array_equal(hout[i].numpy(), ref[i], err_msg=f"member {i}")
-    # per member: finite check, wave speeds, then 8 kernels per Euler step
-    assert s.kernel_launches() == len(states) * (2 + 8 * 3)
+    # per member: finite check, wave speeds, then 9 kernels per Euler step
+    # (begin, tau, five stages, wave speeds, end)
+    assert s.kernel_launches() == len(states) * (2 + 9 * 3)
     s.step(2)
     s.sync()
     s.set_state(states[-1])
