@@ -109,24 +109,31 @@ def variant_shape(desc):
 
 def read_traffic(desc, K):
     """Per-launch DRAM bytes of the stage kernel variant `desc` on a K-element
-    mesh, from the committed ncu summary (profiles/stage_traffic.txt: lines
-    '<K> <bytes_per_launch> <variant shape>'); None when no capture of that
-    variant at that size is recorded."""
+    mesh, from the committed ncu summaries (profiles/stage_traffic.txt: lines
+    '<K> <bytes_per_launch> <variant shape>').  A capture on a smaller mesh of
+    the same variant is scaled by K (these kernels stream each element once,
+    so their traffic grows in proportion; DESIGN.md gives the check).  None
+    when the variant has no capture."""
     path = os.path.join(ROOT, "profiles", "stage_traffic.txt")
     if not os.path.exists(path):
         return None
     want = variant_shape(desc)
+    scaled = None
     with open(path) as f:
         for line in f:
             if line.startswith("#") or not line.strip():
                 continue
             parts = line.split(None, 2)
-            if len(parts) == 3 and parts[0] == str(K) and parts[2].strip() == want:
-                try:
-                    return float(parts[1])
-                except ValueError:
-                    return None
-    return None
+            if len(parts) != 3 or parts[2].strip() != want:
+                continue
+            try:
+                k0, b0 = int(parts[0]), float(parts[1])
+            except ValueError:
+                continue
+            if k0 == K:
+                return b0
+            scaled = b0 * K / k0
+    return scaled
 
 
 class ClockSampler:
