@@ -49,9 +49,10 @@
 //               committed to mma_done[t%2].
 //   compute     per tile t: loads of tile t-1's RK register values, the
 //               volume and face flux tasks of t into image set t%2, then the
-//               epilogue of t-1: the wait for MMA(t-1); warps 0..3 read
-//               D[(t-1)%2] (one lane quarter each) and add the parts into the
-//               rhs staging; all compute warps do the LSERK update with
+//               epilogue of t-1: the wait for MMA(t-1); warps NC-4 .. NC-1
+//               (three of which carry one flux task, not two) read D[(t-1)%2]
+//               (lane quarter warp % 4) and add the parts into the rhs
+//               staging; all compute warps do the LSERK update with
 //               coalesced stores.
 // The tensor cores work on tile t while the compute warps finish t-1 and
 // start t+1.  Every wait is bounded; on expiry a warp sets flag bit 2, waits
@@ -113,7 +114,7 @@ struct TCfg {
   static_assert(E % 8 == 0 && MN <= 256, "MMA N for M = 128");
   static_assert(2 * NPQ <= 32, "both operator parts of a quarter's nodes fit its 32 lanes");
   static_assert(2 * D_COLS + KT <= TMEM_COLS, "accumulators and operator fit tensor memory");
-  static_assert(NC >= 4, "compute warps 0..3 cover the four tensor-memory lane quarters");
+  static_assert(NC >= 4, "compute warps NC-4 .. NC-1 cover the four tensor-memory lane quarters");
   static_assert(NCOPY <= 32, "one producer lane per bulk copy");
   static_assert(4 * E <= 32, "the MMA warp forms node-0 terms with 4 lanes per element");
   static_assert(NCOL <= 64 && NCOL % 2 == 0,
@@ -346,38 +347,52 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
     // epilogue of ring iteration `it` from accumulator buffer it % 2, with
     // its RK register values in kr; false when the wait for its MMAs expired
     // (on every compute warp alike)
-    auto epilogue = [&](int it) -> bool {
+    // D of ring iteration `it` into the rhs staging, by warps NC-4 .. NC-1
+    // (lane quarter warp % 4; with 25 tasks over 14 warps three of them carry
+    // one task, so they read while the others finish their second): waits for
+    // MMA(it) itself; false when that wait expired.  Lane 2j + p of quarter q
+    // holds row (node NPQ q + j, operator part p).
+    auto read_d = [&](int it) -> bool {
       const int db = it & 1;
+      // every compute warp sees MMA(it) complete before it rewrites that
+      // tile's operand image set (the non-readers' wait is short: by then
+      // the MMAs are usually done)
+      if (!mbar_wait(&mma_done[db], (it >> 1) & 1, lim)) return false;
+      if (warp < NC - 4) return true;
+      tc_fence_after();
+      const int q = warp & 3, p = lane & 1, j = lane >> 1, node = C::NPQ * q + j;
+      const bool on = j < C::NPQ && node < Np;
+      float r[2 * NCOL];
+      const unsigned row = tmem + ((unsigned)(32 * q) << 16) + db * C::D_COLS;
+#pragma unroll
+      for (int c = 0; c < 2 * NCOL; c += 4) tmem_ld4(row + c, r + c);
+      tmem_ld_wait();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&d_free[db]);   // the accumulator is free for tile it + 2
+      // part products of this row, then the partner's half: lane p takes
+      // columns [p H, (p+1) H) (register indices stay compile-time)
+      constexpr int H = NCOL / 2;
+#pragma unroll
+      for (int c = 0; c < H; c++) {
+        const float lo_half = r[c] + r[NCOL + c], hi_half = r[H + c] + r[NCOL + H + c];
+        const float other = __shfl_xor_sync(0xffffffffu, p ? lo_half : hi_half, 1);
+        if (on) sR[(p * H + c) * Np + node] = (p ? hi_half : lo_half) + other;
+      }
+      return true;
+    };
+
+    // epilogue of ring iteration `it`: read_d(it) by the reader warps, then
+    // (after a barrier that also carries their wait status) the update;
+    // false when a wait expired (on every compute warp alike)
+    auto epilogue = [&](int it) -> bool {
       const long e0 = tile_e0(it);
       const int ne = (int)min((long)E, (long)a.K - e0);
       double *bU = ring(it);
-      // MMA(it) done; every compute warp is done with the staging of the
-      // previous update
-      if (!consumer_all(mbar_wait(&mma_done[db], (it >> 1) & 1, lim), TC)) return false;
-      tc_fence_after();
-      if (warp < 4) {
-        // lane 2j + p of quarter q holds row (node NPQ q + j, operator part p)
-        const int q = warp, p = lane & 1, j = lane >> 1, node = C::NPQ * q + j;
-        const bool on = j < C::NPQ && node < Np;
-        float r[2 * NCOL];
-        const unsigned row = tmem + ((unsigned)(32 * q) << 16) + db * C::D_COLS;
-#pragma unroll
-        for (int c = 0; c < 2 * NCOL; c += 4) tmem_ld4(row + c, r + c);
-        tmem_ld_wait();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&d_free[db]);   // the accumulator is free for tile it + 2
-        // part products of this row, then the partner's half: lane p takes
-        // columns [p H, (p+1) H) (register indices stay compile-time)
-        constexpr int H = NCOL / 2;
-#pragma unroll
-        for (int c = 0; c < H; c++) {
-          const float lo_half = r[c] + r[NCOL + c], hi_half = r[H + c] + r[NCOL + H + c];
-          const float other = __shfl_xor_sync(0xffffffffu, p ? lo_half : hi_half, 1);
-          if (on) sR[(p * H + c) * Np + node] = (p ? hi_half : lo_half) + other;
-        }
-      }
-      consumer_sync(TC);
+      // the staged rhs of tile it is complete (and the previous update's
+      // reads of the staging happened before the readers began: the
+      // iteration's first barrier separates them)
+      if (!consumer_all(read_d(it), TC)) return false;
       // LSERK update over (variable, element node): staged rhs, u and the
       // RK register values, coalesced stores
       auto update = [&](auto nepc) {
