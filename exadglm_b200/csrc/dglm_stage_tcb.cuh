@@ -69,8 +69,8 @@ struct TBCfg {
   static constexpr size_t OFF_C = OFF_R + 8 * (size_t)S_R;
   static constexpr size_t OFF_BAR = OFF_C + 8 * 2 * (size_t)S_C;
   // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2],
-  // cen[2] (index 0 only for the single-buffered ones)
-  static constexpr int NBARS = 2 * NB + 8;
+  // cen[2], vol_done[2] (index 0 only for the single-buffered ones)
+  static constexpr int NBARS = 2 * NB + 10;
   static constexpr size_t SMEM = OFF_BAR + 8 * (NBARS + 1) + 4 * NFF + 8 * 32 + 64;
   // instruction descriptor: F32 accumulate, BF16 A and B, both K-major, N, M = 128
   static constexpr unsigned IDESC =
@@ -80,7 +80,7 @@ struct TBCfg {
   static_assert(Np <= 128, "one output node per tensor-memory lane");
   static_assert(NBUF * D_COLS + KT <= TMEM_COLS, "accumulators and operator fit tensor memory");
   static_assert(KT % 16 == 0 && A_PART % 8 == 0, "whole MMAs and 8-column operator loads");
-  static_assert(NC >= 4, "compute warps 0..3 cover the four tensor-memory lane quarters");
+  static_assert(NC >= 4, "compute warps NC-4 .. NC-1 cover the four tensor-memory lane quarters");
   static_assert(NCOPY <= 32 && 4 * E <= 32, "producer and MMA warp lane assignments");
   static_assert(NB >= 2 && NB <= 4, "ring of 2..4 tile buffers");
   static_assert((E * Np * 8) % 16 == 0, "16-byte bulk copies");
@@ -120,7 +120,8 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
   double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
   unsigned long long *full = bars, *empty = bars + NB, *flux_done = bars + 2 * NB,
-                     *mma_done = flux_done + 2, *d_free = flux_done + 4, *cen = flux_done + 6;
+                     *mma_done = flux_done + 2, *d_free = flux_done + 4, *cen = flux_done + 6,
+                     *vol_done = flux_done + 8;
   unsigned *sTmem = reinterpret_cast<unsigned *>(bars + C::NBARS);
   int *sFm = reinterpret_cast<int *>(bars + C::NBARS + 1);
   unsigned long long *sMax = reinterpret_cast<unsigned long long *>(sFm + NFF + (NFF & 1));
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&flux_done[b], NC);
+      mbar_init(&vol_done[b], NC);
       mbar_init(&mma_done[b], 1);
       mbar_init(&d_free[b], C::NQ);
       mbar_init(&cen[b], 1);
@@ -394,11 +396,24 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       tc_fence_after();
       if (!DBUF_ && it > 0) read_d(it - 1);
       unsigned char *sBv = smem_raw + bsel(it) * C::B_BYTES, *sBf = sBv + C::BV_BYTES;
+      // one image set: vol_done once this warp's last volume task is written,
+      // so the volume MMAs (on the critical path then) start while the face
+      // tasks run
+      auto vol_signal = [&]() {
+        if constexpr (!DBUF_) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&vol_done[0]);
+        }
+      };
+      if (warp >= C::VOL_WT) vol_signal();
       for (int wt = warp; wt < C::NTASK; wt += NC) {
-        if (wt < C::VOL_WT)
+        if (wt < C::VOL_WT) {
           vol_task(it, wt, ne, sBv);
-        else
+          if (wt + NC >= C::VOL_WT) vol_signal();
+        } else {
           face_task(it, wt - C::VOL_WT, ne, sBf);
+        }
       }
       // operand written; the ring slot is no longer read by this warp
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -519,25 +534,35 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
     if (my_tiles > 0 && !centers_of(0)) ok = false;
     for (int it = 0; ok && it < my_tiles; it++) {
       const int b = bsel(it);
-      bool w = mbar_wait(&flux_done[b], bphase(it), lim);
-      // the accumulator: read back by read_d(it - NBUF)
+      // the volume operand (with two image sets: the whole operand), and the
+      // accumulator (read back by read_d(it - NBUF))
+      bool w = DBUF_ ? mbar_wait(&flux_done[b], bphase(it), lim)
+                     : mbar_wait(&vol_done[0], bphase(it), lim);
       if (w && it >= NBUF) w = mbar_wait(&d_free[b], bphase(it - NBUF), lim);
       if (!__all_sync(0xffffffffu, w)) {
         ok = false;
         break;
       }
+      const unsigned d = tmem + b * C::D_COLS;
+      const unsigned bv = smem_u32(smem_raw + b * C::B_BYTES), bf = bv + C::BV_BYTES;
       if (lane == 0) {
         tc_fence_after();
-        const unsigned d = tmem + b * C::D_COLS;
-        const unsigned bv = smem_u32(smem_raw + b * C::B_BYTES), bf = bv + C::BV_BYTES;
 #pragma unroll 1
         for (int ks = 0; ks < C::KSV; ks++) {
           const unsigned long long bd = smem_desc(bv + ks * 256, 128, C::SBO_V);
           tc_mma_ts_bf16(d, tmem + C::A_COL + ks * 8, bd, C::IDESC, ks > 0);
           tc_mma_ts_bf16(d, tmem + C::A_COL + C::A_PART + ks * 8, bd, C::IDESC, 1);
         }
+      }
+      __syncwarp();
+      // the face operand; on expiry the volume MMAs are still committed, so
+      // their completion can be waited for before the CTA leaves
+      if (!DBUF_) w = mbar_wait(&flux_done[b], bphase(it), lim);
+      const bool fw = __all_sync(0xffffffffu, w);
+      if (lane == 0) {
+        tc_fence_after();
 #pragma unroll 1
-        for (int ks = 0; ks < C::KSF; ks++) {
+        for (int ks = 0; fw && ks < C::KSF; ks++) {
           const unsigned long long bd = smem_desc(bf + ks * 256, 128, C::SBO_F);
           const int kc = C::KVA / 2 + ks * 8;
           tc_mma_ts_bf16(d, tmem + C::A_COL + kc, bd, C::IDESC, 1);
@@ -547,6 +572,10 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       }
       __syncwarp();
       nm++;
+      if (!fw) {
+        ok = false;
+        break;
+      }
       // the next tile's node-0 terms while the tensor cores work
       if (it + 1 < my_tiles && !centers_of(it + 1)) {
         ok = false;
