@@ -61,10 +61,15 @@ typedef enum { DGLM_ADVECTION = 0, DGLM_EULER = 1 } dglm_physics;
  * mode. */
 typedef enum {
     DGLM_PREC_FP64 = 0,        /* plain method: FP64 throughout */
-    DGLM_PREC_TF32X3 = 1,      /* 3-pass TF32 on tcgen05, FP32 accumulate */
-    DGLM_PREC_BF16X3 = 2,      /* split-BF16, 2 parts, 3 products, FP32 accumulate */
+    DGLM_PREC_TF32X3 = 1,      /* split TF32 (2 parts) on tcgen05, FP32 accumulate; the
+                                  operator-in-tensor-memory kernel forms all 4 products */
+    DGLM_PREC_BF16X3 = 2,      /* split BF16 (2 parts), 3 products (4 with the
+                                  operator in tensor memory), FP32 accumulate */
     DGLM_PREC_BF16X6 = 3       /* split-BF16, 3 parts (24 bits), 6 products, FP32 accumulate */
 } dglm_precision;
+/* In every mixed mode the Euler fluxes are centred on each element's node-0
+ * flux before the split (the right-hand side is unchanged); the LSERK state,
+ * fluxes, metrics and update stay FP64. */
 
 /* Solver description: the reference's compile-time common.h parameters
  * (dglm_3d_launcher.py:152-205) as run-time values. */
