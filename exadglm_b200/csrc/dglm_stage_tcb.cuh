@@ -423,16 +423,22 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
         mbar_arrive(&empty[it % NB]);
       }
       if (it > 0) {
-        load_ku(it - 1);
+        // two accumulators: the reader warps (which carry fewer flux tasks)
+        // read D(it - 1) right after their own tasks; the barrier then also
+        // carries the wait status
+        bool w2 = true;
         if (DBUF_) {
-          if (!consumer_all(mbar_wait(&mma_done[bsel(it - 1)], bphase(it - 1), lim), TC)) {
-            ok = false;
-            break;
+          w2 = mbar_wait(&mma_done[bsel(it - 1)], bphase(it - 1), lim);
+          if (w2) {
+            tc_fence_after();
+            read_d(it - 1);
           }
-          tc_fence_after();
-          read_d(it - 1);
         }
-        consumer_sync(TC);
+        load_ku(it - 1);
+        if (!consumer_all(w2, TC)) {
+          ok = false;
+          break;
+        }
         update(it - 1);
       }
     }
