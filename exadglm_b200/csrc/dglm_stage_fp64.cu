@@ -658,90 +658,74 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 // Standalone calc_maxv (initial state, advection velocity, and the end of a
 // step for the stage kernels that do not fuse it): maxv per face and a
 // device-wide max of maxv*Fscale into sc->acc[slot] (slot < 0: the slot the
-// fused copy would use, acc[parity ^ 1]).  One warp per element: its nodes'
-// |v|^2 and c^2 (node_speeds) from coalesced loads into shared memory, then
-// LPF lanes per face take the face maxima by
-// shuffles (max is exact, so the result does not depend on the order).
+// fused copy would use, acc[parity ^ 1]).  A block walks tiles of ET whole
+// elements (ET Np <= 256 consecutive nodes of each variable): one thread per
+// node loads the node's variables (coalesced) and writes its |v|^2 and c^2
+// (node_speeds) to shared memory, then loads the next tile's values, which
+// are in flight while one thread per (element, face) takes the face maxima
+// through Fmask.  Max is exact, so the result does not depend on the order;
+// one atomic per block.
 template <int PHYS, int N>
 __global__ void __launch_bounds__(256) face_maxv_kernel(const StageArgs a, int slot) {
   constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
-  constexpr int LPF = Nfp <= 16 ? 16 : 32, FPW = 32 / LPF, WPB = 8;
-  __shared__ double sV[WPB][Np], sC[WPB][Np];
+  constexpr int ET = 256 / Np, NQ = PHYS == EUL ? 5 : 3;
+  static_assert(ET >= 1 && 4 * ET <= 256, "a tile of whole elements fits the block");
+  __shared__ double sV[ET * Np], sC[ET * Np];
   __shared__ int sFm[NFF];
-  __shared__ unsigned long long sMax[WPB];
-  for (int i = threadIdx.x; i < NFF; i += blockDim.x) sFm[i] = a.Fmask[i];
-  __syncthreads();
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, jn = lane % LPF;
-  // node values of this warp's next element, requested one element ahead
-  constexpr int NI = (Np + 31) / 32, NQ = PHYS == EUL ? 5 : 3;
+  __shared__ unsigned long long sMax[8];
+  const int t = threadIdx.x;
+  for (int i = t; i < NFF; i += blockDim.x) sFm[i] = a.Fmask[i];
   const double *src = PHYS == EUL ? a.u_in : a.vel;
-  double q[NI][NQ];
-  auto fetch = [&](long e) {
+  double q[NQ];
+  auto fetch = [&](long e0) {
+    const long n = (a.K - e0 < ET ? a.K - e0 : ET) * Np;   // nodes of the tile (<= 0: none)
 #pragma unroll
-    for (int r = 0; r < NI; r++) {
-      const int i = lane + 32 * r;
-#pragma unroll
-      for (int v = 0; v < NQ; v++)
-        q[r][v] = (e < a.K && i < Np) ? src[v * a.vs + e * Np + i] : 1.0;
-    }
+    for (int v = 0; v < NQ; v++) q[v] = t < n ? src[v * a.vs + e0 * Np + t] : 1.0;
   };
   unsigned long long local = 0ull;
-  const long stride = (long)gridDim.x * WPB;
-  fetch(blockIdx.x * (long)WPB + w);
-  for (long e = blockIdx.x * (long)WPB + w; e < a.K; e += stride) {
-#pragma unroll
-    for (int r = 0; r < NI; r++) {
-      const int i = lane + 32 * r;
+  const long stride = (long)gridDim.x * ET;
+  fetch((long)blockIdx.x * ET);
+  for (long e0 = (long)blockIdx.x * ET; e0 < a.K; e0 += stride) {
+    const int ne = (int)(a.K - e0 < ET ? a.K - e0 : ET);
+    if (t < ne * Np) {
       double v2, c2 = 0.0;
       if (PHYS == EUL)
-        node_speeds(a.gamma, q[r][0], q[r][1], q[r][2], q[r][3], q[r][4], v2, c2);
+        node_speeds(a.gamma, q[0], q[1], q[2], q[3], q[4], v2, c2);
       else
-        v2 = q[r][0] * q[r][0] + q[r][1] * q[r][1] + q[r][2] * q[r][2];
-      if (i < Np) {
-        sV[w][i] = v2;
-        sC[w][i] = c2;
-      }
+        v2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+      sV[t] = v2;
+      sC[t] = c2;
     }
-    fetch(e + stride);
-    __syncwarp();
-#pragma unroll
-    for (int f0 = 0; f0 < 4; f0 += FPW) {
-      const int f = f0 + lane / LPF;
+    fetch(e0 + stride);
+    __syncthreads();
+    if (t < 4 * ne) {
+      const int e = t >> 2, f = t & 3;
       double v2 = 0.0, c2 = 0.0;
       int bad = 0;
-      for (int j = jn; j < Nfp; j += LPF) {
-        const int nd = sFm[f * Nfp + j];
-        const double w2 = sV[w][nd], d2 = sC[w][nd];
+#pragma unroll 5
+      for (int j = 0; j < Nfp; j++) {
+        const int nd = e * Np + sFm[f * Nfp + j];
+        const double w2 = sV[nd], d2 = sC[nd];
         bad |= (w2 != w2) || (d2 != d2);
         v2 = w2 > v2 ? w2 : v2;
         c2 = d2 > c2 ? d2 : c2;
       }
-#pragma unroll
-      for (int o = LPF / 2; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v2, o);
-        const double oc = __shfl_xor_sync(0xffffffffu, c2, o);
-        v2 = ov > v2 ? ov : v2;
-        c2 = oc > c2 ? oc : c2;
-        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
-      }
-      if (jn == 0) {
-        const long gf = e * 4 + f;
-        double mv = (PHYS == EUL) ? sqrt(v2) + sqrt(c2) : sqrt(v2);
-        if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
-        a.maxv[gf] = mv;
-        const unsigned long long b = dbits(mv * a.fscale[gf]);
-        local = b > local ? b : local;
-      }
+      const long gf = (e0 + e) * 4 + f;
+      double mv = (PHYS == EUL) ? sqrt(v2) + sqrt(c2) : sqrt(v2);
+      if (bad) mv = __longlong_as_double(0x7ff8000000000000LL);
+      a.maxv[gf] = mv;
+      const unsigned long long b = dbits(mv * a.fscale[gf]);
+      local = b > local ? b : local;
     }
-    __syncwarp();
+    __syncthreads();
   }
   local = warp_max_bits(local);
-  if (lane == 0) sMax[w] = local;
+  if ((t & 31) == 0) sMax[t >> 5] = local;
   __syncthreads();
-  if (threadIdx.x < 32) {
-    unsigned long long v = threadIdx.x < WPB ? sMax[threadIdx.x] : 0ull;
+  if (t < 32) {
+    unsigned long long v = t < (int)(blockDim.x >> 5) ? sMax[t] : 0ull;
     v = warp_max_bits(v);
-    if (threadIdx.x == 0) atomicMax(&a.sc->acc[slot >= 0 ? slot : a.sc->parity ^ 1], v);
+    if (t == 0) atomicMax(&a.sc->acc[slot >= 0 ? slot : a.sc->parity ^ 1], v);
   }
 }
 
@@ -900,10 +884,10 @@ static Variant make_mixed() {
   return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC, PW>};
 }
 
-template <int PHYS, int N, int E, int NF, int NB>
+template <int PHYS, int N, int E, int NF, int NB, int NPL>
 static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
-  using C = TCfg<PHYS, N, E, NF, NB>;
-  auto k = stage_tc_kernel<PHYS, N, E, NF, NB>;
+  using C = TCfg<PHYS, N, E, NF, NB, NPL>;
+  auto k = stage_tc_kernel<PHYS, N, E, NF, NB, NPL>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -945,12 +929,13 @@ static Variant make_tcb() {
   return Variant{i, &launch_tcb<PHYS, N, E, NF, NB, DB>};
 }
 
-template <int PHYS, int N, int E, int NF, int NB>
+template <int PHYS, int N, int E, int NF, int NB, int NPL = 1>
 static Variant make_tc() {
-  using C = TCfg<PHYS, N, E, NF, NB>;
+  using C = TCfg<PHYS, N, E, NF, NB, NPL>;
   StageVariantInfo i{};
   i.mode = MODE_TC;
   i.E = E;
+  i.R = NPL;          // nodes per lane in a flux task
   i.threads = C::THREADS;
   i.smem = C::SMEM;
   i.prec = DGLM_PREC_TF32X3;
@@ -961,7 +946,7 @@ static Variant make_tc() {
   i.ring = NB;
   i.producers = NF;   // compute warps
   i.persistent = 1;
-  return Variant{i, &launch_tc<PHYS, N, E, NF, NB>};
+  return Variant{i, &launch_tc<PHYS, N, E, NF, NB, NPL>};
 }
 
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
@@ -1031,6 +1016,8 @@ static const std::vector<Variant> &variants();
 #define V_MXP(P, NN, E, PREC, W, PW) make_mixed<P, NN, E, PREC, W, PW>()
 // split-TF32 with the operator in tensor memory: E elements, NF compute warps, NB ring slots
 #define V_TC(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB>()
+// the same with two nodes per lane in each flux task
+#define V_TC2(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB, 2>()
 // split-BF16 with the operator in tensor memory: DB = double-buffered images and accumulators
 #define V_TCB(P, NN, E, NF, NB, DB) make_tcb<P, NN, E, NF, NB, DB>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
@@ -1059,7 +1046,8 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPE2R(EUL, 4, 8, 1, 5, 3, 2), V_PIPEF(EUL, 4, 8, 1, true, 3, 2),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
               V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2),
-              V_TC(EUL, 4, 8, 14, 3), V_TCB(EUL, 4, 8, 14, 2, true))
+              V_TC(EUL, 4, 8, 14, 3), V_TCB(EUL, 4, 8, 14, 2, true),
+              V_TC2(EUL, 4, 8, 13, 3))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),
@@ -1134,10 +1122,11 @@ cudaError_t launch_stage_fp64(int physics, int N, int variant, const StageArgs &
 
 template <int PHYS, int N>
 static cudaError_t launch_maxv_one(const StageArgs &a, int slot, cudaStream_t s) {
-  // 8 warps per block, one element per warp at a time
-  int blocks = (int)((a.K + 7) / 8);
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  face_maxv_kernel<PHYS, N><<<blocks, 256, 0, s>>>(a, slot);
+  // tiles of 256 / Np whole elements, up to 8 blocks per SM walking them
+  constexpr int ET = 256 / np_of(N);
+  long blocks = (a.K + ET - 1) / ET;
+  if (blocks > 8L * sm_count()) blocks = 8L * sm_count();
+  face_maxv_kernel<PHYS, N><<<(int)blocks, 256, 0, s>>>(a, slot);
   return cudaGetLastError();
 }
 

@@ -50,7 +50,10 @@
 //   compute     per tile t: loads of tile t-1's RK register values, the
 //               volume and face flux tasks of t into image set t%2, then the
 //               epilogue of t-1: the wait for MMA(t-1); warps NC-4 .. NC-1
-//               (three of which carry one flux task, not two) read D[(t-1)%2]
+//               (at Euler N=4 with one node per lane, 25 tasks over 14
+//               warps, three of them carry one flux task, not two; with two
+//               nodes per lane, NPL = 2, 13 tasks, every warp at most one)
+//               read D[(t-1)%2]
 //               (lane quarter warp % 4) and add the parts into the rhs
 //               staging; all compute warps do the LSERK update with
 //               coalesced stores.
@@ -59,7 +62,7 @@
 // (with the default bound) for the MMAs and copies it issued, and leaves.
 #pragma once
 
-template <int PHYS, int N, int E_, int NC_, int NB_>
+template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1>
 struct TCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -92,8 +95,12 @@ struct TCfg {
   static constexpr int S_R = NV * E * Np;
   // warp tasks per tile: volume (8 elements x one node group of 4), face
   // (8 elements x 4 nodes of one face)
+  // (8 elements x 8 nodes with NPL = 2 nodes per lane: pairs of groups)
+  static constexpr int NPL = NPL_;
   static constexpr int NEB = E / 8, NJB = NFPP / 4;
-  static constexpr int VOL_WT = NEB * NG, FACE_WT = NEB * 4 * NJB;
+  static constexpr int NGP = (NG + 1) / 2, NJP = (NJB + 1) / 2;
+  static constexpr int VOL_WT = NEB * (NPL == 2 ? NGP : NG);
+  static constexpr int FACE_WT = NEB * 4 * (NPL == 2 ? NJP : NJB);
   static constexpr int NTASK = VOL_WT + FACE_WT;
   static constexpr int PROD_WARP = NC, MMA_WARP = NC + 1, NWARPS = NC + 2;
   static constexpr int THREADS = 32 * NWARPS, TC = 32 * NC;
@@ -120,6 +127,7 @@ struct TCfg {
   static_assert(NCOL <= 64 && NCOL % 2 == 0,
                 "an epilogue lane holds both parts of its row's columns, split in halves");
   static_assert(NB >= 2 && NB <= 4, "ring of 2..4 tile buffers");
+  static_assert(NPL == 1 || NPL == 2, "one or two nodes per lane in a flux task");
   static_assert((E * Np * 8) % 16 == 0, "16-byte bulk copies");
   static_assert(THREADS <= 1024 && NWARPS <= 32, "block size");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
@@ -162,10 +170,10 @@ __device__ __forceinline__ void split_tf32_pair(double x, unsigned &hi, unsigned
   lo = __float_as_uint(f - __uint_as_float(hi));
 }
 
-template <int PHYS, int N, int E_, int NC_, int NB_>
-__global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
+template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1>
+__global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_>::THREADS, 1)
     stage_tc_kernel(const StageArgs a, int ntiles) {
-  using C = TCfg<PHYS, N, E_, NC_, NB_>;
+  using C = TCfg<PHYS, N, E_, NC_, NB_, NPL_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, NB = C::NB,
                 NC = C::NC, TC = C::TC, NCOL = C::NCOL;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -319,6 +327,95 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       }
     };
 
+    // NPL = 2: task wt of the volume covers 8 elements x node groups 2gp and
+    // 2gp + 1; lane (e = lane % 8, h = bit 3, group = bit 4) takes nodes
+    // 4g + 2h and 4g + 2h + 1, two independent flux chains whose columns
+    // are neighbours in one core-matrix row (one 8-byte store per part), and
+    // the element's metrics and node-0 terms serve both.  Node indices past
+    // the element are clamped for the loads and their values written as 0.
+    auto vol_task2 = [&](int it, int wt, int ne, unsigned char *sBv) {
+      const int eb = wt / C::NGP, g = 2 * (wt - eb * C::NGP) + (lane >> 4);
+      if (g >= C::NG) return;   // the empty half of an odd group count
+      const int h = (lane >> 3) & 1, e = eb * 8 + (lane & 7), i0 = 4 * g + 2 * h;
+      const double *bU = ring(it), *bR = bU + C::S_U + C::S_UP + e * kRecord;
+      const double *cn = sC0 + (it & 1) * C::S_C + e * NV * C::NCEN;
+      const bool on0 = e < ne && i0 < Np, on1 = e < ne && i0 + 1 < Np;
+      double F[2][5], G[2][5], W[2][5];
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const int i = min(i0 + s, Np - 1);
+        double q[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np + i];
+        euler_flux_fast(gam, q, F[s], G[s], W[s]);
+      }
+      double m[9];
+#pragma unroll
+      for (int x = 0; x < 9; x++) m[x] = bR[x];
+#pragma unroll
+      for (int v = 0; v < 5; v++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const double c = -cn[v * C::NCEN + d];
+          unsigned hi0, lo0, hi1, lo1;
+          split_tf32_pair(fma(m[3 * d + 2], W[0][v], fma(m[3 * d + 1], G[0][v],
+                                                         fma(m[3 * d], F[0][v], c))),
+                          hi0, lo0);
+          split_tf32_pair(fma(m[3 * d + 2], W[1][v], fma(m[3 * d + 1], G[1][v],
+                                                         fma(m[3 * d], F[1][v], c))),
+                          hi1, lo1);
+          const int n = v * E + e, k = g * 12 + d * 4 + 2 * h;
+          const int off = (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4;
+          *reinterpret_cast<uint2 *>(sBv + (n >> 3) * C::SBO_V + off) =
+              make_uint2(on0 ? hi0 : 0u, on1 ? hi1 : 0u);
+          *reinterpret_cast<uint2 *>(sBv + ((n + NCOL) >> 3) * C::SBO_V + off) =
+              make_uint2(on0 ? lo0 : 0u, on1 ? lo1 : 0u);
+        }
+    };
+
+    // NPL = 2: face task wt covers 8 elements x face nodes 8jp .. 8jp + 7 of
+    // one face, lane (e, h, bit 4) face nodes j0 = 4jb + 2h and j0 + 1
+    auto face_task2 = [&](int it, int wt, int ne, unsigned char *sBf) {
+      const int eb = wt / (4 * C::NJP), f = (wt / C::NJP) & 3;
+      const int jb = 2 * (wt % C::NJP) + (lane >> 4);
+      if (jb >= C::NJB) return;
+      const int h = (lane >> 3) & 1, e = eb * 8 + (lane & 7), j0 = 4 * jb + 2 * h;
+      const double *bU = ring(it), *bUP = bU + C::S_U;
+      const double *bR = bUP + C::S_UP + e * kRecord, *bT = bUP + C::S_UP + C::S_REC;
+      const double nx = bR[9 + f], ny = bR[13 + f], nz = bR[17 + f], fs = bR[21 + f],
+                   tau = bT[e * 4 + f];
+      const double *cn = sC0 + (it & 1) * C::S_C + e * NV * C::NCEN + 3 + f;
+      const bool on0 = e < ne && j0 < Nfp, on1 = e < ne && j0 + 1 < Nfp;
+      unsigned hv[2][5], lv[2][5];
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const int fj = f * Nfp + min(j0 + s, Nfp - 1), nodeM = sFm[fj];
+        double qm[5], qb[5], F[5], G[5], W[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          qm[v] = bU[v * E * Np + e * Np + nodeM];
+          qb[v] = 0.5 * (qm[v] + bUP[(v * E + e) * C::UPS + fj]);
+        }
+        euler_flux_fast(gam, qb, F, G, W);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const double nd = fma(nz, W[v], fma(ny, G[v], nx * F[v]));
+          split_tf32_pair(fma(nd - tau * (qb[v] - qm[v]), fs, -cn[v * C::NCEN]), hv[s][v],
+                          lv[s][v]);
+        }
+      }
+      const int k = f * C::NFPP + j0;
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        const int n = v * E + e;
+        const int off = (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4;
+        *reinterpret_cast<uint2 *>(sBf + (n >> 3) * C::SBO_F + off) =
+            make_uint2(on0 ? hv[0][v] : 0u, on1 ? hv[1][v] : 0u);
+        *reinterpret_cast<uint2 *>(sBf + ((n + NCOL) >> 3) * C::SBO_F + off) =
+            make_uint2(on0 ? lv[0][v] : 0u, on1 ? lv[1][v] : 0u);
+      }
+    };
+
     // this thread's RK register values of ring iteration `it` (update order:
     // x = tid + r TC over (variable, element node)); the element count is a
     // literal for full tiles, so the index divisions are multiplications
@@ -348,8 +445,8 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
     // its RK register values in kr; false when the wait for its MMAs expired
     // (on every compute warp alike)
     // D of ring iteration `it` into the rhs staging, by warps NC-4 .. NC-1
-    // (lane quarter warp % 4; with 25 tasks over 14 warps three of them carry
-    // one task, so they read while the others finish their second): waits for
+    // (lane quarter warp % 4; where the tasks do not divide evenly they carry
+    // the fewer, so they read while the others finish): waits for
     // MMA(it) itself; false when that wait expired.  Lane 2j + p of quarter q
     // holds row (node NPQ q + j, operator part p).
     auto read_d = [&](int it) -> bool {
@@ -482,10 +579,17 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_>::THREADS, 1)
       if (it > 0) load_k(it - 1);
       unsigned char *sBv = smem_raw + (it & 1) * C::B_BYTES, *sBf = sBv + C::BV_BYTES;
       for (int wt = warp; wt < C::NTASK; wt += NC) {
-        if (wt < C::VOL_WT)
-          vol_task(it, wt, ne, sBv);
-        else
-          face_task(it, wt - C::VOL_WT, ne, sBf);
+        if constexpr (C::NPL == 2) {
+          if (wt < C::VOL_WT)
+            vol_task2(it, wt, ne, sBv);
+          else
+            face_task2(it, wt - C::VOL_WT, ne, sBf);
+        } else {
+          if (wt < C::VOL_WT)
+            vol_task(it, wt, ne, sBv);
+          else
+            face_task(it, wt - C::VOL_WT, ne, sBf);
+        }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
