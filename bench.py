@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint", "batch", "precision",
+    ap.add_argument("--only", choices=["fp64", "mixed", "face_maps", "adjoint", "batch",
+                                       "precision",
                                        "gpu_baseline"],
                     default=None,
                     help="run one section alone (profiling); prints that section's object")
@@ -301,6 +302,36 @@ def _events(stream):
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     return e0, e1
+
+
+def face_maps_section(a, p, stream):
+    """A/B of the neighbour-node source on the same handle: vmapP (4 Nfp ints
+    per face) against the compact face maps (neighbour element and a one-byte
+    node-list code per face), alternated twice, FP64 and TF32x3."""
+    import numpy as np
+    from exadglm_b200.capi import Solver, variants
+    out = {"bytes_per_element": {"vmapP": 4 * 4 * p.Nfp, "compact": 4 * 5}}
+    for prec in ("fp64", "tf32x3"):
+        s = Solver(p, precision=prec)
+        s.set_stream(stream.cuda_stream)
+        ms = {False: [], True: []}
+        for on in (False, True, False, True):
+            s.set_compact_face_maps(on)
+            s.step(a.warmup)
+            s.sync()
+            e0, e1 = _events(stream)
+            e0.record(stream)
+            s.step(a.steps)
+            e1.record(stream)
+            e1.synchronize()
+            s.sync()
+            ms[on].append(e0.elapsed_time(e1) / a.steps)
+        out[prec] = {"kernel": variants(p.physics, p.N)[s.variant()],
+                     "vmapP_ms_per_step": float(np.min(ms[False])),
+                     "compact_ms_per_step": float(np.min(ms[True])),
+                     "node_lists": s.face_map_lists()}
+        s.close()
+    return out
 
 
 def mixed_section(a, p, stream, fp64_ms_per_step):
@@ -661,8 +692,9 @@ def main():
 
     p = build_problem(a)
     stream = torch.cuda.Stream()
-    if a.only in ("mixed", "adjoint", "batch", "precision", "gpu_baseline"):
+    if a.only in ("mixed", "face_maps", "adjoint", "batch", "precision", "gpu_baseline"):
         res = (mixed_section(a, p, stream, None) if a.only == "mixed"
+               else face_maps_section(a, p, stream) if a.only == "face_maps"
                else adjoint_section(a, stream) if a.only == "adjoint"
                else precision_section(a, stream) if a.only == "precision"
                else gpu_baseline_section(a, p, rank) if a.only == "gpu_baseline"
@@ -771,6 +803,7 @@ def main():
     }
     if a.only is None and a.precision == "fp64":
         line["mixed"] = mixed_section(a, p, stream, ms_max / a.steps)
+        line["face_maps"] = face_maps_section(a, p, stream)
         line["adjoint"] = adjoint_section(a, stream)
         if rank == 0:
             gb = gpu_baseline_section(a, p, rank)

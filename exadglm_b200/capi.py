@@ -27,7 +27,8 @@ EXPORTS = (
     "dglm_rhs", "dglm_kernel_launches", "dglm_device_bytes", "dglm_calc_maxv", "dglm_calc_dt",
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
-    "dglm_set_variant", "dglm_get_variant", "dglm_set_wait_limit", "dglm_adjoint_record", "dglm_adjoint_backward",
+    "dglm_set_variant", "dglm_get_variant", "dglm_set_wait_limit",
+    "dglm_set_compact_face_maps", "dglm_face_map_lists", "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
     "dglm_adjoint_record_capped", "dglm_adjoint_tape_plan", "dglm_adjoint_schedule",
     "dglm_calc_maxv_dt_static", "dglm_adjoint_variant_count", "dglm_adjoint_variant_describe",
@@ -97,6 +98,8 @@ def lib():
         L.dglm_set_variant.argtypes = [_P, C.c_int]
         L.dglm_get_variant.argtypes = [_P]
         L.dglm_set_wait_limit.argtypes = [_P, C.c_longlong]
+        L.dglm_set_compact_face_maps.argtypes = [_P, C.c_int]
+        L.dglm_face_map_lists.argtypes = [_P]
         L.dglm_kernel_launches.argtypes = [_P]
         L.dglm_kernel_launches.restype = C.c_long
         L.dglm_device_bytes.argtypes = [_P]
@@ -439,6 +442,16 @@ class Solver:
         """Bound (SM clock cycles) of the hand-off waits of the pipelined
         stage kernels; 0 restores the default (about one second)."""
         check(self.L.dglm_set_wait_limit(self.h, int(cycles)))
+
+    def set_compact_face_maps(self, on=True):
+        """Neighbour node indices from compact face maps (neighbour element
+        and a one-byte node-list code per face) instead of vmapP in the
+        persistent stage kernels; bit for bit the same results."""
+        check(self.L.dglm_set_compact_face_maps(self.h, 1 if on else 0))
+
+    def face_map_lists(self):
+        """Distinct face node lists of the compact face maps (0 before built)."""
+        return int(self.L.dglm_face_map_lists(self.h))
 
     def kernel_launches(self):
         return int(self.L.dglm_kernel_launches(self.h))

@@ -47,6 +47,12 @@ struct StageArgs {
   const double *erec;    // per-element record [K][kRecord] or null (see kRecord)
   const double *tau;     // K*4
   const int *vmapP;      // K*4*Nfp
+  // compact face maps (dglm_set_compact_face_maps) or null: per face (e, f)
+  // the neighbour element and a one-byte code of its node list, with
+  // vmapP[e][f][j] = etoe[4e+f] Np + ftab[fcode[4e+f] Nfp + j]
+  const int *etoe;
+  const unsigned char *fcode;
+  const int *ftab;
   const int *Fmask;      // 4*Nfp
   const double *vel;     // advection: vx, vy, vz with stride vs
   const double *u_in;
@@ -67,6 +73,17 @@ struct StageArgs {
                          // pipelined kernels (kWaitCycles unless a test shortens it);
                          // waits for copies or MMAs already in flight keep kWaitCycles
 };
+
+// Neighbour node index vmapP[e0 NFF + idx] of face point idx = e NFF + f Nfp + j
+// of the tile that starts at element e0, from the compact face maps (20 bytes
+// per element instead of 4 NFF).  Producers branch on a.etoe once per tile,
+// outside their unrolled load loops, so the vmapP loop stays branch-free.
+template <int Np, int Nfp>
+__device__ __forceinline__ int compact_neighbour_node(const StageArgs &a, long e0, int idx) {
+  const int e = idx / (4 * Nfp), fj = idx - e * 4 * Nfp, f = fj / Nfp, j = fj - f * Nfp;
+  const long ge = (e0 + e) * 4 + f;
+  return __ldg(a.etoe + ge) * Np + __ldg(a.ftab + (int)__ldg(a.fcode + ge) * Nfp + j);
+}
 
 // Reference Euler flux (F, G, W) of the state q, in the arithmetic order of
 // euler_dglm.cpp:152-168 / euler_nopad_dglm.cu:181-198 (vb2 is |m|^2).

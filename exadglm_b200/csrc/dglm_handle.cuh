@@ -30,6 +30,12 @@ struct dglm_handle {
   // nx, ny, nz and Fscale of the 4 faces, one pad double; one bulk copy per
   // tile in the tensor-memory kernel
   double *erec = nullptr;
+  // compact face maps (dglm_set_compact_face_maps), built from vmapP on first
+  // use: per face the neighbour element and a code of its node list
+  int *etoe = nullptr, *ftab = nullptr;
+  unsigned char *fcode = nullptr;
+  int ftab_lists = 0;
+  bool compact_built = false, compact = false;
   // state
   double *u[2] = {nullptr, nullptr};
   double *kreg = nullptr;

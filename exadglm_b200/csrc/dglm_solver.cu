@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -65,6 +66,9 @@ StageArgs dglm::stage_args(dglm_handle *h, const double *u_in, double *u_out, in
   a.erec = h->erec;
   a.tau = h->tau;
   a.vmapP = h->vmapP;
+  a.etoe = h->compact ? h->etoe : nullptr;
+  a.fcode = h->compact ? h->fcode : nullptr;
+  a.ftab = h->compact ? h->ftab : nullptr;
   a.Fmask = h->Fmask;
   a.vel = h->vel;
   a.u_in = u_in;
@@ -577,6 +581,8 @@ dglm_status dglm_upload_mesh(dglm_handle *h, const dglm_mesh_arrays *m) {
   // host-side validation of every index array and every real array
   if (!in_range(m->vmapP, (size_t)K * NFF, 0, K * Np))
     return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: vmapP entry outside [0, K*Np)");
+  // compact face maps of an earlier mesh no longer apply (rebuilt on request)
+  h->compact = h->compact_built = false;
   if (!in_range(m->vmapF, (size_t)4 * K, 0, 4 * K))
     return set_error(DGLM_ERR_INVALID, "dglm_upload_mesh: vmapF entry outside [0, 4K)");
   if (!in_range(m->Fmask, (size_t)NFF, 0, Np))
@@ -1089,6 +1095,76 @@ dglm_status dglm_set_wait_limit(dglm_handle *h, long long cycles) {
   drop_graphs(h);   // the captured steps carry the bound in their arguments
   h->wait_cycles = cycles;
   return DGLM_OK;
+}
+
+dglm_status dglm_set_compact_face_maps(dglm_handle *h, int on) {
+  if (!h) return set_error(DGLM_ERR_INVALID, "dglm_set_compact_face_maps: NULL handle");
+  if (!h->mesh_ready)
+    return set_error(DGLM_ERR_INVALID, "dglm_set_compact_face_maps: no mesh uploaded");
+  DeviceGuard g(h->dev);
+  cudaStreamSynchronize(h->stream);
+  drop_graphs(h);   // the captured steps carry the map pointers in their arguments
+  if (!on) {
+    h->compact = false;
+    return DGLM_OK;
+  }
+  if (!h->compact_built) {
+    // from the uploaded vmapP: every face's trace must be one element's
+    // nodes; its local node list gets a code (first seen, first numbered)
+    const int K = h->d.K, Np = h->Np, Nfp = h->Nfp, NFF = h->NFF;
+    std::vector<int> vm((size_t)K * NFF);
+    cudaError_t e = cudaMemcpy(vm.data(), h->vmapP, sizeof(int) * vm.size(),
+                               cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+      return set_error(DGLM_ERR_CUDA, std::string("dglm_set_compact_face_maps: ") +
+                                          cudaGetErrorString(e));
+    std::vector<int> nb((size_t)K * 4), lists;
+    std::vector<unsigned char> code((size_t)K * 4);
+    std::map<std::vector<int>, int> seen;
+    std::vector<int> loc(Nfp);
+    for (size_t fc = 0; fc < (size_t)K * 4; fc++) {
+      const int *p = vm.data() + fc * Nfp;
+      const int n = p[0] / Np;
+      for (int j = 0; j < Nfp; j++) {
+        if (p[j] / Np != n)
+          return set_error(DGLM_ERR_UNSUPPORTED,
+                           "dglm_set_compact_face_maps: a face's trace spans several elements");
+        loc[j] = p[j] - n * Np;
+      }
+      auto it = seen.find(loc);
+      if (it == seen.end()) {
+        if (seen.size() == 256)
+          return set_error(DGLM_ERR_UNSUPPORTED,
+                           "dglm_set_compact_face_maps: more than 256 distinct face node lists");
+        it = seen.emplace(loc, (int)seen.size()).first;
+        lists.insert(lists.end(), loc.begin(), loc.end());
+      }
+      nb[fc] = n;
+      code[fc] = (unsigned char)it->second;
+    }
+    if (!h->etoe) {
+      dglm_status st = dalloc(h, &h->etoe, (size_t)K * 4);
+      if (st == DGLM_OK) st = dalloc(h, &h->fcode, (size_t)K * 4);
+      if (st == DGLM_OK) st = dalloc(h, &h->ftab, (size_t)256 * Nfp);
+      if (st != DGLM_OK) return st;
+    }
+    e = cudaMemcpy(h->etoe, nb.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->fcode, code.data(), code.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->ftab, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess)
+      return set_error(DGLM_ERR_CUDA, std::string("dglm_set_compact_face_maps: ") +
+                                          cudaGetErrorString(e));
+    h->ftab_lists = (int)seen.size();
+    h->compact_built = true;
+  }
+  h->compact = true;
+  return DGLM_OK;
+}
+
+int dglm_face_map_lists(dglm_handle *h) {
+  return h && h->compact_built ? h->ftab_lists : 0;
 }
 
 long dglm_kernel_launches(dglm_handle *h) { return h ? h->launches : 0; }

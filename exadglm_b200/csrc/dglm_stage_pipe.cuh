@@ -277,14 +277,23 @@ __device__ __forceinline__ void pipe_producer(const StageArgs &a, int ntiles, vo
           bulk_g2s(bV + q * E * Np, a.vel + q * vs + e0 * Np, 8u * E * Np, &full[b]);
     }
     // neighbour traces u+ = u[vmapP] into [v][e][UPS]: all of this lane's
-    // vmapP loads are issued first, so their latency is paid once
+    // vmapP loads (or compact face-map lookups) are issued first, so their
+    // latency is paid once
     constexpr int PT = 32 * C::PW;
     constexpr int GPL = (E * NFF + PT - 1) / PT;
     int vmr[GPL];
+    if (a.etoe) {
 #pragma unroll
-    for (int j = 0; j < GPL; j++) {
-      const int idx = 32 * pw + lane + PT * j;
-      vmr[j] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+      for (int j = 0; j < GPL; j++) {
+        const int idx = 32 * pw + lane + PT * j;
+        vmr[j] = idx < ne * NFF ? compact_neighbour_node<Np, C::Nfp>(a, e0, idx) : -1;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < GPL; j++) {
+        const int idx = 32 * pw + lane + PT * j;
+        vmr[j] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+      }
     }
 #pragma unroll
     for (int j = 0; j < GPL; j++) {

@@ -627,10 +627,18 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_>::THREADS, 1)
       // neighbour traces u+ = u[vmapP] into [v][e][UPS]: this lane's vmapP
       // entries are loaded before its gathers are issued
       int vmr[C::GPL];
+      if (a.etoe) {
 #pragma unroll
-      for (int g = 0; g < C::GPL; g++) {
-        const int idx = lane + 32 * g;
-        vmr[g] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+        for (int g = 0; g < C::GPL; g++) {
+          const int idx = lane + 32 * g;
+          vmr[g] = idx < ne * NFF ? compact_neighbour_node<Np, Nfp>(a, e0, idx) : -1;
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < C::GPL; g++) {
+          const int idx = lane + 32 * g;
+          vmr[g] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+        }
       }
 #pragma unroll
       for (int g = 0; g < C::GPL; g++) {

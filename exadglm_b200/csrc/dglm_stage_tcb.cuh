@@ -474,10 +474,18 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       else if (lane == NV + 1)
         bulk_g2s(bT, a.tau + 4 * e0, 8u * C::S_TAU, &full[b]);
       int vmr[C::GPL];
+      if (a.etoe) {
 #pragma unroll
-      for (int g = 0; g < C::GPL; g++) {
-        const int idx = lane + 32 * g;
-        vmr[g] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+        for (int g = 0; g < C::GPL; g++) {
+          const int idx = lane + 32 * g;
+          vmr[g] = idx < ne * NFF ? compact_neighbour_node<Np, Nfp>(a, e0, idx) : -1;
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < C::GPL; g++) {
+          const int idx = lane + 32 * g;
+          vmr[g] = idx < ne * NFF ? __ldg(a.vmapP + e0 * NFF + idx) : -1;
+        }
       }
 #pragma unroll
       for (int g = 0; g < C::GPL; g++) {

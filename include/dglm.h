@@ -183,6 +183,23 @@ int dglm_get_variant(dglm_handle *h);
  * this is how the expiry path is tested.  No counterpart in the reference,
  * whose kernels have no waits between warps. */
 dglm_status dglm_set_wait_limit(dglm_handle *h, long long cycles);
+/* Compact face maps.  on = 1 builds, from the uploaded vmapP (once per mesh),
+ * per face (e, f) the neighbour element and a one-byte code of the
+ * neighbour's local node list (a table of at most 256 lists of Nfp node
+ * indices; a conforming tetrahedral mesh has at most 24), 5 bytes per face
+ * instead of 4 Nfp, and has the producer warps of the persistent stage
+ * kernels (FP64 pipelined, tensor-memory TF32 and BF16) form each neighbour
+ * node index from it instead of reading vmapP; the other kernels keep
+ * reading vmapP.  Results are bit for bit those of vmapP.  on = 0 returns
+ * to vmapP.  DGLM_ERR_UNSUPPORTED when a face's trace is not made of one
+ * element's nodes or the mesh needs more than 256 node lists.  The
+ * reference builds vmapP from the compact EtoE/EtoF connectivity
+ * (mesh_3d_core.cpp:309-356) and its kernels read vmapP
+ * (euler_nopad_dglm.cu:115-135). */
+dglm_status dglm_set_compact_face_maps(dglm_handle *h, int on);
+/* Distinct face node lists of the handle's compact face maps (0 before they
+ * are built). */
+int dglm_face_map_lists(dglm_handle *h);
 /* Number of kernels the last dglm_step call launched (for accounting). */
 long dglm_kernel_launches(dglm_handle *h);
 /* Device bytes held by the handle. */
