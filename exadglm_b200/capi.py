@@ -28,7 +28,8 @@ EXPORTS = (
     "dglm_update_tau", "dglm_update_ub", "dglm_calc_fluxLM", "dglm_calc_fluxes",
     "dglm_update_rhs", "dglm_lserk_stage", "dglm_variant_count", "dglm_variant_describe",
     "dglm_set_variant", "dglm_get_variant", "dglm_set_wait_limit",
-    "dglm_set_compact_face_maps", "dglm_face_map_lists", "dglm_adjoint_record", "dglm_adjoint_backward",
+    "dglm_set_compact_face_maps", "dglm_face_map_lists", "dglm_compact_face_maps",
+    "dglm_adjoint_record", "dglm_adjoint_backward",
     "dglm_adjoint_replay", "dglm_adjoint_rhs", "dglm_adjoint_tape_bytes",
     "dglm_adjoint_record_capped", "dglm_adjoint_tape_plan", "dglm_adjoint_schedule",
     "dglm_calc_maxv_dt_static", "dglm_adjoint_variant_count", "dglm_adjoint_variant_describe",
@@ -100,6 +101,9 @@ def lib():
         L.dglm_set_wait_limit.argtypes = [_P, C.c_longlong]
         L.dglm_set_compact_face_maps.argtypes = [_P, C.c_int]
         L.dglm_face_map_lists.argtypes = [_P]
+        L.dglm_compact_face_maps.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_int,
+                                             C.POINTER(C.c_int)]
         L.dglm_kernel_launches.argtypes = [_P]
         L.dglm_kernel_launches.restype = C.c_long
         L.dglm_device_bytes.argtypes = [_P]
@@ -202,6 +206,23 @@ def adjoint_schedule(nsteps, leaf, slots, prestored=True):
                                   spine.ctypes.data, len(spine), C.byref(ns), acts.ctypes.data,
                                   cap_a, C.byref(na), C.byref(adv)))
     return spine[:ns.value].copy(), acts[:na.value].copy(), adv.value
+
+
+def compact_face_maps(vmapP, Np, Nfp, max_lists=256):
+    """The compact form of a vmapP (K x 4 x Nfp) that
+    Solver.set_compact_face_maps builds (host only): (etoe, code, lists) with
+    vmapP[e, f, j] = etoe[e, f] Np + lists[code[e, f], j]."""
+    L = lib()
+    vm = np.ascontiguousarray(vmapP, dtype=np.int32).reshape(-1, 4, Nfp)
+    K = vm.shape[0]
+    etoe = np.zeros((K, 4), dtype=np.int32)
+    code = np.zeros((K, 4), dtype=np.uint8)
+    lists = np.zeros((max(int(max_lists), 1), Nfp), dtype=np.int32)
+    n = C.c_int()
+    check(L.dglm_compact_face_maps(K, int(Np), int(Nfp), vm.ctypes.data, etoe.ctypes.data,
+                                   code.ctypes.data, lists.ctypes.data, int(max_lists),
+                                   C.byref(n)))
+    return etoe, code, lists[:n.value].copy()
 
 
 def adjoint_variants(physics, N):

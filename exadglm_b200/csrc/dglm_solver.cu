@@ -1097,6 +1097,43 @@ dglm_status dglm_set_wait_limit(dglm_handle *h, long long cycles) {
   return DGLM_OK;
 }
 
+dglm_status dglm_compact_face_maps(int K, int Np, int Nfp, const int *vmapP, int *etoe,
+                                   unsigned char *code, int *lists, int max_lists,
+                                   int *n_lists) {
+  if (!vmapP || !etoe || !code || !n_lists || (max_lists > 0 && !lists))
+    return set_error(DGLM_ERR_INVALID, "dglm_compact_face_maps: NULL argument");
+  if (K < 1 || Np < 1 || Nfp < 1 || max_lists < 0 || max_lists > 256)
+    return set_error(DGLM_ERR_INVALID, "dglm_compact_face_maps: bad sizes");
+  // every face's trace must be one element's nodes; its local node list gets
+  // a code (first seen, first numbered)
+  std::map<std::vector<int>, int> seen;
+  std::vector<int> loc(Nfp);
+  for (size_t fc = 0; fc < (size_t)K * 4; fc++) {
+    const int *p = vmapP + fc * Nfp;
+    if (p[0] < 0 || (long long)p[0] >= (long long)K * Np)
+      return set_error(DGLM_ERR_INVALID, "dglm_compact_face_maps: vmapP entry outside [0, K*Np)");
+    const int n = p[0] / Np;
+    for (int j = 0; j < Nfp; j++) {
+      if (p[j] < 0 || p[j] / Np != n)
+        return set_error(DGLM_ERR_UNSUPPORTED,
+                         "dglm_compact_face_maps: a face's trace spans several elements");
+      loc[j] = p[j] - n * Np;
+    }
+    auto it = seen.find(loc);
+    if (it == seen.end()) {
+      if ((int)seen.size() == max_lists)
+        return set_error(DGLM_ERR_UNSUPPORTED,
+                         "dglm_compact_face_maps: more distinct face node lists than max_lists");
+      it = seen.emplace(loc, (int)seen.size()).first;
+      std::copy(loc.begin(), loc.end(), lists + (size_t)it->second * Nfp);
+    }
+    etoe[fc] = n;
+    code[fc] = (unsigned char)it->second;
+  }
+  *n_lists = (int)seen.size();
+  return DGLM_OK;
+}
+
 dglm_status dglm_set_compact_face_maps(dglm_handle *h, int on) {
   if (!h) return set_error(DGLM_ERR_INVALID, "dglm_set_compact_face_maps: NULL handle");
   if (!h->mesh_ready)
@@ -1109,41 +1146,20 @@ dglm_status dglm_set_compact_face_maps(dglm_handle *h, int on) {
     return DGLM_OK;
   }
   if (!h->compact_built) {
-    // from the uploaded vmapP: every face's trace must be one element's
-    // nodes; its local node list gets a code (first seen, first numbered)
     const int K = h->d.K, Np = h->Np, Nfp = h->Nfp, NFF = h->NFF;
-    std::vector<int> vm((size_t)K * NFF);
+    std::vector<int> vm((size_t)K * NFF), nb((size_t)K * 4), lists((size_t)256 * Nfp);
+    std::vector<unsigned char> code((size_t)K * 4);
     cudaError_t e = cudaMemcpy(vm.data(), h->vmapP, sizeof(int) * vm.size(),
                                cudaMemcpyDeviceToHost);
     if (e != cudaSuccess)
       return set_error(DGLM_ERR_CUDA, std::string("dglm_set_compact_face_maps: ") +
                                           cudaGetErrorString(e));
-    std::vector<int> nb((size_t)K * 4), lists;
-    std::vector<unsigned char> code((size_t)K * 4);
-    std::map<std::vector<int>, int> seen;
-    std::vector<int> loc(Nfp);
-    for (size_t fc = 0; fc < (size_t)K * 4; fc++) {
-      const int *p = vm.data() + fc * Nfp;
-      const int n = p[0] / Np;
-      for (int j = 0; j < Nfp; j++) {
-        if (p[j] / Np != n)
-          return set_error(DGLM_ERR_UNSUPPORTED,
-                           "dglm_set_compact_face_maps: a face's trace spans several elements");
-        loc[j] = p[j] - n * Np;
-      }
-      auto it = seen.find(loc);
-      if (it == seen.end()) {
-        if (seen.size() == 256)
-          return set_error(DGLM_ERR_UNSUPPORTED,
-                           "dglm_set_compact_face_maps: more than 256 distinct face node lists");
-        it = seen.emplace(loc, (int)seen.size()).first;
-        lists.insert(lists.end(), loc.begin(), loc.end());
-      }
-      nb[fc] = n;
-      code[fc] = (unsigned char)it->second;
-    }
+    int nlists = 0;
+    dglm_status st = dglm_compact_face_maps(K, Np, Nfp, vm.data(), nb.data(), code.data(),
+                                            lists.data(), 256, &nlists);
+    if (st != DGLM_OK) return st;
     if (!h->etoe) {
-      dglm_status st = dalloc(h, &h->etoe, (size_t)K * 4);
+      st = dalloc(h, &h->etoe, (size_t)K * 4);
       if (st == DGLM_OK) st = dalloc(h, &h->fcode, (size_t)K * 4);
       if (st == DGLM_OK) st = dalloc(h, &h->ftab, (size_t)256 * Nfp);
       if (st != DGLM_OK) return st;
@@ -1152,11 +1168,11 @@ dglm_status dglm_set_compact_face_maps(dglm_handle *h, int on) {
     if (e == cudaSuccess)
       e = cudaMemcpy(h->fcode, code.data(), code.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-      e = cudaMemcpy(h->ftab, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice);
+      e = cudaMemcpy(h->ftab, lists.data(), sizeof(int) * nlists * Nfp, cudaMemcpyHostToDevice);
     if (e != cudaSuccess)
       return set_error(DGLM_ERR_CUDA, std::string("dglm_set_compact_face_maps: ") +
                                           cudaGetErrorString(e));
-    h->ftab_lists = (int)seen.size();
+    h->ftab_lists = nlists;
     h->compact_built = true;
   }
   h->compact = true;

@@ -200,6 +200,17 @@ dglm_status dglm_set_compact_face_maps(dglm_handle *h, int on);
 /* Distinct face node lists of the handle's compact face maps (0 before they
  * are built). */
 int dglm_face_map_lists(dglm_handle *h);
+/* Host only: the compact form of a vmapP (K x 4 x Nfp ints) that
+ * dglm_set_compact_face_maps builds.  etoe[4e+f] is the neighbour element,
+ * code[4e+f] the index of its local node list in lists (room for max_lists
+ * <= 256 lists of Nfp ints), so that vmapP[e][f][j] = etoe[4e+f] Np +
+ * lists[code[4e+f] Nfp + j]; *n_lists receives the number of lists.
+ * DGLM_ERR_UNSUPPORTED when a face's trace spans several elements or needs
+ * more than max_lists lists.  The reference derives vmapP from its EtoE/EtoF
+ * tables (mesh_3d_core.cpp:309-356) and keeps no compact form. */
+dglm_status dglm_compact_face_maps(int K, int Np, int Nfp, const int *vmapP, int *etoe,
+                                   unsigned char *code, int *lists, int max_lists,
+                                   int *n_lists);
 /* Number of kernels the last dglm_step call launched (for accounting). */
 long dglm_kernel_launches(dglm_handle *h);
 /* Device bytes held by the handle. */
