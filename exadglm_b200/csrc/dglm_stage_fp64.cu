@@ -665,8 +665,10 @@ __global__ void __launch_bounds__(Cfg<PHYS, N, MODE, E_, R_, CPT_, WM_, PR_>::TH
 // are in flight while one thread per (element, face) takes the face maxima
 // through Fmask.  Max is exact, so the result does not depend on the order;
 // one atomic per block.
+constexpr int kMaxvBlocksPerSM = 6;
 template <int PHYS, int N>
-__global__ void __launch_bounds__(256) face_maxv_kernel(const StageArgs a, int slot) {
+__global__ void __launch_bounds__(256, kMaxvBlocksPerSM)
+    face_maxv_kernel(const StageArgs a, int slot) {
   constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
   constexpr int ET = 256 / Np, NQ = PHYS == EUL ? 5 : 3;
   static_assert(ET >= 1 && 4 * ET <= 256, "a tile of whole elements fits the block");
@@ -1122,10 +1124,12 @@ cudaError_t launch_stage_fp64(int physics, int N, int variant, const StageArgs &
 
 template <int PHYS, int N>
 static cudaError_t launch_maxv_one(const StageArgs &a, int slot, cudaStream_t s) {
-  // tiles of 256 / Np whole elements, up to 8 blocks per SM walking them
+  // tiles of 256 / Np whole elements, walked by as many blocks as are
+  // resident at once (kMaxvBlocksPerSM by the launch bounds; a larger grid
+  // leaves a tail of late-starting blocks)
   constexpr int ET = 256 / np_of(N);
   long blocks = (a.K + ET - 1) / ET;
-  if (blocks > 8L * sm_count()) blocks = 8L * sm_count();
+  if (blocks > (long)kMaxvBlocksPerSM * sm_count()) blocks = (long)kMaxvBlocksPerSM * sm_count();
   face_maxv_kernel<PHYS, N><<<(int)blocks, 256, 0, s>>>(a, slot);
   return cudaGetLastError();
 }
