@@ -112,8 +112,8 @@ def read_traffic(desc, K):
     """Per-launch DRAM bytes of the stage kernel variant `desc` on a K-element
     mesh, from the committed ncu summaries (profiles/stage_traffic.txt: lines
     '<K> <bytes_per_launch> <variant shape>').  A capture on a smaller mesh of
-    the same variant is scaled by K (these kernels stream each element once,
-    so their traffic grows in proportion; DESIGN.md gives the check).  None
+    the same variant is scaled by K (these kernels stream each element's data
+    once per launch, so their DRAM traffic grows in proportion to K).  None
     when the variant has no capture."""
     path = os.path.join(ROOT, "profiles", "stage_traffic.txt")
     if not os.path.exists(path):
