@@ -1029,8 +1029,9 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
                                                                                 : "bf16x3",
              v.E, v.CPT, v.WM, v.threads, v.smem);
   else if (v.mode == MODE_TC)
-    snprintf(buf, len, "tc-tmem-tf32x4 E=%d compute=%d threads=%d smem=%zu ring=%d%s", v.E,
-             v.producers, v.threads, v.smem, v.ring, v.R == 2 ? " nodes/lane=2" : "");
+    snprintf(buf, len, "tc-tmem-tf32x4 E=%d compute=%d threads=%d smem=%zu ring=%d%s%s", v.E,
+             v.producers, v.threads, v.smem, v.ring, v.R == 2 ? " nodes/lane=2" : "",
+             v.WM == 1 ? " vol=fp32-diff" : "");
   else if (v.mode == MODE_TCB)
     snprintf(buf, len, "tc-tmem-bf16x4 E=%d compute=%d threads=%d smem=%zu ring=%d buffers=%d",
              v.E, v.producers, v.threads, v.smem, v.ring, v.npad);

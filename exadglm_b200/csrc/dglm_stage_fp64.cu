@@ -886,10 +886,10 @@ static Variant make_mixed() {
   return Variant{i, &launch_mixed<PHYS, N, E, PREC, NWC, PW>};
 }
 
-template <int PHYS, int N, int E, int NF, int NB, int NPL>
+template <int PHYS, int N, int E, int NF, int NB, int NPL, bool DF>
 static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
-  using C = TCfg<PHYS, N, E, NF, NB, NPL>;
-  auto k = stage_tc_kernel<PHYS, N, E, NF, NB, NPL>;
+  using C = TCfg<PHYS, N, E, NF, NB, NPL, DF>;
+  auto k = stage_tc_kernel<PHYS, N, E, NF, NB, NPL, DF>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -931,13 +931,14 @@ static Variant make_tcb() {
   return Variant{i, &launch_tcb<PHYS, N, E, NF, NB, DB>};
 }
 
-template <int PHYS, int N, int E, int NF, int NB, int NPL = 1>
+template <int PHYS, int N, int E, int NF, int NB, int NPL = 1, bool DF = false>
 static Variant make_tc() {
-  using C = TCfg<PHYS, N, E, NF, NB, NPL>;
+  using C = TCfg<PHYS, N, E, NF, NB, NPL, DF>;
   StageVariantInfo i{};
   i.mode = MODE_TC;
   i.E = E;
   i.R = NPL;          // nodes per lane in a flux task
+  i.WM = DF ? 1 : 0;  // 1: difference-form FP32 volume flux
   i.threads = C::THREADS;
   i.smem = C::SMEM;
   i.prec = DGLM_PREC_TF32X3;
@@ -948,7 +949,7 @@ static Variant make_tc() {
   i.ring = NB;
   i.producers = NF;   // compute warps
   i.persistent = 1;
-  return Variant{i, &launch_tc<PHYS, N, E, NF, NB, NPL>};
+  return Variant{i, &launch_tc<PHYS, N, E, NF, NB, NPL, DF>};
 }
 
 template <int PHYS, int N, int MODE, int E, int R, int CPT, int WM, int PR = 0>
@@ -1020,6 +1021,8 @@ static const std::vector<Variant> &variants();
 #define V_TC(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB>()
 // the same with two nodes per lane in each flux task
 #define V_TC2(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB, 2>()
+// the same with the centred volume flux in difference form in FP32
+#define V_TCD(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB, 1, true>()
 // split-BF16 with the operator in tensor memory: DB = double-buffered images and accumulators
 #define V_TCB(P, NN, E, NF, NB, DB) make_tcb<P, NN, E, NF, NB, DB>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
@@ -1049,7 +1052,7 @@ DGLM_VARIANTS(EUL, 4, V_PIPE(EUL, 4, 8, 1, 2, true), V_DMMA(EUL, 4, 8, 1, 5),
               V_PIPEF(EUL, 4, 8, 1, true, 3, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 1),
               V_PIPE2C(EUL, 4, 8, 5, 1, 2, 1), V_PIPE2C(EUL, 4, 8, 1, 5, 2, 2),
               V_TC(EUL, 4, 8, 14, 3), V_TCB(EUL, 4, 8, 14, 2, true),
-              V_TC2(EUL, 4, 8, 13, 3))
+              V_TC2(EUL, 4, 8, 13, 3), V_TCD(EUL, 4, 8, 14, 3))
 DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_SIMT(EUL, 5, 8, 7, 5), V_M16(EUL, 5, 8, 1, 2, 2), V_M16(EUL, 5, 8, 1, 2, 1),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),

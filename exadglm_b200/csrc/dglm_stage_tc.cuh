@@ -62,7 +62,7 @@
 // (with the default bound) for the MMAs and copies it issued, and leaves.
 #pragma once
 
-template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1>
+template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1, bool DF_ = false>
 struct TCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -97,6 +97,11 @@ struct TCfg {
   // (8 elements x 4 nodes of one face)
   // (8 elements x 8 nodes with NPL = 2 nodes per lane: pairs of groups)
   static constexpr int NPL = NPL_;
+  // DF: the centred volume flux F(u_i) - F(u_0) in difference form in FP32
+  // (vol_task_df), from each element's FP32 metrics and node-0 state, which
+  // the MMA warp writes one tile ahead: [slot][e][NDF] floats
+  static constexpr bool DF = DF_;
+  static constexpr int NDF = 17;
   static constexpr int NEB = E / 8, NJB = NFPP / 4;
   static constexpr int NGP = (NG + 1) / 2, NJP = (NJB + 1) / 2;
   static constexpr int VOL_WT = NEB * (NPL == 2 ? NGP : NG);
@@ -109,7 +114,9 @@ struct TCfg {
   static constexpr size_t OFF_RING = 2 * (size_t)B_BYTES;
   static constexpr size_t OFF_R = OFF_RING + 8 * (size_t)NB * S_BUF;
   static constexpr size_t OFF_C = OFF_R + (4 * (size_t)S_R + 15) / 16 * 16;
-  static constexpr size_t OFF_BAR = OFF_C + 8 * 2 * (size_t)S_C;
+  static constexpr int S_DF = DF ? 2 * E * NDF : 0;
+  static constexpr size_t OFF_DF = OFF_C + 8 * 2 * (size_t)S_C;
+  static constexpr size_t OFF_BAR = OFF_DF + (4 * (size_t)S_DF + 15) / 16 * 16;
   // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2],
   // cen[2]; then the tensor-memory address, Fmask, maxima
   static constexpr int NBARS = 2 * NB + 8;
@@ -128,6 +135,7 @@ struct TCfg {
                 "an epilogue lane holds both parts of its row's columns, split in halves");
   static_assert(NB >= 2 && NB <= 4, "ring of 2..4 tile buffers");
   static_assert(NPL == 1 || NPL == 2, "one or two nodes per lane in a flux task");
+  static_assert(!DF || NPL == 1, "the difference-form volume flux has one node per lane");
   static_assert((E * Np * 8) % 16 == 0, "16-byte bulk copies");
   static_assert(THREADS <= 1024 && NWARPS <= 32, "block size");
   static_assert(SMEM <= 232448, "shared memory per CTA exceeds 227 KB");
@@ -170,16 +178,17 @@ __device__ __forceinline__ void split_tf32_pair(double x, unsigned &hi, unsigned
   lo = __float_as_uint(f - __uint_as_float(hi));
 }
 
-template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1>
-__global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_>::THREADS, 1)
+template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1, bool DF_ = false>
+__global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_, DF_>::THREADS, 1)
     stage_tc_kernel(const StageArgs a, int ntiles) {
-  using C = TCfg<PHYS, N, E_, NC_, NB_, NPL_>;
+  using C = TCfg<PHYS, N, E_, NC_, NB_, NPL_, DF_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, NB = C::NB,
                 NC = C::NC, TC = C::TC, NCOL = C::NCOL;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   double *sRing = reinterpret_cast<double *>(smem_raw + C::OFF_RING);
   float *sR = reinterpret_cast<float *>(smem_raw + C::OFF_R);
   double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
+  float *sDF = reinterpret_cast<float *>(smem_raw + C::OFF_DF);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
   unsigned long long *full = bars, *empty = bars + NB, *flux_done = bars + 2 * NB,
                      *mma_done = flux_done + 2, *d_free = flux_done + 4, *cen = flux_done + 6;
@@ -325,6 +334,78 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_>::THREADS, 1)
         *reinterpret_cast<unsigned *>(sBf + (n >> 3) * C::SBO_F + off) = hv[v];
         *reinterpret_cast<unsigned *>(sBf + ((n + NCOL) >> 3) * C::SBO_F + off) = lv[v];
       }
+    };
+
+    // DF: the same volume task with the centred flux F(u_i) - F(u_0) formed
+    // in difference form in FP32.  With du = u_i - u_0 (an FP64 subtraction,
+    // rounded once) and the node-0 state (rho0, m0, v0 = m0/rho0, H0):
+    //   dv_a = (dm_a - v0_a drho) / rho_i,  d(m_a v_b) = dm_a v0_b + m_a,i dv_b,
+    //   dp = (gamma-1) (dE - d(m.v)/2),  d(H v_a) = dH v0_a + H_i dv_a,
+    // so no term cancels and FP32 carries each value to ~1e-7 of its size,
+    // the precision of the TF32 split that follows; the metric combination
+    // and the split run in FP32 too.
+    auto vol_task_df = [&](int it, int wt, int ne, unsigned char *sBv) {
+      const int eb = wt / C::NG, g = wt - eb * C::NG;
+      const int e = eb * 8 + (lane & 7), i = 4 * g + (lane >> 3);
+      const bool okn = e < ne && i < Np;
+      const double *bU = ring(it);
+      unsigned hv[5][3], lv[5][3];
+      if (okn) {
+        const float *sd = sDF + (it & 1) * E * C::NDF + e * C::NDF;
+        float du[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+          du[v] = __double2float_rn(bU[v * E * Np + e * Np + i] - bU[v * E * Np + e * Np]);
+        const float v0[3] = {sd[10], sd[11], sd[12]}, m0[3] = {sd[13], sd[14], sd[15]};
+        const float dr = du[0], dE = du[4], ir1 = 1.0f / (sd[9] + dr);
+        float dv[3], m1[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          dv[c] = (du[1 + c] - v0[c] * dr) * ir1;
+          m1[c] = m0[c] + du[1 + c];
+        }
+        float dmv[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int b = 0; b < 3; b++) dmv[c][b] = fmaf(du[1 + c], v0[b], m1[c] * dv[b]);
+        const float dp = (float)(gam - 1.0) * (dE - 0.5f * (dmv[0][0] + dmv[1][1] + dmv[2][2]));
+        const float dH = dE + dp, H1 = sd[16] + dH;
+        // direction b: (dm_b, d(m_x v_b), d(m_y v_b), d(m_z v_b), d(H v_b)) + dp on 1 + b
+        float Fd[3][5];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          Fd[b][0] = du[1 + b];
+          Fd[b][1] = dmv[0][b];
+          Fd[b][2] = dmv[1][b];
+          Fd[b][3] = dmv[2][b];
+          Fd[b][4] = fmaf(dH, v0[b], H1 * dv[b]);
+          Fd[b][1 + b] += dp;
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const float X =
+                fmaf(sd[3 * d + 2], Fd[2][v], fmaf(sd[3 * d + 1], Fd[1][v], sd[3 * d] * Fd[0][v]));
+            hv[v][d] = __float_as_uint(X) & 0xffffe000u;
+            lv[v][d] = __float_as_uint(X - __uint_as_float(hv[v][d]));
+          }
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+#pragma unroll
+          for (int d = 0; d < 3; d++) hv[v][d] = lv[v][d] = 0u;
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const int n = v * E + e, k = g * 12 + d * 4 + (lane >> 3);
+          const int off = (k >> 2) * 128 + (n & 7) * 16 + (k & 3) * 4;
+          *reinterpret_cast<unsigned *>(sBv + (n >> 3) * C::SBO_V + off) = hv[v][d];
+          *reinterpret_cast<unsigned *>(sBv + ((n + NCOL) >> 3) * C::SBO_V + off) = lv[v][d];
+        }
     };
 
     // NPL = 2: task wt of the volume covers 8 elements x node groups 2gp and
@@ -584,6 +665,11 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_>::THREADS, 1)
             vol_task2(it, wt, ne, sBv);
           else
             face_task2(it, wt - C::VOL_WT, ne, sBf);
+        } else if constexpr (C::DF) {
+          if (wt < C::VOL_WT)
+            vol_task_df(it, wt, ne, sBv);
+          else
+            face_task(it, wt - C::VOL_WT, ne, sBf);
         } else {
           if (wt < C::VOL_WT)
             vol_task(it, wt, ne, sBv);
@@ -677,11 +763,32 @@ __global__ void __launch_bounds__(TCfg<PHYS, N, E_, NC_, NB_, NPL_>::THREADS, 1)
       for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
       euler_flux_fast(gam, q, F, G, W);
       if (r == 0) {
+        if constexpr (C::DF) {
+          // FP32 metrics and node-0 state of the difference-form volume flux
+          float *sd = sDF + (t & 1) * E * C::NDF + e * C::NDF;
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-          const double mx = bR[3 * d], my = bR[3 * d + 1], mz = bR[3 * d + 2];
+          for (int x = 0; x < 9; x++) sd[x] = __double2float_rn(bR[x]);
+          const float r0 = __double2float_rn(q[0]), E0 = __double2float_rn(q[4]);
+          const float m0[3] = {__double2float_rn(q[1]), __double2float_rn(q[2]),
+                               __double2float_rn(q[3])};
+          const float ir0 = 1.0f / r0;
+          const float v0[3] = {m0[0] * ir0, m0[1] * ir0, m0[2] * ir0};
+          const float p0 =
+              (float)(gam - 1.0) * (E0 - 0.5f * (m0[0] * v0[0] + m0[1] * v0[1] + m0[2] * v0[2]));
+          sd[9] = r0;
 #pragma unroll
-          for (int v = 0; v < 5; v++) c[v * C::NCEN + d] = mx * F[v] + my * G[v] + mz * W[v];
+          for (int c2 = 0; c2 < 3; c2++) {
+            sd[10 + c2] = v0[c2];
+            sd[13 + c2] = m0[c2];
+          }
+          sd[16] = E0 + p0;
+        } else {
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const double mx = bR[3 * d], my = bR[3 * d + 1], mz = bR[3 * d + 2];
+#pragma unroll
+            for (int v = 0; v < 5; v++) c[v * C::NCEN + d] = mx * F[v] + my * G[v] + mz * W[v];
+          }
         }
       } else {
         const int nf = r == 3 ? 2 : 1;   // r = 1: face 0, r = 2: face 1, r = 3: faces 2, 3
