@@ -69,7 +69,11 @@ typedef enum {
 } dglm_precision;
 /* In every mixed mode the Euler fluxes are centred on each element's node-0
  * flux before the split (the right-hand side is unchanged); the LSERK state,
- * fluxes, metrics and update stay FP64. */
+ * the face fluxes, the metrics and the update stay FP64.  The volume fluxes
+ * are FP64 too, except in the TF32 tensor-memory variant "vol=fp32-diff"
+ * (the tuned pick for Euler N=4 TF32X3), which forms the centred volume
+ * flux F(u_i) - F(u_0) in difference form in FP32 from u_i - u_0 (an FP64
+ * subtraction), where no term cancels, to about the precision of the split. */
 
 /* Solver description: the reference's compile-time common.h parameters
  * (dglm_3d_launcher.py:152-205) as run-time values. */
