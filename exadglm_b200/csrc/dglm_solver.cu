@@ -1033,8 +1033,9 @@ dglm_status dglm_variant_describe(int physics, int N, int variant, char *buf, si
              v.producers, v.threads, v.smem, v.ring, v.R == 2 ? " nodes/lane=2" : "",
              v.WM == 1 ? " vol=fp32-diff" : "");
   else if (v.mode == MODE_TCB)
-    snprintf(buf, len, "tc-tmem-bf16x4 E=%d compute=%d threads=%d smem=%zu ring=%d buffers=%d",
-             v.E, v.producers, v.threads, v.smem, v.ring, v.npad);
+    snprintf(buf, len, "tc-tmem-bf16x4 E=%d compute=%d threads=%d smem=%zu ring=%d buffers=%d%s",
+             v.E, v.producers, v.threads, v.smem, v.ring, v.npad,
+             v.WM == 1 ? " vol=fp32-diff" : "");
   else if (v.mode == MODE_MIXED) {
     const int n = snprintf(buf, len, "%s E=%d N=%d threads=%d smem=%zu",
                            v.prec == DGLM_PREC_TF32X3   ? "tcgen05-tf32x3"

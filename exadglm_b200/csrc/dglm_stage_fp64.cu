@@ -899,10 +899,10 @@ static cudaError_t launch_tc(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int NF, int NB, bool DB>
+template <int PHYS, int N, int E, int NF, int NB, bool DB, bool DF>
 static cudaError_t launch_tcb(const StageArgs &a, cudaStream_t s) {
-  using C = TBCfg<PHYS, N, E, NF, NB, DB>;
-  auto k = stage_tcb_kernel<PHYS, N, E, NF, NB, DB>;
+  using C = TBCfg<PHYS, N, E, NF, NB, DB, DF>;
+  auto k = stage_tcb_kernel<PHYS, N, E, NF, NB, DB, DF>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)C::SMEM);
   if (e != cudaSuccess) return e;
@@ -912,9 +912,9 @@ static cudaError_t launch_tcb(const StageArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <int PHYS, int N, int E, int NF, int NB, bool DB>
+template <int PHYS, int N, int E, int NF, int NB, bool DB, bool DF = false>
 static Variant make_tcb() {
-  using C = TBCfg<PHYS, N, E, NF, NB, DB>;
+  using C = TBCfg<PHYS, N, E, NF, NB, DB, DF>;
   StageVariantInfo i{};
   i.mode = MODE_TCB;
   i.E = E;
@@ -928,7 +928,8 @@ static Variant make_tcb() {
   i.ring = NB;
   i.producers = NF;      // compute warps
   i.persistent = 1;
-  return Variant{i, &launch_tcb<PHYS, N, E, NF, NB, DB>};
+  i.WM = DF ? 1 : 0;     // 1: difference-form FP32 volume flux
+  return Variant{i, &launch_tcb<PHYS, N, E, NF, NB, DB, DF>};
 }
 
 template <int PHYS, int N, int E, int NF, int NB, int NPL = 1, bool DF = false>
@@ -1025,6 +1026,8 @@ static const std::vector<Variant> &variants();
 #define V_TCD(P, NN, E, NF, NB) make_tc<P, NN, E, NF, NB, 1, true>()
 // split-BF16 with the operator in tensor memory: DB = double-buffered images and accumulators
 #define V_TCB(P, NN, E, NF, NB, DB) make_tcb<P, NN, E, NF, NB, DB>()
+// the same with the centred volume flux in difference form in FP32
+#define V_TCBD(P, NN, E, NF, NB, DB) make_tcb<P, NN, E, NF, NB, DB, true>()
 #define DGLM_VARIANTS(P, NN, ...)                        \
   template <>                                            \
   const std::vector<Variant> &variants<P, NN>() {        \
@@ -1058,7 +1061,7 @@ DGLM_VARIANTS(EUL, 5, V_PIPE(EUL, 5, 8, 1, 7, false), V_DMMA(EUL, 5, 8, 1, 7),
               V_M16(EUL, 5, 8, 1, 2, 3), V_PIPEF(EUL, 5, 8, 1, false, 3, 2),
               V_PM16G(EUL, 5, 8, 1, 2, 1, 2), V_PIPEFW(EUL, 5, 8, 5, 1, false, 1, 2),
               V_PIPEFW(EUL, 5, 8, 5, 1, false, 2, 2), V_PIPEFW(EUL, 5, 8, 5, 2, false, 3, 2),
-              V_TCB(EUL, 5, 8, 14, 2, true))
+              V_TCB(EUL, 5, 8, 14, 2, true), V_TCBD(EUL, 5, 8, 14, 2, true))
 DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEG(EUL, 6, 8, 1, false, 2, 2), V_PIPEG(EUL, 6, 8, 1, false, 2, 1),
               V_PM16G(EUL, 6, 8, 1, 2, 1, 2), V_PM16G(EUL, 6, 8, 1, 2, 2, 2),
@@ -1067,7 +1070,8 @@ DGLM_VARIANTS(EUL, 6, V_DMMA(EUL, 6, 8, 1, 6), V_SIMT(EUL, 6, 8, 7, 5),
               V_PIPEGW(EUL, 6, 8, 5, 1, 1, 2), V_PIPEGW(EUL, 6, 8, 5, 1, 2, 2),
               V_PIPEGW(EUL, 6, 8, 5, 2, 2, 2), V_PIPEGW(EUL, 6, 8, 5, 2, 3, 2),
               V_PIPEGW(EUL, 6, 8, 5, 3, 2, 2), V_PIPEGW(EUL, 6, 8, 5, 3, 3, 2),
-              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 1), V_TCB(EUL, 6, 8, 14, 2, false))
+              V_PIPEGW(EUL, 6, 8, 5, 2, 2, 1), V_TCB(EUL, 6, 8, 14, 2, false),
+              V_TCBD(EUL, 6, 8, 14, 2, false))
 DGLM_VARIANTS(EUL, 7, V_DMMA(EUL, 7, 8, 1, 5), V_SIMT(EUL, 7, 4, 8, 5))
 // N=8 Euler: the DMMA layout needs 8 elements per tile (40 columns), 242 KB
 DGLM_VARIANTS(EUL, 8, V_SIMT(EUL, 8, 4, 8, 5), V_SIMT(EUL, 8, 4, 6, 5))

@@ -27,7 +27,7 @@
 // KVA + f NFPP + j; KVA and KFA are multiples of 16 (one MMA's K).
 #pragma once
 
-template <int PHYS, int N, int E_, int NC_, int NB_, bool DBUF_>
+template <int PHYS, int N, int E_, int NC_, int NB_, bool DBUF_, bool DF_ = false>
 struct TBCfg {
   static constexpr int NV = PHYS == EUL ? 5 : 1;
   static constexpr int Np = np_of(N), Nfp = nfp_of(N), NFF = 4 * Nfp;
@@ -67,7 +67,12 @@ struct TBCfg {
   static constexpr size_t OFF_RING = NBUF * (size_t)B_BYTES;
   static constexpr size_t OFF_R = OFF_RING + 8 * (size_t)NB * S_BUF;
   static constexpr size_t OFF_C = OFF_R + 8 * (size_t)S_R;
-  static constexpr size_t OFF_BAR = OFF_C + 8 * 2 * (size_t)S_C;
+  // DF: the centred volume flux in difference form in FP32, as in
+  // stage_tc_kernel's vol_task_df; FP32 metrics and node-0 state [slot][e][NDF]
+  static constexpr bool DF = DF_;
+  static constexpr int NDF = 17, S_DF = DF ? 2 * E * NDF : 0;
+  static constexpr size_t OFF_DF = OFF_C + 8 * 2 * (size_t)S_C;
+  static constexpr size_t OFF_BAR = OFF_DF + (4 * (size_t)S_DF + 15) / 16 * 16;
   // barriers: full[NB], empty[NB], flux_done[2], mma_done[2], d_free[2],
   // cen[2], vol_done[2] (index 0 only for the single-buffered ones)
   static constexpr int NBARS = 2 * NB + 10;
@@ -108,16 +113,17 @@ __device__ __forceinline__ void split_bf16_pair(double x, unsigned short &hi,
   lo = __bfloat16_as_ushort(__float2bfloat16_rn(f - __bfloat162float(h)));
 }
 
-template <int PHYS, int N, int E_, int NC_, int NB_, bool DBUF_>
-__global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 1)
+template <int PHYS, int N, int E_, int NC_, int NB_, bool DBUF_, bool DF_ = false>
+__global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_, DF_>::THREADS, 1)
     stage_tcb_kernel(const StageArgs a, int ntiles) {
-  using C = TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>;
+  using C = TBCfg<PHYS, N, E_, NC_, NB_, DBUF_, DF_>;
   constexpr int NV = C::NV, Np = C::Np, Nfp = C::Nfp, NFF = C::NFF, E = C::E, NB = C::NB,
                 NC = C::NC, TC = C::TC, NCOL = C::NCOL, NBUF = C::NBUF;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   double *sRing = reinterpret_cast<double *>(smem_raw + C::OFF_RING);
   double *sR = reinterpret_cast<double *>(smem_raw + C::OFF_R);
   double *sC0 = reinterpret_cast<double *>(smem_raw + C::OFF_C);
+  float *sDF = reinterpret_cast<float *>(smem_raw + C::OFF_DF);
   unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + C::OFF_BAR);
   unsigned long long *full = bars, *empty = bars + NB, *flux_done = bars + 2 * NB,
                      *mma_done = flux_done + 2, *d_free = flux_done + 4, *cen = flux_done + 6,
@@ -213,6 +219,70 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
                                 fma(m[3 * d + 1], G[v], fma(m[3 * d], F[v],
                                                             -cn[v * C::NCEN + d]))),
                             hv[v][d], lv[v][d]);
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+#pragma unroll
+          for (int d = 0; d < 3; d++) hv[v][d] = lv[v][d] = 0;
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const int n = v * E + e, k = g * 12 + d * 4 + (lane >> 3);
+          *reinterpret_cast<unsigned short *>(sBv + boff(n, k, C::SBO_V)) = hv[v][d];
+          *reinterpret_cast<unsigned short *>(sBv + boff(n + NCOL, k, C::SBO_V)) = lv[v][d];
+        }
+    };
+    // DF: the centred volume flux in difference form in FP32 (the algebra of
+    // stage_tc_kernel's vol_task_df), split into BF16 parts
+    auto vol_task_df = [&](int it, int wt, int ne, unsigned char *sBv) {
+      const int eb = wt / C::NG, g = wt - eb * C::NG;
+      const int e = eb * 8 + (lane & 7), i = 4 * g + (lane >> 3);
+      const bool okn = e < ne && i < Np;
+      const double *bU = ring(it);
+      unsigned short hv[5][3], lv[5][3];
+      if (okn) {
+        const float *sd = sDF + (it & 1) * E * C::NDF + e * C::NDF;
+        float du[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+          du[v] = __double2float_rn(bU[v * E * Np + e * Np + i] - bU[v * E * Np + e * Np]);
+        const float v0[3] = {sd[10], sd[11], sd[12]}, m0[3] = {sd[13], sd[14], sd[15]};
+        const float dr = du[0], dE = du[4], ir1 = 1.0f / (sd[9] + dr);
+        float dv[3], m1[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          dv[c] = (du[1 + c] - v0[c] * dr) * ir1;
+          m1[c] = m0[c] + du[1 + c];
+        }
+        float dmv[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int b = 0; b < 3; b++) dmv[c][b] = fmaf(du[1 + c], v0[b], m1[c] * dv[b]);
+        const float dp = (float)(gam - 1.0) * (dE - 0.5f * (dmv[0][0] + dmv[1][1] + dmv[2][2]));
+        const float dH = dE + dp, H1 = sd[16] + dH;
+        float Fd[3][5];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          Fd[b][0] = du[1 + b];
+          Fd[b][1] = dmv[0][b];
+          Fd[b][2] = dmv[1][b];
+          Fd[b][3] = dmv[2][b];
+          Fd[b][4] = fmaf(dH, v0[b], H1 * dv[b]);
+          Fd[b][1 + b] += dp;
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const float X =
+                fmaf(sd[3 * d + 2], Fd[2][v], fmaf(sd[3 * d + 1], Fd[1][v], sd[3 * d] * Fd[0][v]));
+            const __nv_bfloat16 h = __float2bfloat16_rn(X);
+            hv[v][d] = __bfloat16_as_ushort(h);
+            lv[v][d] = __bfloat16_as_ushort(__float2bfloat16_rn(X - __bfloat162float(h)));
+          }
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++)
@@ -409,7 +479,10 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       if (warp >= C::VOL_WT) vol_signal();
       for (int wt = warp; wt < C::NTASK; wt += NC) {
         if (wt < C::VOL_WT) {
-          vol_task(it, wt, ne, sBv);
+          if constexpr (C::DF)
+            vol_task_df(it, wt, ne, sBv);
+          else
+            vol_task(it, wt, ne, sBv);
           if (wt + NC >= C::VOL_WT) vol_signal();
         } else {
           face_task(it, wt - C::VOL_WT, ne, sBf);
@@ -519,11 +592,32 @@ __global__ void __launch_bounds__(TBCfg<PHYS, N, E_, NC_, NB_, DBUF_>::THREADS, 
       for (int v = 0; v < 5; v++) q[v] = bU[v * E * Np + e * Np];
       euler_flux_fast(gam, q, F, G, W);
       if (r == 0) {
+        if constexpr (C::DF) {
+          // FP32 metrics and node-0 state of the difference-form volume flux
+          float *sd = sDF + (t & 1) * E * C::NDF + e * C::NDF;
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-          const double mx = bR[3 * d], my = bR[3 * d + 1], mz = bR[3 * d + 2];
+          for (int x = 0; x < 9; x++) sd[x] = __double2float_rn(bR[x]);
+          const float r0 = __double2float_rn(q[0]), E0 = __double2float_rn(q[4]);
+          const float m0[3] = {__double2float_rn(q[1]), __double2float_rn(q[2]),
+                               __double2float_rn(q[3])};
+          const float ir0 = 1.0f / r0;
+          const float v0[3] = {m0[0] * ir0, m0[1] * ir0, m0[2] * ir0};
+          const float p0 =
+              (float)(gam - 1.0) * (E0 - 0.5f * (m0[0] * v0[0] + m0[1] * v0[1] + m0[2] * v0[2]));
+          sd[9] = r0;
 #pragma unroll
-          for (int v = 0; v < 5; v++) c[v * C::NCEN + d] = mx * F[v] + my * G[v] + mz * W[v];
+          for (int c2 = 0; c2 < 3; c2++) {
+            sd[10 + c2] = v0[c2];
+            sd[13 + c2] = m0[c2];
+          }
+          sd[16] = E0 + p0;
+        } else {
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const double mx = bR[3 * d], my = bR[3 * d + 1], mz = bR[3 * d + 2];
+#pragma unroll
+            for (int v = 0; v < 5; v++) c[v * C::NCEN + d] = mx * F[v] + my * G[v] + mz * W[v];
+          }
         }
       } else {
         const int nf = r == 3 ? 2 : 1;   // r = 1: face 0, r = 2: face 1, r = 3: faces 2, 3
