@@ -60,6 +60,12 @@
 // The tensor cores work on tile t while the compute warps finish t-1 and
 // start t+1.  Every wait is bounded; on expiry a warp sets flag bit 2, waits
 // (with the default bound) for the MMAs and copies it issued, and leaves.
+//
+// Variants: NPL = 2 gives each lane two nodes of a flux task (13 tasks per
+// tile at N=4); DF forms the centred volume flux in difference form in FP32
+// (vol_task_df: no cancelling term, ~1e-7 of each value, the split's own
+// precision) from each element's FP32 metrics and node-0 state, which the
+// MMA warp writes with the node-0 terms.  The face flux stays FP64 in all.
 #pragma once
 
 template <int PHYS, int N, int E_, int NC_, int NB_, int NPL_ = 1, bool DF_ = false>
